@@ -1,0 +1,331 @@
+"""Benchmark: spectral paths/s of the 1920x1080 thin-film sphere scene.
+
+Workload (one step = one full frame): 64 thin-film spheres (r = 0.4, jittered 8x8
+grid, seed 3; film n = [1 1.33 1.5], Worley thickness 200-800 nm at frequency 3),
+Lambertian ground (0.5), one quad light (10); 1920x1080, depth 16, 256 spp,
+380-780 nm, render seed 3. 530,841,600 spectral paths per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode surrogate|exact]
+  python bench.py --impl reference ...   (the reference's CPU renderer, same workload)
+
+`value` is device time (CUDA events on the library's stream) with the image left
+in HBM; `e2e` goes through the C ABI with host buffers every step (scene upload
+H2D, image D2H). Between timed steps L2 is flushed by writing 256 MB. For N > 1
+each rank renders its own frame (replicas, weak scaling) and the slowest rank's
+time counts.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "spectral paths/sec on 1080p thin-film scene at ≤1% relRMSE, MLP vs exact TMM"
+UNIT = "spectral paths/s"
+WORKLOAD = ("thinfilm_spheres 1920x1080 depth16 256spp 380-780nm: 64 spheres r=0.4 jittered 8x8 (seed 3), "
+            "thinfilm [1 1.33 1.5] worley 200-800nm freq 3, lambertian ground 0.5, quad light 10, render seed 3")
+W, H, SPP, DEPTH = 1920, 1080, 256, 16
+
+
+def peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(n_gpus: int):
+    if n_gpus <= 1 and "RANK" not in os.environ:
+        return 0, 1, 0
+    import datetime
+
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", n_gpus))
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    import torch
+
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's CPU renderer (oracle/_ref), else the C port
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(lrd: str, seed: int, target_s: float = 15.0):
+    """Times the reference's Renderer::renderImage on all host threads over a
+    bounded sample: the full 1920x1080 frame at a reduced, perfect-square spp
+    chosen so the timed render takes about target_s seconds."""
+    from oracle import ref
+
+    if not ref.available():
+        return None
+    r = ref.RefScene(lrd)
+    threads = ref.max_threads()
+    r.set_samples(1)
+    _, t1 = r.render(seed, threads)
+    spp = max(1, int(math.floor(math.sqrt(max(1.0, target_s / max(t1, 1e-3))))) ** 2)
+    spp = min(spp, SPP)
+    r.set_samples(spp)
+    _, secs = r.render(seed, threads)
+    paths = W * H * spp
+    return {"value": paths / secs, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"full 1920x1080 frame at {spp} spp of the 256-spp workload ({paths} paths, {secs:.2f} s)",
+            "seconds": secs}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return 0
+    from lambda_b200 import scenes
+
+    d = tempfile.mkdtemp()
+    sc = scenes.thinfilm_spheres(d, W, H, SPP, DEPTH)
+    from oracle import ref
+
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_lambda.so not built"}))
+        return 0
+    r = ref.RefScene(sc.lrd)
+    threads = ref.max_threads()
+    # calibrate a per-step sample of about 10 s
+    r.set_samples(1)
+    _, t1 = r.render(sc.seed, threads)
+    spp = max(1, int(math.floor(math.sqrt(max(1.0, 10.0 / max(t1, 1e-3))))) ** 2)
+    r.set_samples(spp)
+    for _ in range(args.warmup):
+        r.render(sc.seed, threads)
+    total = 0.0
+    for _ in range(args.steps):
+        _, s = r.render(sc.seed, threads)
+        total += s
+    paths = W * H * spp * args.steps
+    value = paths / total
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample": f"{spp} spp per step of the 256-spp frame",
+                   "parallelism": f"OpenMP {threads} threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"full 1920x1080 frame at {spp} spp per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lambda_b200", choices=["lambda_b200", "reference"])
+    ap.add_argument("--mode", default="auto", choices=["auto", "surrogate", "exact"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spp", type=int, default=SPP)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+
+    rank, world, local = dist_init(args.gpus)
+    import torch
+
+    import lambda_b200 as lb
+    from lambda_b200 import scenes
+
+    d = tempfile.mkdtemp()
+    sc = scenes.thinfilm_spheres(d, W, H, args.spp, DEPTH)
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx = lb.Context(local)
+    ctx.upload(scene)
+
+    mode = args.mode
+    if mode in ("auto", "surrogate"):
+        try:
+            from lambda_b200 import surrogate as lbs
+
+            lbs.install(ctx)
+            mode = "surrogate"
+        except Exception as e:  # no trained weights: the exact form is what can run
+            if args.mode == "surrogate":
+                raise
+            mode = "exact"
+            if rank == 0:
+                print(f"# surrogate unavailable ({e}); measuring the exact transfer matrix", file=sys.stderr)
+    flags = lb.RENDER_THINFILM_SURROGATE if mode == "surrogate" else lb.RENDER_THINFILM_EXACT
+    dev_out = torch.empty((H, W, 3), dtype=torch.float32, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    desc = scene.render_desc(seed=sc.seed, flags=flags | lb.RENDER_OUTPUT_DEVICE)
+    paths_per_step = W * H * args.spp
+
+    for _ in range(args.warmup):
+        ctx.render(desc, out=dev_out)
+    torch.cuda.synchronize()
+    barrier(world)
+
+    launches = 0
+    total_ms = 0.0
+    stats = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ctx.render(desc, out=dev_out)
+            st = ctx.stats()
+            stats.append(st)
+            total_ms += st.render_ms
+            launches += st.kernel_launches
+        torch.cuda.synchronize()
+    barrier(world)
+    max_ms = max_over_ranks(total_ms, world)
+    value = world * paths_per_step * args.steps / (max_ms / 1000.0)
+
+    # per-stage kernel times (CUDA events inside the library) for the roofline
+    stage = lb.stage_profile(ctx, desc, dev_out)
+
+    # end to end through the C ABI with host buffers
+    host_out = torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy()
+    e2e_desc = scene.render_desc(seed=sc.seed, flags=flags)
+    h2d = lb.scene_bytes(scene)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.upload(scene)
+        ctx.render(e2e_desc, out=host_out)
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(t1 - t0, world)
+    e2e_value = world * paths_per_step * args.steps / e2e_s
+
+    if rank == 0:
+        hbm, tf, tf_sus, peak_kind = peaks()
+        roof = lb.roofline(stage, hbm, tf, peak_kind)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if mode == "exact" else "f32+bf16",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "spp": args.spp, "thinfilm": mode,
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
+                       "paths_per_step": paths_per_step},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": W * H * 12},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "roofline": roof,
+            "stages": stage,
+            "segments_per_path": stats[-1].segments / stats[-1].paths,
+        }
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(sc.lrd, sc.seed)
+            if cb is not None:
+                cb.pop("seconds", None)
+                out["cpu_baseline"] = cb
+        print(json.dumps(out))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,376 @@
+/*
+ * lambda_gpu.h - C ABI of the B200 spectral path-tracing render loop.
+ *
+ * The reference renderer's boundary is a C++ class plus one kernel:
+ *   Parser::parseLRD      src/core/parser.h:29   (scene file -> 15 host containers)
+ *   Renderer::setScene    src/render/renderer.h:38
+ *   Renderer::setCamera   src/render/renderer.h:36
+ *   Renderer::setBuffer   src/render/renderer.h:40
+ *   Renderer::renderImage src/render/renderer.h:42  (CPU) / renderKernel :200 (GPU)
+ *   Writer::write         src/core/writer.h:11
+ * This header replaces that boundary with plain C: POD scene arrays that keep the
+ * reference containers' indices and byte layouts, opaque handles, and status codes.
+ * No entry point throws; every failure is a lambda_status plus a message that
+ * lambda_last_error() returns.
+ *
+ * Pointers: unless an entry point says otherwise, array arguments may be host or
+ * device memory. The library asks the CUDA runtime which one it was given and
+ * stages host memory through its own device buffers.
+ */
+#ifndef LAMBDA_GPU_H
+#define LAMBDA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LAMBDA_ABI_VERSION 1
+
+/* Wavelength grid of every dense spectrum: 1 nm bins over [360, 830] nm
+ * (src/core/constants.h:20-22, src/math/spectrum.h:158-188). */
+#define LAMBDA_CIE_LAMBDA_MIN 360
+#define LAMBDA_CIE_LAMBDA_MAX 830
+#define LAMBDA_CIE_BINS 471
+/* Wavelengths carried by one path (hero wavelength + 3 rotations), constants.h:12. */
+#define LAMBDA_HERO_COUNT 4
+
+typedef enum lambda_status {
+    LAMBDA_OK = 0,
+    LAMBDA_ERR_INVALID_ARGUMENT = 1,
+    LAMBDA_ERR_PARSE = 2,          /* scene file error: message is "file:line: text" */
+    LAMBDA_ERR_IO = 3,             /* file could not be opened or written */
+    LAMBDA_ERR_CUDA = 4,           /* CUDA runtime error */
+    LAMBDA_ERR_OUT_OF_MEMORY = 5,
+    LAMBDA_ERR_NO_SCENE = 6,       /* render or trace before lambda_scene_upload */
+    LAMBDA_ERR_UNSUPPORTED = 7,    /* input outside what this build implements */
+    LAMBDA_ERR_QUEUE_OVERFLOW = 8, /* a device work queue or traversal stack overflowed */
+    LAMBDA_ERR_TIMEOUT = 9,        /* a bounded device wait gave up */
+    LAMBDA_ERR_ABORTED = 10,       /* the caller's abort flag was raised */
+    LAMBDA_ERR_INTERNAL = 11
+} lambda_status;
+
+/* ---------------------------------------------------------------------------
+ * Flat scene: the 15 containers Parser::parseLRD fills (parser.h:29), in the
+ * reference's order after BVH::makeBVH reordered objects and instances
+ * (bvh.h:61-108). Each struct has the byte layout of the reference class it
+ * mirrors, so indices and bytes can be compared one to one.
+ * ------------------------------------------------------------------------- */
+
+/* ObjectType, src/scene/object.h:13 */
+enum { LAMBDA_OBJECT_SPHERE = 0, LAMBDA_OBJECT_QUAD = 1, LAMBDA_OBJECT_TRI = 2 };
+
+/* class Object, object.h:15-164 (116 bytes).
+ * sphere: g[0..2] center, g[3] radius
+ * quad:   g[0..2] corner, g[3..5] horizontal, g[6..8] vertical, g[9..11] normal = horizontal x vertical
+ * tri:    as quad, then g[12..20] vertex normals n0 n1 n2, g[21..23] u0 u1 u2, g[24..26] v0 v1 v2 */
+typedef struct lambda_object {
+    int32_t type;
+    int32_t material;
+    float g[27];
+} lambda_object;
+
+/* class Instance, src/scene/instance.h:11-116 (144 bytes). transform = T*Rz*Ry*Rx*S,
+ * row-major; inverse_transform is its cofactor inverse. material < 0 means "use the
+ * object's own material" (instance.h:38). node is the root of the object's BLAS. */
+typedef struct lambda_instance {
+    int32_t object;
+    int32_t count;
+    int32_t node;
+    int32_t material;
+    float transform[16];
+    float inverse_transform[16];
+} lambda_instance;
+
+/* class BVHNode, src/scene/bvh.h:14-57 (32 bytes). Leaf iff count > 0; a leaf's
+ * index is its first instance (TLAS) or object (BLAS); an inner node's left
+ * child is the next node and index is its right child. */
+typedef struct lambda_bvh_node {
+    float min[3];
+    float max[3];
+    int32_t index;
+    int32_t count;
+} lambda_bvh_node;
+
+/* MaterialType, src/scene/material.h:15 */
+enum {
+    LAMBDA_MATERIAL_LAMBERTIAN = 0,
+    LAMBDA_MATERIAL_MIRROR = 1,
+    LAMBDA_MATERIAL_DIELECTRIC = 2,
+    LAMBDA_MATERIAL_EMISSIVE = 3,
+    LAMBDA_MATERIAL_THINFILM = 4
+};
+
+/* class Material, material.h:17-138 (16 bytes).
+ * lambertian/mirror: p[0] albedo spectrum texture; dielectric: p[0] n0, p[1] n1 spectra;
+ * emissive: p[0] emission spectrum texture;
+ * thinfilm: p[0] layer count L, p[1] offset of L+2 complex-spectrum indices in
+ * material_properties (outer medium, layers, substrate), p[2] offset of L scalar
+ * texture indices (layer thickness in nm). */
+typedef struct lambda_material {
+    int32_t type;
+    int32_t p[3];
+} lambda_material;
+
+/* ScalarTextureType, src/scene/texture.h:8 */
+enum { LAMBDA_SCALAR_CONSTANT = 0, LAMBDA_SCALAR_PERLIN = 1, LAMBDA_SCALAR_WORLEY = 2 };
+
+/* class ScalarTexture, texture.h:10-96 (16 bytes). constant: p[0] value;
+ * perlin/worley: p[0] min, p[1] max, p[2] frequency. */
+typedef struct lambda_scalar_texture {
+    int32_t type;
+    float p[3];
+} lambda_scalar_texture;
+
+/* SpectrumTextureType, texture.h:9 */
+enum { LAMBDA_SPECTRUM_CONSTANT = 0, LAMBDA_SPECTRUM_CHECKER = 1, LAMBDA_SPECTRUM_SCALAR = 2 };
+
+/* class SpectrumTexture, texture.h:98-210 (16 bytes). constant: value1 = spectrum;
+ * checker: value1, value2 spectra, scale; scalar: value1 = scalar texture. */
+typedef struct lambda_spectrum_texture {
+    int32_t type;
+    int32_t value1;
+    int32_t value2;
+    float scale;
+} lambda_spectrum_texture;
+
+/* class Camera, src/render/camera.h:7-19 */
+typedef struct lambda_camera {
+    float position[3];
+    float corner[3];
+    float horizontal[3];
+    float vertical[3];
+} lambda_camera;
+
+/* The Renderer constructor arguments (renderer.h:28) plus its camera. */
+typedef struct lambda_render_settings {
+    int32_t width;
+    int32_t height;
+    int32_t depth;        /* maximum bounce index; a path has at most depth+1 segments */
+    int32_t samples;      /* perfect square */
+    int32_t sqrt_samples;
+    float lambda_min;
+    float lambda_max;
+    lambda_camera camera;
+} lambda_render_settings;
+
+/* Renderer::setScene arguments (renderer.h:38). Background::makeEquirectangular
+ * holds only a spectrum texture index (background.h:9-17). */
+typedef struct lambda_scene_desc {
+    const float *spectra;              /* [num_spectra][471] */
+    int32_t num_spectra;
+    const double *complex_spectra;     /* [num_complex_spectra][471][2] (re, im) */
+    int32_t num_complex_spectra;
+    int32_t background_texture;
+    const lambda_object *objects;
+    int32_t num_objects;
+    const lambda_instance *instances;
+    int32_t num_instances;
+    const lambda_bvh_node *nodes;
+    int32_t num_nodes;
+    const int32_t *light_instances;    /* [num_lights]; the last light is the background (-1) */
+    const int32_t *light_objects;
+    const float *light_powers;
+    int32_t num_lights;
+    float total_light_power;
+    const lambda_material *materials;
+    int32_t num_materials;
+    const int32_t *material_properties;
+    int32_t num_material_properties;
+    const lambda_scalar_texture *scalar_textures;
+    int32_t num_scalar_textures;
+    const lambda_spectrum_texture *spectrum_textures;
+    int32_t num_spectrum_textures;
+} lambda_scene_desc;
+
+/* ---------------------------------------------------------------------------
+ * Host side: scene parsing and image output (no GPU needed).
+ * ------------------------------------------------------------------------- */
+
+typedef struct lambda_host_scene lambda_host_scene;
+
+/* Parser::parseLRD (src/core/parser.h:29-379) + Parser::parseOBJ (:639-786) +
+ * BVH::makeBVH (src/scene/bvh.h:61-108). Reads a .lrd file (and the .obj files it
+ * names), builds the two-level SAH BVH and the light list. On failure returns
+ * LAMBDA_ERR_PARSE or LAMBDA_ERR_IO and writes the reference's message text
+ * ("file:line: message" or "file: failed to open file (...)") into err. */
+lambda_status lambda_parse_lrd(const char *path, lambda_host_scene **out, char *err, size_t err_len);
+
+/* Views of a parsed scene; pointers stay valid until lambda_host_scene_destroy. */
+lambda_status lambda_host_scene_get(const lambda_host_scene *scene, lambda_scene_desc *desc,
+                                    lambda_render_settings *settings);
+
+void lambda_host_scene_destroy(lambda_host_scene *scene);
+
+/* Writer::hasValidExtension + Writer::write (src/core/writer.h:9-28): tonemap,
+ * sRGB OETF, dither from PCG32(0, 0) and write ASCII P3. rgb is host memory,
+ * [height][width][3] linear sRGB. Errors as in the reference (": invalid file
+ * extension", ": failed to open file (...)"). */
+lambda_status lambda_write_ppm(const char *path, int32_t width, int32_t height, const float *rgb,
+                               char *err, size_t err_len);
+
+/* ---------------------------------------------------------------------------
+ * GPU context.
+ * ------------------------------------------------------------------------- */
+
+typedef struct lambda_ctx lambda_ctx;
+
+/* Creates a context on one CUDA device (one stream, its own device arena). No
+ * reference counterpart: the reference uses the current device and managed memory
+ * (src/core/buffer.h:9-44). */
+lambda_status lambda_ctx_create(int32_t device, lambda_ctx **out);
+
+void lambda_ctx_destroy(lambda_ctx *ctx);
+
+/* Message of the last failed call on this context ("" if none). A NULL ctx
+ * returns the message of the last failed lambda_ctx_create on this thread. */
+const char *lambda_last_error(const lambda_ctx *ctx);
+
+/* Renderer::setScene (renderer.h:38) with the Buffer<T> uploads of main.cpp:84-103:
+ * copies the scene into device memory and derives the device layouts (SoA object
+ * records, light CDF, noise lattices). Replaces any previous scene. */
+lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene_desc *scene);
+
+/* Render flags */
+#define LAMBDA_RENDER_THINFILM_EXACT 0u       /* FP32 transfer-matrix thin-film reflectance */
+#define LAMBDA_RENDER_THINFILM_SURROGATE 1u   /* BF16 MLP on tensor cores, FP32 fallback per hit */
+#define LAMBDA_RENDER_OUTPUT_DEVICE 2u        /* out_rgb is device memory: no copy back */
+#define LAMBDA_RENDER_PROFILE_STAGES 4u       /* time every kernel launch with CUDA events (no graph replay) */
+
+typedef struct lambda_render_desc {
+    lambda_render_settings settings;
+    uint64_t seed;                            /* main.cpp:122 uses 42 */
+    uint32_t flags;
+    int32_t reserved;
+} lambda_render_desc;
+
+/* Renderer::renderImage(completed, seed) (renderer.h:42-55) / renderKernel
+ * (renderer.h:200-213): renders the uploaded scene and writes [height][width][3]
+ * linear sRGB floats (renderer.h:87-91) to out_rgb. Pixel (px, py) draws from PCG32
+ * stream py*width+px seeded with desc->seed, in the reference's order, so results
+ * follow the reference sample for sample. completed (may be NULL) is raised
+ * monotonically towards width*height while the call runs (pixels x finished
+ * sample waves / samples). Blocks until the image is written. */
+lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc *desc, float *out_rgb,
+                            volatile int32_t *completed);
+
+/* Per-render statistics of the last lambda_render on this context. */
+typedef struct lambda_render_stats {
+    double render_ms;          /* device time from first raygen to film write */
+    int64_t paths;             /* width*height*samples */
+    int64_t segments;          /* ray segments traced (closest-hit queries) */
+    int64_t shadow_rays;       /* NEE occlusion queries */
+    int64_t thinfilm_hits;     /* thin-film scatter events */
+    int64_t thinfilm_fallback; /* of those, evaluated exactly because the surrogate's range did not cover them */
+    int32_t kernel_launches;   /* kernels launched by the render */
+    int32_t waves;
+} lambda_render_stats;
+
+lambda_status lambda_get_render_stats(const lambda_ctx *ctx, lambda_render_stats *stats);
+
+/* Per-stage device time of the last render made with LAMBDA_RENDER_PROFILE_STAGES.
+ * Stages: 0 init, 1 wave prologue, 2 raygen, 3 intersect, 4 shade, 5 shadow,
+ * 6 finish, 7 thin-film surrogate eval, 8 thin-film scatter. items = paths or rays
+ * the stage processed over the whole render. No reference counterpart (the
+ * reference's single kernel has no stages). */
+#define LAMBDA_NUM_STAGES 9
+typedef struct lambda_stage_time {
+    double ms;
+    int64_t launches;
+    int64_t items;
+} lambda_stage_time;
+
+lambda_status lambda_get_stage_times(const lambda_ctx *ctx, lambda_stage_time *out /* [LAMBDA_NUM_STAGES] */);
+
+/* ---------------------------------------------------------------------------
+ * Ray queries on the uploaded scene: Scene::hit (src/scene/scene.h:51-124).
+ * ------------------------------------------------------------------------- */
+
+/* Closest hit of n rays; rays is [n][6] (origin xyz, direction xyz). Writes the
+ * hit instance and object index (-1 on a miss) and t (1e30 on a miss). Same
+ * arithmetic and visit order as the reference, so ids and t match bit for bit. */
+lambda_status lambda_trace_closest(lambda_ctx *ctx, const float *rays, int32_t n,
+                                   int32_t *out_instance, int32_t *out_object, float *out_t);
+
+/* Shadow queries Scene::hit(r, i, occludedInstance, occludedObject) (scene.h:51,
+ * renderer.h:166): occluded[k] = 1 when ray k does not reach light (instance,
+ * object) = (light_instance[k], light_object[k]); (-1, -1) is the background. */
+lambda_status lambda_trace_shadow(lambda_ctx *ctx, const float *rays, const int32_t *light_instance,
+                                  const int32_t *light_object, int32_t n, int32_t *out_occluded);
+
+/* ---------------------------------------------------------------------------
+ * Thin-film transfer matrix (material.h:263-309) and its learned surrogate.
+ * ------------------------------------------------------------------------- */
+
+/* One single-layer film query: outer medium index 1, film index n_film, substrate
+ * n_sub, all real; thickness in nm; cos_theta of incidence in the outer medium. */
+typedef struct lambda_film_query {
+    float lambda_nm;
+    float cos_theta;
+    float thickness_nm;
+    float n_film;
+    float n_sub;
+} lambda_film_query;
+
+/* Exact FP32 transfer matrix: out is [n][4] = (R_s, R_p, T_s, T_p). */
+lambda_status lambda_thinfilm_exact(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, float *out);
+
+/* FP64 transfer matrix (the training labeller and error audit): out [n][4] doubles. */
+lambda_status lambda_thinfilm_fp64(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, double *out);
+
+/* Surrogate MLP 5->64->64->64->4 (ReLU hidden layers), BF16 weights. */
+#define LAMBDA_MLP_IN 5
+#define LAMBDA_MLP_HIDDEN 64
+#define LAMBDA_MLP_OUT 4
+#define LAMBDA_MLP_PARAMS (5 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 * 4 + 4) /* 8964 */
+
+/* Trained range of the surrogate (queries outside it use the exact path). */
+typedef struct lambda_film_range {
+    float lambda_nm[2];
+    float cos_theta[2];
+    float thickness_nm[2];
+    float n_film[2];
+    float n_sub[2];
+} lambda_film_range;
+
+typedef struct lambda_train_desc {
+    int64_t samples;        /* training set size, labelled by the FP64 transfer matrix (2^24) */
+    int32_t epochs;
+    int32_t batch;          /* minibatch rows */
+    float learning_rate;    /* Adam step size */
+    uint64_t seed;
+    lambda_film_range range;
+} lambda_train_desc;
+
+typedef struct lambda_train_report {
+    double train_ms;
+    double label_ms;
+    float final_loss;       /* mean squared error over the last epoch */
+    float max_abs_error;    /* max |surrogate - fp64| over a held-out audit set */
+    float mean_abs_error;
+    int32_t audit_samples;
+} lambda_train_report;
+
+/* Trains the surrogate on the GPU with the library's forward/backward kernels and
+ * installs it on the context. */
+lambda_status lambda_surrogate_train(lambda_ctx *ctx, const lambda_train_desc *desc,
+                                     lambda_train_report *report);
+
+/* Installs surrogate weights: params is LAMBDA_MLP_PARAMS floats in the order
+ * W1[64][5] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[4][64] b4[4] (row-major,
+ * out x in), with the input normalisation range. */
+lambda_status lambda_surrogate_set(lambda_ctx *ctx, const float *params, const lambda_film_range *range);
+
+/* Reads back the installed weights (LAMBDA_MLP_PARAMS floats) and range. */
+lambda_status lambda_surrogate_get(const lambda_ctx *ctx, float *params, lambda_film_range *range);
+
+/* Surrogate inference on the tensor cores: out [n][4] = (R_s, R_p, T_s, T_p). */
+lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LAMBDA_GPU_H */

@@ -1,0 +1,330 @@
+// Two-level binned-SAH BVH build and light list for the host scene.
+//
+// The split rule is the reference's (src/scene/bvh.h:111-246): 16 centroid bins
+// per axis, SAH cost without a traversal term, a leaf when one item is left, at
+// depth 20, when no split beats the item count, or when no axis has centroid
+// extent >= 1e-4; partition by centroid < plane with std::partition, falling back
+// to the middle when one side is empty. The tree, and with it the reordering of
+// objects and instances, must come out identical, because hit object/instance
+// ids are indices into the reordered arrays.
+//
+// Unlike the reference, every item's bounds and centroid are computed once and
+// cached: the reference re-derives an instance's bounds from all of its objects'
+// eight transformed corners on every visit (instance.h:54-101), which makes the
+// build quadratic for instanced scenes. Caching changes no value.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <vector>
+
+#include "hmath.h"
+#include "scene.h"
+
+namespace lambda_host {
+
+namespace {
+
+V3 load3(const float *p) { return v3(p[0], p[1], p[2]); }
+
+struct ObjectGeom {
+    const lambda_object &o;
+    V3 corner() const { return load3(o.g); }
+    V3 horizontal() const { return load3(o.g + 3); }
+    V3 vertical() const { return load3(o.g + 6); }
+    V3 normal() const { return load3(o.g + 9); }
+    float radius_param() const { return o.g[3]; }
+
+    // object.h:166-172
+    V3 min() const {
+        const V3 e = v3(kEpsilon, kEpsilon, kEpsilon);
+        switch (o.type) {
+            case LAMBDA_OBJECT_SPHERE: {
+                float r = radius_param();
+                return corner() - v3(r, r, r);
+            }
+            case LAMBDA_OBJECT_QUAD: {
+                V3 c = corner(), h = horizontal(), v = vertical();
+                return vmin(c, vmin(c + h, vmin(c + v, c + h + v))) - e;
+            }
+            default: {
+                V3 c = corner(), h = horizontal(), v = vertical();
+                return vmin(c, vmin(c + h, c + v)) - e;
+            }
+        }
+    }
+    V3 max() const {
+        const V3 e = v3(kEpsilon, kEpsilon, kEpsilon);
+        switch (o.type) {
+            case LAMBDA_OBJECT_SPHERE: {
+                float r = radius_param();
+                return corner() + v3(r, r, r);
+            }
+            case LAMBDA_OBJECT_QUAD: {
+                V3 c = corner(), h = horizontal(), v = vertical();
+                return vmax(c, vmax(c + h, vmax(c + v, c + h + v))) + e;
+            }
+            default: {
+                V3 c = corner(), h = horizontal(), v = vertical();
+                return vmax(c, vmax(c + h, c + v)) + e;
+            }
+        }
+    }
+    // object.h:174-176
+    V3 center() const {
+        switch (o.type) {
+            case LAMBDA_OBJECT_SPHERE: return corner();
+            case LAMBDA_OBJECT_QUAD: return corner() + 0.5f * horizontal() + 0.5f * vertical();
+            default: return corner() + (horizontal() + vertical()) / 3.0f;
+        }
+    }
+    // object.h:178-195
+    float bounding_radius() const {
+        switch (o.type) {
+            case LAMBDA_OBJECT_SPHERE: return radius_param();
+            case LAMBDA_OBJECT_QUAD: {
+                float d1 = length_sq(horizontal() + vertical());
+                float d2 = length_sq(horizontal() - vertical());
+                return 0.5f * std::sqrt(std::fmax(d1, d2));
+            }
+            default: {
+                V3 c = center();
+                float d1 = length_sq(corner() - c);
+                float d2 = length_sq(corner() + horizontal() - c);
+                float d3 = length_sq(corner() + vertical() - c);
+                return std::sqrt(std::fmax(d1, std::fmax(d2, d3)));
+            }
+        }
+    }
+    // object.h:197-199
+    float area() const {
+        switch (o.type) {
+            case LAMBDA_OBJECT_SPHERE: return 4.0f * kPi * radius_param() * radius_param();
+            case LAMBDA_OBJECT_QUAD: return length(normal());
+            default: return length(normal()) / 2.0f;
+        }
+    }
+};
+
+struct ItemBounds {
+    V3 lo, hi, centroid;
+};
+
+V3 col0(const lambda_instance &in) { return v3(in.transform[0], in.transform[4], in.transform[8]); }
+
+// Instance::min/max/center (instance.h:54-101): world bounds of the eight corners
+// of every object's box, and the mean of the objects' transformed centres.
+ItemBounds instance_bounds(const HostScene &s, const lambda_instance &in) {
+    ItemBounds b;
+    b.lo = v3(kMax, kMax, kMax);
+    b.hi = v3(-kMax, -kMax, -kMax);
+    V3 sum = v3(0, 0, 0);
+    for (int i = 0; i < in.count; i++) {
+        ObjectGeom g{s.objects[in.object + i]};
+        V3 a = g.min(), c = g.max();
+        const V3 corners[8] = {a, c, v3(a[0], a[1], c[2]), v3(a[0], c[1], a[2]), v3(a[0], c[1], c[2]),
+                               v3(c[0], a[1], a[2]), v3(c[0], a[1], c[2]), v3(c[0], c[1], a[2])};
+        for (const V3 &k : corners) {
+            V3 w = transform(in.transform, k, 1);
+            b.lo = vmin(b.lo, w);
+            b.hi = vmax(b.hi, w);
+        }
+        sum = sum + transform(in.transform, g.center(), 1);
+    }
+    b.centroid = sum / float(in.count);
+    return b;
+}
+
+ItemBounds object_bounds(const lambda_object &o) {
+    ObjectGeom g{o};
+    return ItemBounds{g.min(), g.max(), g.center()};
+}
+
+float half_area(const V3 &e) { return 2 * (e[0] * e[1] + e[0] * e[2] + e[1] * e[2]); }
+
+// One recursive binned-SAH build over order[start, end) (bvh.h:111-246). Returns
+// the node index of the subtree root.
+int build_range(const std::vector<ItemBounds> &items, std::vector<int> &order, int start, int end,
+                std::vector<lambda_bvh_node> &nodes, int depth) {
+    V3 lo = v3(kMax, kMax, kMax), hi = v3(-kMax, -kMax, -kMax);
+    V3 clo = lo, chi = hi;
+    for (int i = start; i < end; i++) {
+        const ItemBounds &b = items[order[i]];
+        lo = vmin(lo, b.lo);
+        hi = vmax(hi, b.hi);
+        clo = vmin(clo, b.centroid);
+        chi = vmax(chi, b.centroid);
+    }
+
+    float best_cost = kMax;
+    int best_axis = 0, best_split = -1;
+    for (int axis = 0; axis < 3; axis++) {
+        const float extent = chi[axis] - clo[axis];
+        if (!(extent >= kEpsilon)) continue;
+        V3 bin_lo[kBinCount], bin_hi[kBinCount];
+        int bin_n[kBinCount];
+        for (int j = 0; j < kBinCount; j++) {
+            bin_lo[j] = v3(kMax, kMax, kMax);
+            bin_hi[j] = v3(-kMax, -kMax, -kMax);
+            bin_n[j] = 0;
+        }
+        for (int j = start; j < end; j++) {
+            const ItemBounds &b = items[order[j]];
+            int bin = int(float(kBinCount) * (b.centroid[axis] - clo[axis]) / extent);
+            bin = std::clamp(bin, 0, kBinCount - 1);
+            bin_lo[bin] = vmin(bin_lo[bin], b.lo);
+            bin_hi[bin] = vmax(bin_hi[bin], b.hi);
+            bin_n[bin]++;
+        }
+        // prefix (left) and suffix (right) sweeps
+        V3 left_lo[kBinCount], left_hi[kBinCount], right_lo[kBinCount], right_hi[kBinCount];
+        int left_n[kBinCount], right_n[kBinCount];
+        V3 rlo = v3(kMax, kMax, kMax), rhi = v3(-kMax, -kMax, -kMax);
+        int rn = 0;
+        for (int j = 0; j < kBinCount; j++) {
+            rlo = vmin(rlo, bin_lo[j]);
+            rhi = vmax(rhi, bin_hi[j]);
+            rn += bin_n[j];
+            left_lo[j] = rlo;
+            left_hi[j] = rhi;
+            left_n[j] = rn;
+        }
+        rlo = v3(kMax, kMax, kMax);
+        rhi = v3(-kMax, -kMax, -kMax);
+        rn = 0;
+        for (int j = kBinCount - 1; j >= 0; j--) {
+            rlo = vmin(rlo, bin_lo[j]);
+            rhi = vmax(rhi, bin_hi[j]);
+            rn += bin_n[j];
+            right_lo[j] = rlo;
+            right_hi[j] = rhi;
+            right_n[j] = rn;
+        }
+        const float total_area = half_area(hi - lo);
+        for (int j = 0; j < kBinCount - 1; j++) {
+            if (left_n[j] == 0 || right_n[j + 1] == 0) continue;
+            float la = half_area(left_hi[j] - left_lo[j]);
+            float ra = half_area(right_hi[j + 1] - right_lo[j + 1]);
+            float cost = la / total_area * float(left_n[j]) + ra / total_area * float(right_n[j + 1]);
+            if (cost < best_cost) {
+                best_cost = cost;
+                best_axis = axis;
+                best_split = j;
+            }
+        }
+    }
+
+    if (end - start == 1 || depth >= kMaxDepth || best_cost >= float(end - start) || best_split == -1) {
+        lambda_bvh_node leaf{};
+        for (int k = 0; k < 3; k++) {
+            leaf.min[k] = lo[k];
+            leaf.max[k] = hi[k];
+        }
+        leaf.index = start;
+        leaf.count = end - start;
+        nodes.push_back(leaf);
+        return int(nodes.size()) - 1;
+    }
+
+    const float plane = clo[best_axis] + float(best_split + 1) * (chi[best_axis] - clo[best_axis]) / float(kBinCount);
+    auto split = std::partition(order.begin() + start, order.begin() + end,
+                                [&](int i) { return items[i].centroid[best_axis] < plane; });
+    int mid = int(split - order.begin());
+    if (mid == start || mid == end) mid = start + (end - start) / 2;
+
+    const int self = int(nodes.size());
+    lambda_bvh_node inner{};
+    for (int k = 0; k < 3; k++) {
+        inner.min[k] = lo[k];
+        inner.max[k] = hi[k];
+    }
+    inner.index = -1;
+    inner.count = 0;
+    nodes.push_back(inner);
+    build_range(items, order, start, mid, nodes, depth + 1);
+    const int right = build_range(items, order, mid, end, nodes, depth + 1);
+    nodes[self].index = right;
+    return self;
+}
+
+}  // namespace
+
+void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
+    s.nodes.clear();
+    if (s.objects.empty()) return;
+    s.nodes.reserve(2 * s.objects.size());
+
+    // TLAS over instances
+    std::vector<ItemBounds> inst_bounds(s.instances.size());
+    for (size_t i = 0; i < s.instances.size(); i++) inst_bounds[i] = instance_bounds(s, s.instances[i]);
+    std::vector<int> order(s.instances.size());
+    std::iota(order.begin(), order.end(), 0);
+    build_range(inst_bounds, order, 0, int(s.instances.size()), s.nodes, 1);
+    {
+        std::vector<lambda_instance> reordered;
+        reordered.reserve(s.instances.size());
+        for (int i : order) reordered.push_back(s.instances[i]);
+        s.instances.swap(reordered);
+    }
+
+    // one BLAS per object group, over a shared object order
+    std::vector<ItemBounds> obj_bounds(s.objects.size());
+    for (size_t i = 0; i < s.objects.size(); i++) obj_bounds[i] = object_bounds(s.objects[i]);
+    std::vector<int> obj_order(s.objects.size());
+    std::iota(obj_order.begin(), obj_order.end(), 0);
+    std::map<int, int> root_of_group;
+    for (size_t g = 0; g + 1 < group_offsets.size(); g++) {
+        root_of_group[group_offsets[g]] = int(s.nodes.size());
+        build_range(obj_bounds, obj_order, group_offsets[g], group_offsets[g + 1], s.nodes, 1);
+    }
+    for (auto &in : s.instances) in.node = root_of_group.at(in.object);
+    {
+        std::vector<lambda_object> reordered;
+        reordered.reserve(s.objects.size());
+        for (int i : obj_order) reordered.push_back(s.objects[i]);
+        s.objects.swap(reordered);
+    }
+}
+
+void build_lights(HostScene &s) {
+    V3 scene_center = v3(0, 0, 0);
+    float scene_radius = 0;
+    for (int i = 0; i < int(s.instances.size()); i++) {
+        const lambda_instance &in = s.instances[i];
+        const float scale = length(col0(in));
+        const float scale_sq = length_sq(col0(in));
+        for (int j = 0; j < in.count; j++) {
+            const int object_index = in.object + j;
+            ObjectGeom g{s.objects[object_index]};
+            const V3 object_center = transform(in.transform, g.center(), 1);
+            const float object_radius = g.bounding_radius() * scale;
+            const V3 to_object = object_center - scene_center;
+            const float distance = length(to_object);
+            if (distance + scene_radius <= object_radius) {
+                scene_center = object_center;
+                scene_radius = object_radius;
+            } else if (distance + object_radius > scene_radius) {
+                const float grown = 0.5f * (distance + scene_radius + object_radius);
+                scene_center = scene_center + (grown - scene_radius) * to_object / distance;
+                scene_radius = grown;
+            }
+            const int material = in.material >= 0 ? in.material : s.objects[object_index].material;
+            const lambda_material &m = s.materials[material];
+            if (m.type == LAMBDA_MATERIAL_EMISSIVE) {
+                s.light_instances.push_back(i);
+                s.light_objects.push_back(object_index);
+                const float power = g.area() * scale_sq * spectrum_texture_average(s, m.p[0]);
+                s.light_powers.push_back(power);
+                s.total_light_power += power;
+            }
+        }
+    }
+    s.light_instances.push_back(-1);
+    s.light_objects.push_back(-1);
+    const float background_power =
+        4.0f * kPi * scene_radius * scene_radius * spectrum_texture_average(s, s.background_texture);
+    s.light_powers.push_back(background_power);
+    s.total_light_power += background_power;
+}
+
+}  // namespace lambda_host

@@ -1,0 +1,633 @@
+// Device scene: layouts in HBM and the functions the render loop calls on them.
+//
+// Layouts (all read-only during a render; uploaded once per scene):
+//   nodes      float4[2n]   (min.xyz, index)  (max.xyz, count); index/count are int bits
+//   prims      float4[4m]   p0 = (corner or centre .xyz, type), p1 = (horizontal.xyz or
+//                           radius, material), p2 = (vertical.xyz, 0), p3 = (normal.xyz, 0)
+//   tri_attr   float4[4m]   (n0.xyz, n1.x) (n1.yz, n2.xy) (n2.z, u0, u1, u2) (v0, v1, v2, 0)
+//   instances  float4[9k]   (object, count, node, material as int bits), M rows, M^-1 rows
+//   spectra    float[s][471] plus a per-spectrum "all bins equal" flag
+//   cspectra   double2[c][471] (complex refractive indices)
+// Functions follow the reference's object.h, instance.h, scene.h, texture.h,
+// background.h and material.h, in its operand order (see dmath.cuh).
+#pragma once
+
+#include <cstdint>
+
+#include "dmath.cuh"
+#include "dtypes.cuh"
+
+namespace lambda_dev {
+
+
+// ---------------------------------------------------------------------------
+// Spectra (DenseSpectrum::operator(), spectrum.h:176-188): linear interpolation
+// on the 1 nm grid with the index held in double, result rounded to float.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float spectrum_at(const DeviceScene &s, int k, float lambda) {
+    const float *d = s.spectra + size_t(k) * kCieBins;
+    if (s.spectrum_flat[k]) return d[0];  // all bins equal: interpolation returns the bin value exactly
+    const double index = double(lambda - 360.0f);
+    const int lo = int(index);
+    if (lo == kCieBins - 1) return d[lo];
+    const int hi = lo + 1;
+    return float((double(hi) - index) * double(d[lo]) + (index - double(lo)) * double(d[hi]));
+}
+
+__device__ __forceinline__ double2 cspectrum_at(const DeviceScene &s, int k, float lambda) {
+    const double2 *d = s.cspectra + size_t(k) * kCieBins;
+    if (s.cspectrum_flat[k]) return d[0];
+    const double index = double(lambda - 360.0f);
+    const int lo = int(index);
+    if (lo == kCieBins - 1) return d[lo];
+    const int hi = lo + 1;
+    const double a = double(hi) - index, b = index - double(lo);
+    return make_double2(a * d[lo].x + b * d[hi].x, a * d[lo].y + b * d[hi].y);
+}
+
+// ---------------------------------------------------------------------------
+// Noise (utils.h:97-171)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int perm_at(const DeviceScene &s, int i) { return s.perm[i & 255]; }
+
+// t^5-style fade t^3 (t (6t - 15) + 10). The reference takes t^3 from powf; the
+// cube is formed exactly in double (t^2 has 48 significant bits) and rounded once.
+__device__ __forceinline__ float fade(float t) {
+    const double t2 = double(t) * double(t);
+    const float cube = float(t2 * double(t));
+    return cube * (t * (6 * t - 15) + 10);
+}
+
+__device__ __forceinline__ float grad(int hash, float x, float y, float z) {
+    switch (hash % 12) {
+        case 0: return x + y;
+        case 1: return -x + y;
+        case 2: return x - y;
+        case 3: return -x - y;
+        case 4: return x + z;
+        case 5: return -x + z;
+        case 6: return x - z;
+        case 7: return -x - z;
+        case 8: return y + z;
+        case 9: return -y + z;
+        case 10: return y - z;
+        case 11: return -y - z;
+        default: return 0;
+    }
+}
+
+__device__ __forceinline__ float lerp(float a, float b, float x) { return a + x * (b - a); }
+
+// Improved noise mapped to [0, 1] (utils.h:123-148).
+__device__ inline float perlin_noise(const DeviceScene &s, f3 p) {
+    const float fx = floorf(p.x), fy = floorf(p.y), fz = floorf(p.z);
+    const int i = int(fx) & 255, j = int(fy) & 255, k = int(fz) & 255;
+    const float tx = p.x - fx, ty = p.y - fy, tz = p.z - fz;
+    const float u = fade(tx), v = fade(ty), w = fade(tz);
+    const int pi0 = perm_at(s, i), pi1 = perm_at(s, i + 1);
+    const int a0 = perm_at(s, pi0 + j), a1 = perm_at(s, pi0 + j + 1);
+    const int b0 = perm_at(s, pi1 + j), b1 = perm_at(s, pi1 + j + 1);
+    const int aaa = perm_at(s, a0 + k), aba = perm_at(s, a1 + k), aab = perm_at(s, a0 + k + 1), abb = perm_at(s, a1 + k + 1);
+    const int baa = perm_at(s, b0 + k), bba = perm_at(s, b1 + k), bab = perm_at(s, b0 + k + 1), bbb = perm_at(s, b1 + k + 1);
+    float x1 = lerp(grad(aaa, tx, ty, tz), grad(baa, tx - 1, ty, tz), u);
+    float x2 = lerp(grad(aba, tx, ty - 1, tz), grad(bba, tx - 1, ty - 1, tz), u);
+    const float y1 = lerp(x1, x2, v);
+    x1 = lerp(grad(aab, tx, ty, tz - 1), grad(bab, tx - 1, ty, tz - 1), u);
+    x2 = lerp(grad(abb, tx, ty - 1, tz - 1), grad(bbb, tx - 1, ty - 1, tz - 1), u);
+    const float y2 = lerp(x1, x2, v);
+    return (lerp(y1, y2, w) + 1) / 2;
+}
+
+__device__ __forceinline__ float fract(float x) { return x - floorf(x); }
+
+// Feature offset of one Worley lattice cell: fract(sin(cell . k) * 43758.5453)
+// per axis (utils.h:165). Cells inside the scene's table were evaluated on the host
+// with the C library's sinf at upload; others are computed here, with the sine
+// taken in double and rounded to float.
+__device__ __forceinline__ f3 worley_feature(const DeviceScene &s, int cx, int cy, int cz) {
+    const int ix = cx - s.worley_lo.x, iy = cy - s.worley_lo.y, iz = cz - s.worley_lo.z;
+    if (unsigned(ix) < unsigned(s.worley_dim.x) && unsigned(iy) < unsigned(s.worley_dim.y) &&
+        unsigned(iz) < unsigned(s.worley_dim.z)) {
+        const float4 h = __ldg(&s.worley_cells[(size_t(iz) * s.worley_dim.y + iy) * s.worley_dim.x + ix]);
+        return mk(h.x, h.y, h.z);
+    }
+    const f3 c = mk(float(cx), float(cy), float(cz));
+    const float a = dot(c, mk(127.1f, 311.7f, 74.7f));
+    const float b = dot(c, mk(269.5f, 183.3f, 246.1f));
+    const float d = dot(c, mk(113.5f, 271.9f, 124.6f));
+    return mk(fract(float(sin(double(a))) * 43758.5453f), fract(float(sin(double(b))) * 43758.5453f),
+              fract(float(sin(double(d))) * 43758.5453f));
+}
+
+// F1 Worley distance over the 27 neighbouring cells (utils.h:154-171).
+__device__ inline float worley_noise(const DeviceScene &s, f3 p) {
+    const int xi = int(floorf(p.x)), yi = int(floorf(p.y)), zi = int(floorf(p.z));
+    float distance = 9999;
+    for (int xo = -1; xo <= 1; xo++)
+        for (int yo = -1; yo <= 1; yo++)
+            for (int zo = -1; zo <= 1; zo++) {
+                const f3 cell = mk(float(xi + xo), float(yi + yo), float(zi + zo));
+                const f3 feature = worley_feature(s, xi + xo, yi + yo, zi + zo) + cell;
+                distance = fminf(distance, length(p - feature));
+            }
+    return distance;
+}
+
+// ---------------------------------------------------------------------------
+// Textures (texture.h)
+// ---------------------------------------------------------------------------
+
+struct ShadePoint {
+    f3 point;
+    float u, v;
+};
+
+__device__ __forceinline__ float scalar_texture(const DeviceScene &s, int t, f3 p) {
+    const float4 x = __ldg(&s.scalar_tex[t]);
+    const int type = __float_as_int(x.x);
+    if (type == 0) return x.y;                                            // constant
+    if (type == 1) return x.y + (x.z - x.y) * perlin_noise(s, p * x.w);   // perlin
+    return x.y + (x.z - x.y) * worley_noise(s, p * x.w);                  // worley
+}
+
+__device__ __forceinline__ float spectrum_texture(const DeviceScene &s, int t, const ShadePoint &sp, float lambda) {
+    const int4 x = __ldg(&s.spectrum_tex[t]);
+    if (x.x == 0) return spectrum_at(s, x.y, lambda);
+    if (x.x == 1) {
+        const float scale = __int_as_float(x.w);
+        const int cx = int(floorf(sp.u / scale));
+        const int cy = int(floorf(sp.v / scale));
+        return (cx + cy) % 2 == 0 ? spectrum_at(s, x.y, lambda) : spectrum_at(s, x.z, lambda);
+    }
+    return scalar_texture(s, x.y, sp.point);
+}
+
+// A spectrum texture at the four hero wavelengths; a texture that does not
+// depend on the wavelength (scalar) is evaluated once.
+__device__ __forceinline__ s4 spectrum_texture4(const DeviceScene &s, int t, const ShadePoint &sp, const s4 &lam) {
+    const int4 x = __ldg(&s.spectrum_tex[t]);
+    if (x.x == 2) return s4_fill(scalar_texture(s, x.y, sp.point));
+    s4 r;
+    for (int k = 0; k < kHero; k++) r.v[k] = spectrum_texture(s, t, sp, lam.v[k]);
+    return r;
+}
+
+// Background::evaluate (background.h:81-95): equirectangular lookup of direction d.
+__device__ __forceinline__ s4 background_eval(const DeviceScene &s, f3 d, const s4 &lam) {
+    ShadePoint sp;
+    sp.point = d;
+    sp.u = (atan2f(d.z, d.x) + kPi) / (2 * kPi);
+    sp.v = acosf(d.y) / kPi;
+    return spectrum_texture4(s, s.background_texture, sp, lam);
+}
+
+// ---------------------------------------------------------------------------
+// Geometry: BVH node slab test and primitive intersection (bvh.h:30-52,
+// object.h:301-400). Traversal only needs t; attributes of the winning
+// primitive are computed once at the end with the same arithmetic.
+// ---------------------------------------------------------------------------
+
+struct Ray3 {
+    f3 o, d, inv;
+};
+
+__device__ __forceinline__ Ray3 make_ray(f3 o, f3 d) { return Ray3{o, d, mk(1 / d.x, 1 / d.y, 1 / d.z)}; }
+
+__device__ __forceinline__ bool slab(float4 lo, float4 hi, const Ray3 &r, float &t_entry) {
+    float t1 = 0, t2 = kMax;
+    {
+        float a = (lo.x - r.o.x) * r.inv.x, b = (hi.x - r.o.x) * r.inv.x;
+        if (r.inv.x < 0) { const float t = a; a = b; b = t; }
+        t1 = fmaxf(a, t1);
+        t2 = fminf(b, t2);
+    }
+    {
+        float a = (lo.y - r.o.y) * r.inv.y, b = (hi.y - r.o.y) * r.inv.y;
+        if (r.inv.y < 0) { const float t = a; a = b; b = t; }
+        t1 = fmaxf(a, t1);
+        t2 = fminf(b, t2);
+    }
+    {
+        float a = (lo.z - r.o.z) * r.inv.z, b = (hi.z - r.o.z) * r.inv.z;
+        if (r.inv.z < 0) { const float t = a; a = b; b = t; }
+        t1 = fmaxf(a, t1);
+        t2 = fminf(b, t2);
+    }
+    t_entry = t1;
+    return t1 <= t2 && t2 >= 0;
+}
+
+struct Prim {
+    float4 p0, p1, p2, p3;
+};
+
+__device__ __forceinline__ Prim load_prim(const DeviceScene &s, int i) {
+    const float4 *p = s.prims + 4 * size_t(i);
+    return Prim{__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3)};
+}
+
+__device__ __forceinline__ int prim_type(const Prim &p) { return __float_as_int(p.p0.w); }
+__device__ __forceinline__ int prim_material(const Prim &p) { return __float_as_int(p.p1.w); }
+
+// t of the first intersection beyond EPSILON that is closer than `best`, else -1.
+__device__ __forceinline__ float intersect_t(const Prim &p, const Ray3 &r, float best) {
+    const int type = prim_type(p);
+    if (type == 0) {  // sphere
+        const f3 c = mk(p.p0.x, p.p0.y, p.p0.z);
+        const float rad = p.p1.x;
+        const f3 oc = r.o - c;
+        const float a = length_sq(r.d);
+        const float b = 2 * dot(r.d, oc);
+        const float cc = dot(oc, oc) - rad * rad;
+        float disc = b * b - 4 * a * cc;
+        if (disc < 0) return -1;
+        disc = sqrtf(disc);
+        const float t1 = (-b - disc) / (2 * a);
+        const float t2 = (-b + disc) / (2 * a);
+        if (t1 < kEps && t2 < kEps) return -1;
+        const float t = (t1 < kEps) ? t2 : t1;
+        return t >= best ? -1 : t;
+    }
+    const f3 corner = mk(p.p0.x, p.p0.y, p.p0.z);
+    const f3 h = mk(p.p1.x, p.p1.y, p.p1.z);
+    const f3 v = mk(p.p2.x, p.p2.y, p.p2.z);
+    if (type == 1) {  // quad
+        const f3 nn = mk(p.p3.x, p.p3.y, p.p3.z);
+        const f3 n = normalize(nn);
+        const float den = dot(n, r.d);
+        if (fabsf(den) < kEps) return -1;
+        const float t = dot(n, corner - r.o) / den;
+        if (t < kEps || t >= best) return -1;
+        const f3 point = r.o + t * r.d;
+        const f3 proj = point - corner;
+        const float nsq = length_sq(nn);
+        const float alpha = dot(nn, cross(proj, v)) / nsq;
+        const float beta = dot(nn, cross(h, proj)) / nsq;
+        if (alpha < 0 || alpha > 1 || beta < 0 || beta > 1) return -1;
+        return t;
+    }
+    // triangle
+    const f3 rcv = cross(r.d, v);
+    const float det = dot(h, rcv);
+    if (fabsf(det) < kEpsSq) return -1;
+    const float inv = 1 / det;
+    const f3 oc = r.o - corner;
+    const float alpha = inv * dot(oc, rcv);
+    if (alpha < 0 || alpha > 1) return -1;
+    const f3 och = cross(oc, h);
+    const float beta = inv * dot(r.d, och);
+    if (beta < 0 || alpha + beta > 1) return -1;
+    const float t = inv * dot(v, och);
+    if (t < kEps || t >= best) return -1;
+    return t;
+}
+
+struct Hit {
+    float t;
+    int instance;
+    int object;
+    f3 point;
+    f3 normal;
+    float u, v;
+    bool front;
+};
+
+struct InstanceRef {
+    const float4 *base;
+    __device__ __forceinline__ int4 header() const {
+        const float4 h = __ldg(base);
+        return make_int4(__float_as_int(h.x), __float_as_int(h.y), __float_as_int(h.z), __float_as_int(h.w));
+    }
+    __device__ __forceinline__ void load_m(float *m, int which) const {
+        const float4 *p = base + 1 + 4 * which;
+        for (int r = 0; r < 4; r++) {
+            const float4 q = __ldg(p + r);
+            m[4 * r] = q.x;
+            m[4 * r + 1] = q.y;
+            m[4 * r + 2] = q.z;
+            m[4 * r + 3] = q.w;
+        }
+    }
+};
+
+__device__ __forceinline__ InstanceRef instance_ref(const DeviceScene &s, int i) { return InstanceRef{s.instances + 9 * size_t(i)}; }
+
+// Full attributes of a hit on primitive p in instance space (object.h:301-400).
+__device__ __forceinline__ void prim_attributes(const DeviceScene &s, int obj, const Prim &p, f3 o, f3 d, float t, Hit &h) {
+    const int type = prim_type(p);
+    h.t = t;
+    h.point = o + t * d;
+    if (type == 0) {
+        const f3 c = mk(p.p0.x, p.p0.y, p.p0.z);
+        h.normal = normalize(h.point - c);
+        h.u = (atan2f(-h.normal.z, h.normal.x) + kPi) / (2 * kPi);
+        h.v = acosf(-h.normal.y) / kPi;
+        h.front = dot(d, h.normal) < 0;
+        if (!h.front) h.normal = h.normal * -1.0f;
+        return;
+    }
+    const f3 corner = mk(p.p0.x, p.p0.y, p.p0.z);
+    const f3 hz = mk(p.p1.x, p.p1.y, p.p1.z);
+    const f3 v = mk(p.p2.x, p.p2.y, p.p2.z);
+    const f3 nn = mk(p.p3.x, p.p3.y, p.p3.z);
+    if (type == 1) {
+        const f3 proj = h.point - corner;
+        const float nsq = length_sq(nn);
+        h.u = dot(nn, cross(proj, v)) / nsq;
+        h.v = dot(nn, cross(hz, proj)) / nsq;
+        h.normal = normalize(nn);
+        h.front = dot(d, h.normal) < 0;
+        if (!h.front) h.normal = h.normal * -1.0f;
+        return;
+    }
+    const f3 rcv = cross(d, v);
+    const float det = dot(hz, rcv);
+    const float inv = 1 / det;
+    const f3 oc = o - corner;
+    const float alpha = inv * dot(oc, rcv);
+    const f3 och = cross(oc, hz);
+    const float beta = inv * dot(d, och);
+    const float4 *ta = s.tri_attr + 4 * size_t(obj);
+    const float4 a0 = __ldg(ta), a1 = __ldg(ta + 1), a2 = __ldg(ta + 2), a3 = __ldg(ta + 3);
+    const f3 n0 = mk(a0.x, a0.y, a0.z), n1 = mk(a0.w, a1.x, a1.y), n2 = mk(a1.z, a1.w, a2.x);
+    const float w0 = 1 - alpha - beta;
+    h.normal = normalize(w0 * n0 + alpha * n1 + beta * n2);
+    h.u = w0 * a2.y + alpha * a2.z + beta * a2.w;
+    h.v = w0 * a3.x + alpha * a3.y + beta * a3.z;
+    h.front = dot(d, nn) < 0;
+    if (!h.front) h.normal = h.normal * -1.0f;
+}
+
+// Scene::hit in closest-hit mode (scene.h:51-124): two-level depth-first
+// traversal with 20-entry stacks, right child popped first, a TLAS leaf tests
+// only its first instance (scene.h:80), candidates accepted when t < best.
+// Returns false on a miss. `overflow` is set if a stack would overflow.
+__device__ inline bool closest_hit(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow) {
+    const Ray3 wr = make_ray(o, d);
+    float best = kMax;
+    int best_obj = -1, best_inst = -1;
+    int stack[kStackDepth];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int cur = stack[--sp];
+        const float4 lo = __ldg(&s.nodes[2 * cur]), hi = __ldg(&s.nodes[2 * cur + 1]);
+        float te;
+        if (!slab(lo, hi, wr, te) || te > best) continue;
+        const int count = __float_as_int(hi.w);
+        if (count > 0) {
+            const int inst = __float_as_int(lo.w);
+            const InstanceRef ir = instance_ref(s, inst);
+            const int4 hd = ir.header();
+            float mi[16];
+            ir.load_m(mi, 1);
+            const Ray3 lr = make_ray(xform(mi, o, 1), xform(mi, d, 0));
+            int sub[kStackDepth];
+            int ssp = 0;
+            sub[ssp++] = hd.z;
+            while (ssp > 0) {
+                const int sc = sub[--ssp];
+                const float4 l2 = __ldg(&s.nodes[2 * sc]), h2 = __ldg(&s.nodes[2 * sc + 1]);
+                if (!slab(l2, h2, lr, te) || te > best) continue;
+                const int c2 = __float_as_int(h2.w);
+                if (c2 > 0) {
+                    const int first = __float_as_int(l2.w);
+                    for (int k = 0; k < c2; k++) {
+                        const float t = intersect_t(load_prim(s, first + k), lr, best);
+                        if (t >= 0) {
+                            best = t;
+                            best_obj = first + k;
+                            best_inst = inst;
+                        }
+                    }
+                } else {
+                    if (ssp + 2 > kStackDepth) {
+                        overflow = true;
+                        break;
+                    }
+                    sub[ssp++] = sc + 1;
+                    sub[ssp++] = __float_as_int(l2.w);
+                }
+            }
+        } else {
+            if (sp + 2 > kStackDepth) {
+                overflow = true;
+                break;
+            }
+            stack[sp++] = cur + 1;
+            stack[sp++] = __float_as_int(lo.w);
+        }
+    }
+    if (best_obj < 0) {
+        h.t = kMax;
+        h.instance = -1;
+        h.object = -1;
+        return false;
+    }
+    const InstanceRef ir = instance_ref(s, best_inst);
+    float m[16];
+    ir.load_m(m, 1);
+    const f3 lo_ = xform(m, o, 1), ld = xform(m, d, 0);
+    prim_attributes(s, best_obj, load_prim(s, best_obj), lo_, ld, best, h);
+    h.instance = best_inst;
+    h.object = best_obj;
+    // instance space -> world (instance.h:42, :48); m still holds M^-1
+    h.normal = normalize(xform_t(m, h.normal, 0));
+    ir.load_m(m, 0);
+    h.point = xform(m, h.point, 1);
+    return true;
+}
+
+// Scene::hit in shadow mode (scene.h:51-124 with occludedInstance/Object): for a
+// scene light, first intersect the light primitive itself (a miss counts as
+// occluded), then any primitive other than the light closer than it occludes.
+// For the background light (-1, -1), any hit occludes. On a visible light,
+// `light` holds the light's hit record for its emission lookup.
+__device__ inline bool occluded(const DeviceScene &s, f3 o, f3 d, int light_inst, int light_obj, Hit &light, bool &overflow) {
+    const Ray3 wr = make_ray(o, d);
+    float best = kMax;
+    if (light_inst != -1) {
+        const InstanceRef ir = instance_ref(s, light_inst);
+        float m[16];
+        ir.load_m(m, 1);
+        const f3 lo = xform(m, o, 1), ld = xform(m, d, 0);
+        const Prim p = load_prim(s, light_obj);
+        const float t = intersect_t(p, make_ray(lo, ld), kMax);
+        if (t < 0) return true;
+        prim_attributes(s, light_obj, p, lo, ld, t, light);
+        light.instance = light_inst;
+        light.object = light_obj;
+        light.normal = normalize(xform_t(m, light.normal, 0));
+        ir.load_m(m, 0);
+        light.point = xform(m, light.point, 1);
+        best = t;
+    }
+    int stack[kStackDepth];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int cur = stack[--sp];
+        const float4 lo = __ldg(&s.nodes[2 * cur]), hi = __ldg(&s.nodes[2 * cur + 1]);
+        float te;
+        if (!slab(lo, hi, wr, te) || te > best) continue;
+        const int count = __float_as_int(hi.w);
+        if (count > 0) {
+            const int inst = __float_as_int(lo.w);
+            const InstanceRef ir = instance_ref(s, inst);
+            const int4 hd = ir.header();
+            float mi[16];
+            ir.load_m(mi, 1);
+            const Ray3 lr = make_ray(xform(mi, o, 1), xform(mi, d, 0));
+            int sub[kStackDepth];
+            int ssp = 0;
+            sub[ssp++] = hd.z;
+            while (ssp > 0) {
+                const int sc = sub[--ssp];
+                const float4 l2 = __ldg(&s.nodes[2 * sc]), h2 = __ldg(&s.nodes[2 * sc + 1]);
+                if (!slab(l2, h2, lr, te) || te > best) continue;
+                const int c2 = __float_as_int(h2.w);
+                if (c2 > 0) {
+                    const int first = __float_as_int(l2.w);
+                    for (int k = 0; k < c2; k++) {
+                        if (light_inst != -1 && inst == light_inst && first + k == light_obj) continue;
+                        if (intersect_t(load_prim(s, first + k), lr, best) >= 0) return true;
+                    }
+                } else {
+                    if (ssp + 2 > kStackDepth) {
+                        overflow = true;
+                        return true;
+                    }
+                    sub[ssp++] = sc + 1;
+                    sub[ssp++] = __float_as_int(l2.w);
+                }
+            }
+        } else {
+            if (sp + 2 > kStackDepth) {
+                overflow = true;
+                return true;
+            }
+            stack[sp++] = cur + 1;
+            stack[sp++] = __float_as_int(lo.w);
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Lights (object.h:201-299, instance.h:105-111, background.h:77-79)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float prim_pdf(const Prim &p, f3 point, f3 dir) {
+    const int type = prim_type(p);
+    if (type == 0) {
+        const f3 c = mk(p.p0.x, p.p0.y, p.p0.z);
+        const float rad = p.p1.x;
+        const f3 oc = c - point;
+        const float dsq = length_sq(oc);
+        const float rsq = rad * rad;
+        if (dsq <= rsq) return 1 / (4 * kPi);
+        const float cos_max = sqrtf(1 - rsq / dsq);
+        const float cos_t = dot(normalize(oc), dir);
+        if (cos_t < cos_max) return 0;
+        return 1 / (2 * kPi * (1 - cos_max));
+    }
+    const f3 corner = mk(p.p0.x, p.p0.y, p.p0.z);
+    const f3 h = mk(p.p1.x, p.p1.y, p.p1.z);
+    const f3 v = mk(p.p2.x, p.p2.y, p.p2.z);
+    const f3 nn = mk(p.p3.x, p.p3.y, p.p3.z);
+    if (type == 1) {
+        const float cos_t = dot(normalize(nn), dir);
+        if (fabsf(cos_t) < kEps) return 0;
+        const float t = dot(corner - point, normalize(nn)) / cos_t;
+        if (t < kEps) return 0;
+        const f3 local = (point + dir * t) - corner;
+        const float u = dot(nn, cross(local, v)) / length_sq(nn);
+        const float w = dot(nn, cross(h, local)) / length_sq(nn);
+        if (u < 0 || u > 1 || w < 0 || w > 1) return 0;
+        return t * t / (fabsf(cos_t) * length(nn));
+    }
+    const f3 rcv = cross(dir, v);
+    const float det = dot(h, rcv);
+    if (fabsf(det) < kEpsSq) return 0;
+    const float inv = 1 / det;
+    const f3 oc = point - corner;
+    const float alpha = inv * dot(oc, rcv);
+    if (alpha < 0 || alpha > 1) return 0;
+    const f3 och = cross(oc, h);
+    const float beta = inv * dot(dir, och);
+    if (beta < 0 || alpha + beta > 1) return 0;
+    const float t = inv * dot(v, och);
+    if (t < kEps) return 0;
+    const float area = length(nn) * 0.5f;
+    const float cos_t = dot(normalize(nn), dir);
+    return t * t / (fabsf(cos_t) * area);
+}
+
+__device__ __forceinline__ f3 prim_sample(const Prim &p, f3 point, Rng &rng) {
+    const int type = prim_type(p);
+    if (type == 0) {
+        const f3 c = mk(p.p0.x, p.p0.y, p.p0.z);
+        const float rad = p.p1.x;
+        const f3 oc = c - point;
+        const float dsq = length_sq(oc);
+        const float rsq = rad * rad;
+        if (dsq <= rsq) return random_unit_vector(rng);
+        const float cos_max = sqrtf(1 - rsq / dsq);
+        return random_in_cone(oc, cos_max, rng);
+    }
+    const f3 corner = mk(p.p0.x, p.p0.y, p.p0.z);
+    const f3 h = mk(p.p1.x, p.p1.y, p.p1.z);
+    const f3 v = mk(p.p2.x, p.p2.y, p.p2.z);
+    float u = rng.next();
+    float w = rng.next();
+    if (type == 2 && u + w > 1) {
+        u = 1 - u;
+        w = 1 - w;
+    }
+    const f3 q = corner + h * u + v * w;
+    return normalize(q - point);
+}
+
+// Instance::area (instance.h:107): primitive area times |column 0 of M|^2.
+__device__ __forceinline__ float prim_area(const Prim &p) {
+    const int type = prim_type(p);
+    if (type == 0) return 4 * kPi * p.p1.x * p.p1.x;
+    const float l = length(mk(p.p3.x, p.p3.y, p.p3.z));
+    return type == 1 ? l : l / 2;
+}
+
+// ---------------------------------------------------------------------------
+// Materials (material.h)
+// ---------------------------------------------------------------------------
+
+enum : int { kLambertian = 0, kMirror = 1, kDielectric = 2, kEmissive = 3, kThinFilm = 4 };
+
+// CIE 1931 lookup with linear interpolation (utils.h:195-203) and the
+// spectrum -> XYZ -> linear sRGB conversion (utils.h:212-231).
+__device__ __forceinline__ float xyz31(const DeviceScene &s, float lambda, int i) {
+    const int lo = int(lambda);
+    if (lo == 830) return s.cie[(lo - 360) * 3 + i];
+    const int hi = lo + 1;
+    return (float(hi) - lambda) * s.cie[(lo - 360) * 3 + i] + (lambda - float(lo)) * s.cie[(hi - 360) * 3 + i];
+}
+
+__device__ __forceinline__ f3 spectrum_to_rgb(const DeviceScene &s, const s4 &L, const s4 &lam, float range) {
+    float x = 0, y = 0, z = 0;
+    const float w = range / kHero;
+    for (int i = 0; i < kHero; i++) {
+        const float l = lam.v[i];
+        const float r = L.v[i];
+        x += xyz31(s, l, 0) * r * w;
+        y += xyz31(s, l, 1) * r * w;
+        z += xyz31(s, l, 2) * r * w;
+    }
+    x /= 106.856895f;
+    y /= 106.856895f;
+    z /= 106.856895f;
+    return mk(x * 3.2406255f - y * 1.5372080f - z * 0.4986286f, -x * 0.9689307f + y * 1.8757561f + z * 0.0415175f,
+              x * 0.0557101f - y * 0.2040211f + z * 1.0569959f);
+}
+
+}  // namespace lambda_dev

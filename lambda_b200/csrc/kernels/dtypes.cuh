@@ -1,0 +1,75 @@
+// Plain structs shared by the kernels and the host-side engine: the device
+// scene view, per-render parameters and the wavefront path state.
+#pragma once
+
+#include <cstdint>
+
+#include "dmath.cuh"
+
+namespace lambda_dev {
+
+constexpr int kMaxFilmLayers = 8;  // thin-film layers handled by the FP32 transfer matrix
+
+struct DeviceScene {
+    const float4 *nodes;
+    const float4 *prims;
+    const float4 *tri_attr;
+    const float4 *instances;
+    const float *spectra;
+    const uint8_t *spectrum_flat;
+    const double2 *cspectra;
+    const uint8_t *cspectrum_flat;
+    const int4 *materials;
+    const int *material_props;
+    const float4 *scalar_tex;
+    const int4 *spectrum_tex;
+    const int *light_inst;
+    const int *light_obj;
+    const float *light_power;
+    const float *light_cdf;      // running sums of light_power in list order
+    const float *material_emission;  // per material: average emission (0 if not emissive)
+    const float *cie;            // [471][3] as float
+    const int *perm;             // [256]
+    const float4 *worley_cells;  // feature offsets of lattice cells (xyz), cell-major
+    int3 worley_lo;              // first cell of the table
+    int3 worley_dim;             // cells per axis (0 when there is no table)
+    int num_nodes;
+    int num_objects;
+    int num_instances;
+    int num_lights;
+    float total_light_power;
+    int background_texture;
+};
+
+struct RenderParams {
+    int width, height, depth, samples, sqrt_samples;
+    float lambda_min, lambda_max, lambda_range;
+    f3 cam_pos, cam_corner, cam_h, cam_v;
+    uint64_t seed;
+    int num_pixels;
+};
+
+struct PathState {
+    uint64_t *rng;        // PCG32 state per pixel
+    float4 *film;         // accumulated linear sRGB (xyz)
+    float4 *lam;          // four hero wavelengths
+    float4 *ray_o;        // origin xyz, w = pdf of the last scatter
+    float4 *ray_d;        // direction xyz, w = 1 if the last scatter was specular
+    float4 *throughput;
+    float4 *radiance;
+    float4 *hit_p;        // world point xyz, w = u
+    float4 *hit_n;        // shading normal xyz, w = v
+    int4 *hit_id;         // instance (-1 = miss), object, front facing, 0
+    float4 *sh_o;         // NEE ray origin xyz, w = MIS weight
+    float4 *sh_d;         // NEE ray direction xyz, w = light pdf
+    float4 *sh_a;         // throughput * BSDF * cos
+    int2 *sh_light;       // light (instance, object)
+    int *queue[2];        // active pixel ids, ping-pong by bounce parity
+    int *shadow_queue;    // pixel ids with a pending NEE ray
+    int *counts;          // [2 * (depth + 2)]: active paths per bounce, then NEE rays per bounce
+    int *wave;            // [2]: wave to run next, wave being run
+    unsigned long long *stats;  // segments, shadow rays, thin-film hits
+    int *error;           // bit 0: traversal stack overflow
+};
+
+}  // namespace lambda_dev

@@ -1,0 +1,920 @@
+// GPU half of the C ABI (include/lambda_gpu.h): context, scene upload, the
+// wavefront render loop, ray queries and thin-film queries.
+//
+// A render is a sequence of sample waves (wavefront.cuh). One wave's kernels
+// (prologue, raygen, then intersect/shade/shadow per bounce) are captured once
+// into a CUDA graph and replayed `samples` times, so the host issues one graph
+// launch per wave; kernels read queue sizes from device counters and exit early
+// when their queue is empty.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lambda_gpu.h"
+#include "engine.h"
+#include "wavefront.cuh"
+
+#include "../host/tables.inc"
+
+using namespace lambda_dev;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context plumbing
+// ---------------------------------------------------------------------------
+
+lambda_status lambda_ctx::fail(lambda_status s, const std::string &msg) {
+    last_error = msg;
+    return s;
+}
+
+lambda_status lambda_ctx::cuda_fail(cudaError_t e, const char *what) {
+    last_error = std::string(what) + " (" + cudaGetErrorString(e) + ")";
+    return e == cudaErrorMemoryAllocation ? LAMBDA_ERR_OUT_OF_MEMORY : LAMBDA_ERR_CUDA;
+}
+
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+cudaError_t DeviceBuffer::reserve(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+}
+
+cudaError_t DeviceBuffer::upload(const void *src, size_t n, cudaStream_t st) {
+    cudaError_t e = reserve(n ? n : 16);
+    if (e != cudaSuccess || n == 0) return e;
+    return cudaMemcpyAsync(ptr, src, n, cudaMemcpyHostToDevice, st);
+}
+
+bool is_device_pointer(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+#define CK(call, what)                                        \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return ctx->cuda_fail(e_, what); \
+    } while (0)
+
+extern "C" lambda_status lambda_ctx_create(int32_t device, lambda_ctx **out) {
+    if (!out) return LAMBDA_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        g_create_error = std::string("no CUDA device (") + cudaGetErrorString(e) + ")";
+        cudaGetLastError();
+        return LAMBDA_ERR_CUDA;
+    }
+    if (device < 0 || device >= n) {
+        g_create_error = "device index out of range";
+        return LAMBDA_ERR_INVALID_ARGUMENT;
+    }
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("cudaSetDevice failed (") + cudaGetErrorString(e) + ")";
+        return LAMBDA_ERR_CUDA;
+    }
+    auto ctx = std::make_unique<lambda_ctx>();
+    ctx->device = device;
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    ctx->sm_count = prop.multiProcessorCount;
+    if (prop.major < 10) {
+        g_create_error = "this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major) +
+                         std::to_string(prop.minor);
+        return LAMBDA_ERR_UNSUPPORTED;
+    }
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("cudaStreamCreate failed (") + cudaGetErrorString(e) + ")";
+        return LAMBDA_ERR_CUDA;
+    }
+    cudaEventCreate(&ctx->ev_start);
+    cudaEventCreate(&ctx->ev_stop);
+    *out = ctx.release();
+    return LAMBDA_OK;
+}
+
+lambda_ctx::~lambda_ctx() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (DeviceBuffer *b : all_buffers()) b->release();
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_stop) cudaEventDestroy(ev_stop);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+extern "C" void lambda_ctx_destroy(lambda_ctx *ctx) { delete ctx; }
+
+extern "C" const char *lambda_last_error(const lambda_ctx *ctx) {
+    if (!ctx) return g_create_error.c_str();
+    return ctx->last_error.c_str();
+}
+
+// ---------------------------------------------------------------------------
+// Scene upload
+// ---------------------------------------------------------------------------
+
+namespace {
+
+float host_fract(float x) { return x - std::floor(x); }
+
+// Feature offsets of Worley cells as the reference computes them (utils.h:165)
+// with the C library's sinf, for every cell the scene's Worley textures can
+// reach: the world bounds (TLAS root) and the unit sphere (background lookups),
+// each times the texture frequency, plus a margin of two cells.
+void build_worley_table(const lambda_scene_desc &d, std::vector<float4> &cells, int3 &lo, int3 &dim) {
+    dim = make_int3(0, 0, 0);
+    lo = make_int3(0, 0, 0);
+    if (d.num_nodes == 0) return;
+    double bmin[3], bmax[3];
+    bool any = false;
+    for (int t = 0; t < d.num_scalar_textures; t++) {
+        const lambda_scalar_texture &x = d.scalar_textures[t];
+        if (x.type != LAMBDA_SCALAR_WORLEY) continue;
+        const double f = std::fabs(double(x.p[2]));
+        for (int k = 0; k < 3; k++) {
+            const double a = std::min({double(d.nodes[0].min[k]) * f, double(d.nodes[0].max[k]) * f, -f});
+            const double b = std::max({double(d.nodes[0].min[k]) * f, double(d.nodes[0].max[k]) * f, f});
+            bmin[k] = any ? std::min(bmin[k], a) : a;
+            bmax[k] = any ? std::max(bmax[k], b) : b;
+        }
+        any = true;
+    }
+    if (!any) return;
+    long long n = 1;
+    int l[3], e[3];
+    for (int k = 0; k < 3; k++) {
+        if (!(std::fabs(bmin[k]) < 1e6 && std::fabs(bmax[k]) < 1e6)) return;
+        l[k] = int(std::floor(bmin[k])) - 2;
+        e[k] = int(std::floor(bmax[k])) + 2 - l[k] + 1;
+        n *= e[k];
+    }
+    constexpr long long kMaxCells = 8ll << 20;  // 128 MB of float4
+    if (n > kMaxCells) return;
+    cells.resize(size_t(n));
+    for (int z = 0; z < e[2]; z++)
+        for (int y = 0; y < e[1]; y++)
+            for (int x = 0; x < e[0]; x++) {
+                const float cx = float(l[0] + x), cy = float(l[1] + y), cz = float(l[2] + z);
+                const float a = cx * 127.1f + cy * 311.7f + cz * 74.7f;
+                const float b = cx * 269.5f + cy * 183.3f + cz * 246.1f;
+                const float c = cx * 113.5f + cy * 271.9f + cz * 124.6f;
+                cells[(size_t(z) * e[1] + y) * e[0] + x] = make_float4(host_fract(std::sin(a) * 43758.5453f),
+                                                                       host_fract(std::sin(b) * 43758.5453f),
+                                                                       host_fract(std::sin(c) * 43758.5453f), 0.0f);
+            }
+    lo = make_int3(l[0], l[1], l[2]);
+    dim = make_int3(e[0], e[1], e[2]);
+}
+
+float spectrum_average_host(const float *d) {
+    float s = 0;
+    for (int k = 0; k < LAMBDA_CIE_BINS; k++) s += d[k];
+    return s / LAMBDA_CIE_BINS;
+}
+
+float spectrum_texture_average_host(const lambda_scene_desc &d, int t) {
+    const lambda_spectrum_texture &x = d.spectrum_textures[t];
+    if (x.type == LAMBDA_SPECTRUM_CONSTANT) return spectrum_average_host(d.spectra + size_t(x.value1) * LAMBDA_CIE_BINS);
+    if (x.type == LAMBDA_SPECTRUM_CHECKER)
+        return 0.5f * (spectrum_average_host(d.spectra + size_t(x.value1) * LAMBDA_CIE_BINS) +
+                       spectrum_average_host(d.spectra + size_t(x.value2) * LAMBDA_CIE_BINS));
+    const lambda_scalar_texture &s = d.scalar_textures[x.value1];
+    return s.type == LAMBDA_SCALAR_CONSTANT ? s.p[0] : (s.p[0] + s.p[1]) / 2;
+}
+
+lambda_status validate_scene(lambda_ctx *ctx, const lambda_scene_desc &d) {
+    if (d.num_nodes < 1 || d.num_objects < 1 || d.num_instances < 1 || d.num_lights < 1 || d.num_spectra < 1 ||
+        d.num_materials < 1 || d.num_spectrum_textures < 1 || d.num_scalar_textures < 1)
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "scene has an empty required container");
+    if (!d.nodes || !d.objects || !d.instances || !d.spectra || !d.materials || !d.spectrum_textures ||
+        !d.scalar_textures || !d.light_instances || !d.light_objects || !d.light_powers)
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "scene has a null container pointer");
+    if (d.background_texture < 0 || d.background_texture >= d.num_spectrum_textures)
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "background texture index out of range");
+    auto bad = [&](const char *m) { return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, m); };
+    for (int i = 0; i < d.num_nodes; i++) {
+        const lambda_bvh_node &n = d.nodes[i];
+        if (n.count > 0 ? n.index < 0 : (n.index <= i || n.index >= d.num_nodes || i + 1 >= d.num_nodes))
+            return bad("BVH node index out of range");
+    }
+    for (int i = 0; i < d.num_instances; i++) {
+        const lambda_instance &in = d.instances[i];
+        if (in.object < 0 || in.count < 1 || in.object + in.count > d.num_objects || in.node < 0 ||
+            in.node >= d.num_nodes || in.material >= d.num_materials)
+            return bad("instance fields out of range");
+    }
+    for (int i = 0; i < d.num_objects; i++)
+        if (d.objects[i].material < 0 || d.objects[i].material >= d.num_materials || d.objects[i].type < 0 ||
+            d.objects[i].type > 2)
+            return bad("object fields out of range");
+    auto spec_tex_ok = [&](int t) { return t >= 0 && t < d.num_spectrum_textures; };
+    for (int i = 0; i < d.num_materials; i++) {
+        const lambda_material &m = d.materials[i];
+        if (m.type == LAMBDA_MATERIAL_THINFILM) {
+            if (m.p[0] < 0 || m.p[0] > kMaxFilmLayers) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "thin film with more than 8 layers");
+            if (!d.complex_spectra || !d.material_properties || m.p[1] < 0 ||
+                m.p[1] + m.p[0] + 2 > d.num_material_properties || m.p[2] < 0 ||
+                m.p[2] + m.p[0] > d.num_material_properties)
+                return bad("thin-film properties out of range");
+            for (int k = 0; k < m.p[0] + 2; k++) {
+                const int c = d.material_properties[m.p[1] + k];
+                if (c < 0 || c >= d.num_complex_spectra) return bad("thin-film index spectrum out of range");
+            }
+            for (int k = 0; k < m.p[0]; k++) {
+                const int t = d.material_properties[m.p[2] + k];
+                if (t < 0 || t >= d.num_scalar_textures) return bad("thin-film thickness texture out of range");
+            }
+        } else if (m.type == LAMBDA_MATERIAL_DIELECTRIC) {
+            if (m.p[0] < 0 || m.p[0] >= d.num_spectra || m.p[1] < 0 || m.p[1] >= d.num_spectra)
+                return bad("dielectric spectrum out of range");
+        } else if (m.type == LAMBDA_MATERIAL_LAMBERTIAN || m.type == LAMBDA_MATERIAL_MIRROR ||
+                   m.type == LAMBDA_MATERIAL_EMISSIVE) {
+            if (!spec_tex_ok(m.p[0])) return bad("material texture out of range");
+        } else {
+            return bad("material type out of range");
+        }
+    }
+    for (int i = 0; i < d.num_spectrum_textures; i++) {
+        const lambda_spectrum_texture &t = d.spectrum_textures[i];
+        const bool ok = t.type == LAMBDA_SPECTRUM_CONSTANT ? (t.value1 >= 0 && t.value1 < d.num_spectra)
+                      : t.type == LAMBDA_SPECTRUM_CHECKER
+                          ? (t.value1 >= 0 && t.value1 < d.num_spectra && t.value2 >= 0 && t.value2 < d.num_spectra)
+                      : t.type == LAMBDA_SPECTRUM_SCALAR ? (t.value1 >= 0 && t.value1 < d.num_scalar_textures) : false;
+        if (!ok) return bad("spectrum texture fields out of range");
+    }
+    for (int i = 0; i < d.num_scalar_textures; i++)
+        if (d.scalar_textures[i].type < 0 || d.scalar_textures[i].type > 2) return bad("scalar texture type out of range");
+    for (int i = 0; i < d.num_lights; i++) {
+        const int li = d.light_instances[i], lo = d.light_objects[i];
+        const bool bg = li == -1 && lo == -1;
+        if (!bg && (li < 0 || li >= d.num_instances || lo < 0 || lo >= d.num_objects)) return bad("light id out of range");
+    }
+    if (d.light_instances[d.num_lights - 1] != -1) return bad("the last light must be the background (-1, -1)");
+    return LAMBDA_OK;
+}
+
+}  // namespace
+
+extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene_desc *desc) {
+    if (!ctx || !desc) return LAMBDA_ERR_INVALID_ARGUMENT;
+    const lambda_scene_desc &d = *desc;
+    lambda_status st = validate_scene(ctx, d);
+    if (st != LAMBDA_OK) return st;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = ctx->stream;
+    SceneBuffers &b = ctx->scene;
+
+    // nodes: (min, index) (max, count)
+    std::vector<float4> nodes(2 * size_t(d.num_nodes));
+    for (int i = 0; i < d.num_nodes; i++) {
+        const lambda_bvh_node &n = d.nodes[i];
+        float idx, cnt;
+        std::memcpy(&idx, &n.index, 4);
+        std::memcpy(&cnt, &n.count, 4);
+        nodes[2 * i] = make_float4(n.min[0], n.min[1], n.min[2], idx);
+        nodes[2 * i + 1] = make_float4(n.max[0], n.max[1], n.max[2], cnt);
+    }
+    std::vector<float4> prims(4 * size_t(d.num_objects)), tri(4 * size_t(d.num_objects));
+    for (int i = 0; i < d.num_objects; i++) {
+        const lambda_object &o = d.objects[i];
+        float ty, ma;
+        std::memcpy(&ty, &o.type, 4);
+        std::memcpy(&ma, &o.material, 4);
+        const float *g = o.g;
+        if (o.type == LAMBDA_OBJECT_SPHERE) {
+            prims[4 * i] = make_float4(g[0], g[1], g[2], ty);
+            prims[4 * i + 1] = make_float4(g[3], 0, 0, ma);
+            prims[4 * i + 2] = make_float4(0, 0, 0, 0);
+            prims[4 * i + 3] = make_float4(0, 0, 0, 0);
+        } else {
+            prims[4 * i] = make_float4(g[0], g[1], g[2], ty);
+            prims[4 * i + 1] = make_float4(g[3], g[4], g[5], ma);
+            prims[4 * i + 2] = make_float4(g[6], g[7], g[8], 0);
+            prims[4 * i + 3] = make_float4(g[9], g[10], g[11], 0);
+        }
+        if (o.type == LAMBDA_OBJECT_TRI) {
+            tri[4 * i] = make_float4(g[12], g[13], g[14], g[15]);
+            tri[4 * i + 1] = make_float4(g[16], g[17], g[18], g[19]);
+            tri[4 * i + 2] = make_float4(g[20], g[21], g[22], g[23]);
+            tri[4 * i + 3] = make_float4(g[24], g[25], g[26], 0);
+        } else {
+            for (int k = 0; k < 4; k++) tri[4 * i + k] = make_float4(0, 0, 0, 0);
+        }
+    }
+    std::vector<float4> inst(9 * size_t(d.num_instances));
+    for (int i = 0; i < d.num_instances; i++) {
+        const lambda_instance &in = d.instances[i];
+        float h[4];
+        std::memcpy(h, &in.object, 16);
+        inst[9 * i] = make_float4(h[0], h[1], h[2], h[3]);
+        for (int r = 0; r < 4; r++) {
+            inst[9 * i + 1 + r] = make_float4(in.transform[4 * r], in.transform[4 * r + 1], in.transform[4 * r + 2], in.transform[4 * r + 3]);
+            inst[9 * i + 5 + r] = make_float4(in.inverse_transform[4 * r], in.inverse_transform[4 * r + 1],
+                                              in.inverse_transform[4 * r + 2], in.inverse_transform[4 * r + 3]);
+        }
+    }
+    std::vector<uint8_t> flat(d.num_spectra), cflat(std::max(d.num_complex_spectra, 1), 0);
+    for (int i = 0; i < d.num_spectra; i++) {
+        const float *x = d.spectra + size_t(i) * LAMBDA_CIE_BINS;
+        flat[i] = std::all_of(x, x + LAMBDA_CIE_BINS, [&](float v) { return v == x[0]; }) ? 1 : 0;
+    }
+    for (int i = 0; i < d.num_complex_spectra; i++) {
+        const double *x = d.complex_spectra + size_t(i) * LAMBDA_CIE_BINS * 2;
+        bool same = true;
+        for (int k = 1; k < LAMBDA_CIE_BINS && same; k++) same = x[2 * k] == x[0] && x[2 * k + 1] == x[1];
+        cflat[i] = same ? 1 : 0;
+    }
+    std::vector<int4> mats(d.num_materials);
+    std::vector<float> emission(d.num_materials, 0.0f);
+    for (int i = 0; i < d.num_materials; i++) {
+        const lambda_material &m = d.materials[i];
+        mats[i] = make_int4(m.type, m.p[0], m.p[1], m.p[2]);
+        if (m.type == LAMBDA_MATERIAL_EMISSIVE) emission[i] = spectrum_texture_average_host(d, m.p[0]);
+    }
+    std::vector<float4> stex(d.num_scalar_textures);
+    for (int i = 0; i < d.num_scalar_textures; i++) {
+        const lambda_scalar_texture &t = d.scalar_textures[i];
+        float ty;
+        std::memcpy(&ty, &t.type, 4);
+        stex[i] = make_float4(ty, t.p[0], t.p[1], t.p[2]);
+    }
+    std::vector<int4> sptex(d.num_spectrum_textures);
+    for (int i = 0; i < d.num_spectrum_textures; i++) {
+        const lambda_spectrum_texture &t = d.spectrum_textures[i];
+        int sc;
+        std::memcpy(&sc, &t.scale, 4);
+        sptex[i] = make_int4(t.type, t.value1, t.value2, sc);
+    }
+    std::vector<float> cdf(d.num_lights);
+    float run = 0;
+    for (int i = 0; i < d.num_lights; i++) {
+        run += d.light_powers[i];
+        cdf[i] = run;
+    }
+    std::vector<float> cie(LAMBDA_CIE_BINS * 3);
+    for (int i = 0; i < LAMBDA_CIE_BINS; i++)
+        for (int k = 0; k < 3; k++) cie[3 * i + k] = float(kCieXyz1931[i][k]);
+    std::vector<float4> worley;
+    int3 wlo, wdim;
+    build_worley_table(d, worley, wlo, wdim);
+    const std::vector<int> props(d.material_properties, d.material_properties + d.num_material_properties);
+
+    CK(b.nodes.upload(nodes.data(), nodes.size() * sizeof(float4), s), "upload nodes");
+    CK(b.prims.upload(prims.data(), prims.size() * sizeof(float4), s), "upload objects");
+    CK(b.tri.upload(tri.data(), tri.size() * sizeof(float4), s), "upload triangles");
+    CK(b.instances.upload(inst.data(), inst.size() * sizeof(float4), s), "upload instances");
+    CK(b.spectra.upload(d.spectra, size_t(d.num_spectra) * LAMBDA_CIE_BINS * sizeof(float), s), "upload spectra");
+    CK(b.spectrum_flat.upload(flat.data(), flat.size(), s), "upload spectra");
+    CK(b.cspectra.upload(d.complex_spectra, size_t(d.num_complex_spectra) * LAMBDA_CIE_BINS * 2 * sizeof(double), s),
+       "upload complex spectra");
+    CK(b.cspectrum_flat.upload(cflat.data(), cflat.size(), s), "upload complex spectra");
+    CK(b.materials.upload(mats.data(), mats.size() * sizeof(int4), s), "upload materials");
+    CK(b.material_props.upload(props.data(), props.size() * sizeof(int), s), "upload material properties");
+    CK(b.scalar_tex.upload(stex.data(), stex.size() * sizeof(float4), s), "upload textures");
+    CK(b.spectrum_tex.upload(sptex.data(), sptex.size() * sizeof(int4), s), "upload textures");
+    CK(b.light_inst.upload(d.light_instances, size_t(d.num_lights) * sizeof(int), s), "upload lights");
+    CK(b.light_obj.upload(d.light_objects, size_t(d.num_lights) * sizeof(int), s), "upload lights");
+    CK(b.light_power.upload(d.light_powers, size_t(d.num_lights) * sizeof(float), s), "upload lights");
+    CK(b.light_cdf.upload(cdf.data(), cdf.size() * sizeof(float), s), "upload lights");
+    CK(b.material_emission.upload(emission.data(), emission.size() * sizeof(float), s), "upload materials");
+    CK(b.cie.upload(cie.data(), cie.size() * sizeof(float), s), "upload CIE table");
+    CK(b.perm.upload(kPerlinPermutation, sizeof(kPerlinPermutation), s), "upload permutation");
+    CK(b.worley.upload(worley.data(), worley.size() * sizeof(float4), s), "upload Worley lattice");
+    CK(cudaStreamSynchronize(s), "scene upload");
+
+    DeviceScene &ds = ctx->dscene;
+    ds.nodes = b.nodes.as<float4>();
+    ds.prims = b.prims.as<float4>();
+    ds.tri_attr = b.tri.as<float4>();
+    ds.instances = b.instances.as<float4>();
+    ds.spectra = b.spectra.as<float>();
+    ds.spectrum_flat = b.spectrum_flat.as<uint8_t>();
+    ds.cspectra = b.cspectra.as<double2>();
+    ds.cspectrum_flat = b.cspectrum_flat.as<uint8_t>();
+    ds.materials = b.materials.as<int4>();
+    ds.material_props = b.material_props.as<int>();
+    ds.scalar_tex = b.scalar_tex.as<float4>();
+    ds.spectrum_tex = b.spectrum_tex.as<int4>();
+    ds.light_inst = b.light_inst.as<int>();
+    ds.light_obj = b.light_obj.as<int>();
+    ds.light_power = b.light_power.as<float>();
+    ds.light_cdf = b.light_cdf.as<float>();
+    ds.material_emission = b.material_emission.as<float>();
+    ds.cie = b.cie.as<float>();
+    ds.perm = b.perm.as<int>();
+    ds.worley_cells = b.worley.as<float4>();
+    ds.worley_lo = wlo;
+    ds.worley_dim = wdim;
+    ds.num_nodes = d.num_nodes;
+    ds.num_objects = d.num_objects;
+    ds.num_instances = d.num_instances;
+    ds.num_lights = d.num_lights;
+    ds.total_light_power = d.total_light_power;
+    ds.background_texture = d.background_texture;
+    ctx->has_scene = true;
+    ctx->film_layers_max = 0;
+    for (int i = 0; i < d.num_materials; i++)
+        if (d.materials[i].type == LAMBDA_MATERIAL_THINFILM) ctx->film_layers_max = std::max(ctx->film_layers_max, d.materials[i].p[0]);
+    return LAMBDA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Render
+// ---------------------------------------------------------------------------
+
+namespace {
+
+int grid_for(int sm_count, const void *kernel, int block) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+    return std::max(1, per_sm) * sm_count;
+}
+
+struct Progress {
+    volatile int32_t *completed;
+    int32_t value;
+};
+
+void CUDART_CB progress_cb(void *p) {
+    auto *pr = static_cast<Progress *>(p);
+    *pr->completed = pr->value;
+}
+
+}  // namespace
+
+StageProfiler::StageProfiler(cudaStream_t s) : stream(s) {}
+
+StageProfiler::~StageProfiler() {
+    for (auto &e : pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+}
+
+void StageProfiler::begin(int stage) {
+    if (used == pool.size()) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        pool.push_back({a, b});
+        stages.push_back(0);
+    }
+    stages[used] = stage;
+    cudaEventRecord(pool[used].first, stream);
+}
+
+void StageProfiler::end() {
+    cudaEventRecord(pool[used].second, stream);
+    used++;
+}
+
+cudaError_t StageProfiler::collect() {
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    for (size_t i = 0; i < used; i++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, pool[i].first, pool[i].second);
+        totals[stages[i]] += ms;
+        counts[stages[i]]++;
+    }
+    used = 0;
+    return cudaSuccess;
+}
+
+lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
+    lambda_ctx *ctx = this;
+    const size_t P = size_t(pixels);
+    RenderBuffers &r = rbuf;
+    CK(r.rng.reserve(P * 8), "allocate path state");
+    CK(r.film.reserve(P * 16), "allocate path state");
+    CK(r.lam.reserve(P * 16), "allocate path state");
+    CK(r.ray_o.reserve(P * 16), "allocate path state");
+    CK(r.ray_d.reserve(P * 16), "allocate path state");
+    CK(r.throughput.reserve(P * 16), "allocate path state");
+    CK(r.radiance.reserve(P * 16), "allocate path state");
+    CK(r.hit_p.reserve(P * 16), "allocate path state");
+    CK(r.hit_n.reserve(P * 16), "allocate path state");
+    CK(r.hit_id.reserve(P * 16), "allocate path state");
+    CK(r.sh_o.reserve(P * 16), "allocate path state");
+    CK(r.sh_d.reserve(P * 16), "allocate path state");
+    CK(r.sh_a.reserve(P * 16), "allocate path state");
+    CK(r.sh_light.reserve(P * 8), "allocate path state");
+    CK(r.q0.reserve(P * 4), "allocate queues");
+    CK(r.q1.reserve(P * 4), "allocate queues");
+    CK(r.qs.reserve(P * 4), "allocate queues");
+    CK(r.counts.reserve(size_t(2 * (depth + 2)) * 4), "allocate queues");
+    CK(r.wave.reserve(16), "allocate queues");
+    CK(r.stats.reserve(8 * 8), "allocate statistics");
+    CK(r.error.reserve(16), "allocate flags");
+    CK(r.out.reserve(P * 12), "allocate output");
+    PathState &ps = pstate;
+    ps.rng = r.rng.as<uint64_t>();
+    ps.film = r.film.as<float4>();
+    ps.lam = r.lam.as<float4>();
+    ps.ray_o = r.ray_o.as<float4>();
+    ps.ray_d = r.ray_d.as<float4>();
+    ps.throughput = r.throughput.as<float4>();
+    ps.radiance = r.radiance.as<float4>();
+    ps.hit_p = r.hit_p.as<float4>();
+    ps.hit_n = r.hit_n.as<float4>();
+    ps.hit_id = r.hit_id.as<int4>();
+    ps.sh_o = r.sh_o.as<float4>();
+    ps.sh_d = r.sh_d.as<float4>();
+    ps.sh_a = r.sh_a.as<float4>();
+    ps.sh_light = r.sh_light.as<int2>();
+    ps.queue[0] = r.q0.as<int>();
+    ps.queue[1] = r.q1.as<int>();
+    ps.shadow_queue = r.qs.as<int>();
+    ps.counts = r.counts.as<int>();
+    ps.wave = r.wave.as<int>();
+    ps.stats = r.stats.as<unsigned long long>();
+    ps.error = r.error.as<int>();
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc *desc, float *out_rgb,
+                                       volatile int32_t *completed) {
+    if (!ctx || !desc || !out_rgb) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
+    const lambda_render_settings &st = desc->settings;
+    if (st.width <= 0 || st.height <= 0 || st.depth < 0 || st.samples < 1 || st.sqrt_samples * st.sqrt_samples != st.samples)
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "invalid render settings");
+    if (!(st.lambda_min >= LAMBDA_CIE_LAMBDA_MIN && st.lambda_max <= LAMBDA_CIE_LAMBDA_MAX && st.lambda_min < st.lambda_max))
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "wavelength range outside [360, 830] nm");
+    if (int64_t(st.width) * st.height > (int64_t(1) << 30)) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "image too large");
+    if (st.depth > 1024) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "depth above 1024");
+    if (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) {
+        lambda_status s = ctx->surrogate_ready();
+        if (s != LAMBDA_OK) return s;
+    }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const bool out_device = (desc->flags & LAMBDA_RENDER_OUTPUT_DEVICE) != 0;
+    if (out_device && !is_device_pointer(out_rgb))
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "LAMBDA_RENDER_OUTPUT_DEVICE given a host pointer");
+
+    RenderParams rp{};
+    rp.width = st.width;
+    rp.height = st.height;
+    rp.depth = st.depth;
+    rp.samples = st.samples;
+    rp.sqrt_samples = st.sqrt_samples;
+    rp.lambda_min = st.lambda_min;
+    rp.lambda_max = st.lambda_max;
+    rp.lambda_range = st.lambda_max - st.lambda_min;
+    const lambda_camera &c = st.camera;
+    rp.cam_pos = mk(c.position[0], c.position[1], c.position[2]);
+    rp.cam_corner = mk(c.corner[0], c.corner[1], c.corner[2]);
+    rp.cam_h = mk(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
+    rp.cam_v = mk(c.vertical[0], c.vertical[1], c.vertical[2]);
+    rp.seed = desc->seed;
+    rp.num_pixels = st.width * st.height;
+
+    lambda_status s = ctx->ensure_state(rp.num_pixels, rp.depth);
+    if (s != LAMBDA_OK) return s;
+    cudaStream_t stream = ctx->stream;
+    const PathState ps = ctx->pstate;
+    const DeviceScene sc = ctx->dscene;
+    const int P = rp.num_pixels;
+    const int pix_blocks = (P + 255) / 256;
+    const int qgrid = std::min(pix_blocks, grid_for(ctx->sm_count, (const void *)k_shade, 256));
+    const bool surrogate = (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) != 0;
+
+    CK(cudaMemsetAsync(ps.stats, 0, 8 * 8, stream), "clear statistics");
+    CK(cudaMemsetAsync(ps.error, 0, 16, stream), "clear flags");
+    CK(cudaMemsetAsync(ps.counts, 0, size_t(2 * (rp.depth + 2)) * 4, stream), "clear counters");
+    CK(cudaEventRecord(ctx->ev_start, stream), "event");
+    k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps);
+    CK(cudaGetLastError(), "launch init");
+    int launches = 1;
+
+    // One wave's launches. With a profiler every launch is bracketed by events.
+    const bool profile = (desc->flags & LAMBDA_RENDER_PROFILE_STAGES) != 0;
+    StageProfiler prof(stream);
+    auto wave = [&](StageProfiler *pr) -> int {
+        int n = 0;
+        auto timed = [&](int stage, auto &&launch) {
+            if (pr) pr->begin(stage);
+            launch();
+            if (pr) pr->end();
+            n++;
+        };
+        timed(1, [&] { k_wave_prologue<<<1, 256, 0, stream>>>(rp.depth, ps); });
+        timed(2, [&] { k_raygen<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
+        for (int b = 0; b <= rp.depth; b++) {
+            timed(3, [&] { k_intersect<<<qgrid, 256, 0, stream>>>(b, sc, ps); });
+            if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, qgrid, pr);
+            else timed(4, [&] { k_shade<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+            timed(5, [&] { k_shadow<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+        }
+        return n;
+    };
+    std::vector<Progress> progress(completed ? size_t(rp.samples) : 0);
+    auto report = [&](int w) -> cudaError_t {
+        if (!completed) return cudaSuccess;
+        progress[w] = Progress{completed, int32_t(int64_t(P) * (w + 1) / rp.samples)};
+        if (w + 1 == rp.samples) progress[w].value = P;
+        return cudaLaunchHostFunc(stream, progress_cb, &progress[w]);
+    };
+    if (profile) {
+        for (int w = 0; w < rp.samples; w++) {
+            launches += wave(&prof);
+            CK(cudaGetLastError(), "launch wave");
+            CK(report(w), "progress callback");
+            CK(prof.collect(), "stage timing");
+        }
+    } else {
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        const int wave_launches = wave(nullptr);
+        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+        if (ce != cudaSuccess) return ctx->cuda_fail(ce, "capture wave graph");
+        if (ctx->graph_exec) {
+            cudaGraphExecDestroy(ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+        }
+        ce = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return ctx->cuda_fail(ce, "instantiate wave graph");
+        for (int w = 0; w < rp.samples; w++) {
+            CK(cudaGraphLaunch(ctx->graph_exec, stream), "launch wave");
+            launches += wave_launches;
+            CK(report(w), "progress callback");
+        }
+    }
+    k_wave_prologue<<<1, 256, 0, stream>>>(rp.depth, ps);  // folds the last wave's counts into the statistics
+    float *dout = out_device ? out_rgb : ctx->rbuf.out.as<float>();
+    k_finish<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps, dout);
+    launches += 2;
+    CK(cudaGetLastError(), "launch finish");
+    CK(cudaEventRecord(ctx->ev_stop, stream), "event");
+    if (!out_device)
+        CK(cudaMemcpyAsync(out_rgb, dout, size_t(P) * 12, cudaMemcpyDeviceToHost, stream), "copy image to host");
+    unsigned long long stats[8] = {0};
+    int err[4] = {0};
+    CK(cudaMemcpyAsync(stats, ps.stats, sizeof(stats), cudaMemcpyDeviceToHost, stream), "read statistics");
+    CK(cudaMemcpyAsync(err, ps.error, sizeof(err), cudaMemcpyDeviceToHost, stream), "read flags");
+    CK(cudaStreamSynchronize(stream), "render");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+    ctx->stats = lambda_render_stats{};
+    ctx->stats.render_ms = ms;
+    ctx->stats.paths = int64_t(P) * rp.samples;
+    ctx->stats.segments = int64_t(stats[0]);
+    ctx->stats.shadow_rays = int64_t(stats[1]);
+    ctx->stats.thinfilm_hits = int64_t(stats[2]);
+    ctx->stats.thinfilm_fallback = int64_t(stats[3]);
+    ctx->stats.kernel_launches = launches;
+    ctx->stats.waves = rp.samples;
+    if (profile) {
+        prof.totals[0] = 0;
+        for (int i = 0; i < LAMBDA_NUM_STAGES; i++) {
+            ctx->stage_times[i].ms = prof.totals[i];
+            ctx->stage_times[i].launches = prof.counts[i];
+        }
+        ctx->stage_times[0].launches = 1;
+        ctx->stage_times[1].items = rp.samples;
+        ctx->stage_times[2].items = int64_t(P) * rp.samples;
+        ctx->stage_times[3].items = ctx->stats.segments;
+        ctx->stage_times[4].items = ctx->stats.segments;
+        ctx->stage_times[5].items = ctx->stats.shadow_rays;
+        ctx->stage_times[6].items = P;
+        ctx->stage_times[7].items = ctx->stats.thinfilm_hits;
+        ctx->stage_times[8].items = ctx->stats.thinfilm_hits;
+    }
+    if (err[0] & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_get_stage_times(const lambda_ctx *ctx, lambda_stage_time *out) {
+    if (!ctx || !out) return LAMBDA_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < LAMBDA_NUM_STAGES; i++) out[i] = ctx->stage_times[i];
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_get_render_stats(const lambda_ctx *ctx, lambda_render_stats *stats) {
+    if (!ctx || !stats) return LAMBDA_ERR_INVALID_ARGUMENT;
+    *stats = ctx->stats;
+    return LAMBDA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ray queries
+// ---------------------------------------------------------------------------
+
+namespace {
+
+__global__ void k_trace_closest(DeviceScene sc, const float *rays, int n, int *inst, int *obj, float *t, int *error) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float *r = rays + 6 * size_t(k);
+    Hit h;
+    bool overflow = false;
+    closest_hit(sc, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), h, overflow);
+    inst[k] = h.instance;
+    obj[k] = h.object;
+    t[k] = h.t;
+    if (overflow) atomicOr(error, 1);
+}
+
+__global__ void k_trace_shadow(DeviceScene sc, const float *rays, const int *li, const int *lo, int n, int *occ,
+                               int *error) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float *r = rays + 6 * size_t(k);
+    Hit h;
+    bool overflow = false;
+    occ[k] = occluded(sc, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), li[k], lo[k], h, overflow) ? 1 : 0;
+    if (overflow) atomicOr(error, 1);
+}
+
+}  // namespace
+
+// Stages caller arrays (host or device) in and out of device memory.
+struct Staging {
+    lambda_ctx *ctx;
+    std::vector<void *> owned;
+    ~Staging() {
+        for (void *p : owned) cudaFree(p);
+    }
+    template <typename T>
+    cudaError_t in(const T *src, size_t n, const T **dst) {
+        if (is_device_pointer(src)) {
+            *dst = src;
+            return cudaSuccess;
+        }
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n * sizeof(T), 16));
+        if (e != cudaSuccess) return e;
+        owned.push_back(p);
+        *dst = static_cast<const T *>(p);
+        return cudaMemcpyAsync(p, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    }
+    template <typename T>
+    cudaError_t out(T *user, size_t n, T **dst, std::vector<std::pair<void *, std::pair<void *, size_t>>> &back) {
+        if (is_device_pointer(user)) {
+            *dst = user;
+            return cudaSuccess;
+        }
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n * sizeof(T), 16));
+        if (e != cudaSuccess) return e;
+        owned.push_back(p);
+        *dst = static_cast<T *>(p);
+        back.push_back({user, {p, n * sizeof(T)}});
+        return cudaSuccess;
+    }
+};
+
+using CopyBack = std::vector<std::pair<void *, std::pair<void *, size_t>>>;
+
+static lambda_status finish_staging(lambda_ctx *ctx, CopyBack &back) {
+    for (auto &b : back)
+        CK(cudaMemcpyAsync(b.first, b.second.first, b.second.second, cudaMemcpyDeviceToHost, ctx->stream), "copy results");
+    CK(cudaStreamSynchronize(ctx->stream), "query");
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_trace_closest(lambda_ctx *ctx, const float *rays, int32_t n, int32_t *out_instance,
+                                              int32_t *out_object, float *out_t) {
+    if (!ctx || n < 0 || (n > 0 && (!rays || !out_instance || !out_object || !out_t))) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
+    if (n == 0) return LAMBDA_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    Staging sg{ctx, {}};
+    CopyBack back;
+    const float *dr;
+    int *di, *dobj;
+    float *dt;
+    CK(sg.in(rays, size_t(n) * 6, &dr), "stage rays");
+    CK(sg.out(out_instance, size_t(n), &di, back), "stage results");
+    CK(sg.out(out_object, size_t(n), &dobj, back), "stage results");
+    CK(sg.out(out_t, size_t(n), &dt, back), "stage results");
+    CK(ctx->rbuf.error.reserve(16), "allocate flags");
+    int *err = ctx->rbuf.error.as<int>();
+    CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
+    k_trace_closest<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->dscene, dr, n, di, dobj, dt, err);
+    CK(cudaGetLastError(), "launch trace");
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");
+    lambda_status s = finish_staging(ctx, back);
+    if (s != LAMBDA_OK) return s;
+    if (herr & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_trace_shadow(lambda_ctx *ctx, const float *rays, const int32_t *light_instance,
+                                             const int32_t *light_object, int32_t n, int32_t *out_occluded) {
+    if (!ctx || n < 0 || (n > 0 && (!rays || !light_instance || !light_object || !out_occluded)))
+        return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
+    if (n == 0) return LAMBDA_OK;
+    // light ids are checked on the host: the kernel indexes instances/objects with them
+    std::vector<int32_t> hli(n), hlo(n);
+    if (is_device_pointer(light_instance)) CK(cudaMemcpy(hli.data(), light_instance, 4 * size_t(n), cudaMemcpyDeviceToHost), "read lights");
+    else std::memcpy(hli.data(), light_instance, 4 * size_t(n));
+    if (is_device_pointer(light_object)) CK(cudaMemcpy(hlo.data(), light_object, 4 * size_t(n), cudaMemcpyDeviceToHost), "read lights");
+    else std::memcpy(hlo.data(), light_object, 4 * size_t(n));
+    for (int k = 0; k < n; k++) {
+        const bool bg = hli[k] == -1 && hlo[k] == -1;
+        const bool ok = bg || (hli[k] >= 0 && hli[k] < ctx->dscene.num_instances && hlo[k] >= 0 && hlo[k] < ctx->dscene.num_objects);
+        if (!ok) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "light id out of range");
+    }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    Staging sg{ctx, {}};
+    CopyBack back;
+    const float *dr;
+    const int *dli, *dlo;
+    int *docc;
+    CK(sg.in(rays, size_t(n) * 6, &dr), "stage rays");
+    CK(sg.in(hli.data(), size_t(n), &dli), "stage lights");
+    CK(sg.in(hlo.data(), size_t(n), &dlo), "stage lights");
+    CK(sg.out(out_occluded, size_t(n), &docc, back), "stage results");
+    CK(ctx->rbuf.error.reserve(16), "allocate flags");
+    int *err = ctx->rbuf.error.as<int>();
+    CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
+    k_trace_shadow<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->dscene, dr, dli, dlo, n, docc, err);
+    CK(cudaGetLastError(), "launch trace");
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");
+    lambda_status s = finish_staging(ctx, back);
+    if (s != LAMBDA_OK) return s;
+    if (herr & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
+    return LAMBDA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Thin-film queries: single film between air (n = 1) and a substrate.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+template <typename R>
+__global__ void k_film_query(const lambda_film_query *q, int n, R *out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const lambda_film_query x = q[k];
+    cx<R> idx[3] = {cx<R>{R(1), R(0)}, cx<R>{R(x.n_film), R(0)}, cx<R>{R(x.n_sub), R(0)}};
+    const R d = R(x.thickness_nm);
+    const FilmResult<R> r = film_stack<R, 1>(1, idx, &d, R(x.cos_theta), R(x.lambda_nm));
+    out[4 * size_t(k)] = r.rs;
+    out[4 * size_t(k) + 1] = r.rp;
+    out[4 * size_t(k) + 2] = r.ts;
+    out[4 * size_t(k) + 3] = r.tp;
+}
+
+template <typename R>
+lambda_status film_query(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, R *out) {
+    if (!ctx || n < 0 || (n > 0 && (!q || !out))) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (n == 0) return LAMBDA_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    Staging sg{ctx, {}};
+    CopyBack back;
+    const lambda_film_query *dq;
+    R *dout;
+    CK(sg.in(q, size_t(n), &dq), "stage queries");
+    CK(sg.out(out, size_t(n) * 4, &dout, back), "stage results");
+    k_film_query<R><<<(n + 127) / 128, 128, 0, ctx->stream>>>(dq, n, dout);
+    CK(cudaGetLastError(), "launch thin-film query");
+    return finish_staging(ctx, back);
+}
+
+}  // namespace
+
+extern "C" lambda_status lambda_thinfilm_exact(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, float *out) {
+    return film_query<float>(ctx, q, n, out);
+}
+
+extern "C" lambda_status lambda_thinfilm_fp64(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, double *out) {
+    return film_query<double>(ctx, q, n, out);
+}

@@ -1,0 +1,101 @@
+// The context object behind the C ABI and its device buffers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "lambda_gpu.h"
+#include "dtypes.cuh"
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t n);
+    cudaError_t upload(const void *src, size_t n, cudaStream_t s);
+    void release();
+    template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+bool is_device_pointer(const void *p);
+
+// Brackets kernel launches with CUDA events and totals their device time per
+// stage (LAMBDA_RENDER_PROFILE_STAGES).
+struct StageProfiler {
+    cudaStream_t stream;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+    std::vector<int> stages;
+    size_t used = 0;
+    double totals[LAMBDA_NUM_STAGES] = {0};
+    int64_t counts[LAMBDA_NUM_STAGES] = {0};
+    explicit StageProfiler(cudaStream_t s);
+    ~StageProfiler();
+    void begin(int stage);
+    void end();
+    cudaError_t collect();
+};
+
+struct SceneBuffers {
+    DeviceBuffer nodes, prims, tri, instances, spectra, spectrum_flat, cspectra, cspectrum_flat, materials,
+        material_props, scalar_tex, spectrum_tex, light_inst, light_obj, light_power, light_cdf, material_emission,
+        cie, perm, worley;
+};
+
+struct RenderBuffers {
+    DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
+        q0, q1, qs, counts, wave, stats, error, out;
+    // thin-film surrogate batch
+    DeviceBuffer tf_queue, tf_in, tf_out;
+};
+
+struct SurrogateBuffers {
+    DeviceBuffer weights_bf16;  // packed tensor-core operand tiles
+    DeviceBuffer weights_f32;   // master copy, LAMBDA_MLP_PARAMS floats
+    DeviceBuffer scratch;
+};
+
+struct lambda_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    std::string last_error;
+
+    bool has_scene = false;
+    int film_layers_max = 0;
+    SceneBuffers scene;
+    lambda_dev::DeviceScene dscene{};
+
+    RenderBuffers rbuf;
+    lambda_dev::PathState pstate{};
+    cudaGraphExec_t graph_exec = nullptr;
+    lambda_render_stats stats{};
+    lambda_stage_time stage_times[LAMBDA_NUM_STAGES]{};
+
+    // surrogate
+    bool has_surrogate = false;
+    lambda_film_range surrogate_range{};
+    SurrogateBuffers sbuf;
+
+    ~lambda_ctx();
+
+    lambda_status fail(lambda_status s, const std::string &msg);
+    lambda_status cuda_fail(cudaError_t e, const char *what);
+    lambda_status ensure_state(int pixels, int depth);
+    lambda_status surrogate_ready();
+    int launch_shade_surrogate(int bounce, const lambda_dev::RenderParams &rp, const lambda_dev::DeviceScene &sc,
+                               const lambda_dev::PathState &ps, int grid, StageProfiler *prof);
+
+    std::vector<DeviceBuffer *> all_buffers() {
+        SceneBuffers &s = scene;
+        RenderBuffers &r = rbuf;
+        return {&s.nodes, &s.prims, &s.tri, &s.instances, &s.spectra, &s.spectrum_flat, &s.cspectra,
+                &s.cspectrum_flat, &s.materials, &s.material_props, &s.scalar_tex, &s.spectrum_tex, &s.light_inst,
+                &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley,
+                &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
+                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.counts, &r.wave,
+                &r.stats, &r.error, &r.out, &r.tf_queue, &r.tf_in, &r.tf_out, &sbuf.weights_bf16,
+                &sbuf.weights_f32, &sbuf.scratch};
+    }
+};
