@@ -1,0 +1,79 @@
+"""The C ABI library loads and exports every entry point include/lambda_gpu.h
+declares; entry points fail cleanly (status codes, messages) without a GPU."""
+
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from lambda_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "lambda_gpu.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lambda_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_bound_symbols():
+    assert set(declared()) == set(N.EXPORTED_SYMBOLS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = N.load()
+    for name in declared():
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", N.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (lambda_[a-z0-9_]+)", out))
+    assert set(declared()) <= exported
+
+
+def test_struct_sizes_match_reference_layout():
+    assert ctypes.sizeof(N.Object) == 116
+    assert ctypes.sizeof(N.Instance) == 144
+    assert ctypes.sizeof(N.BVHNode) == 32
+    assert ctypes.sizeof(N.Material) == 16
+    assert ctypes.sizeof(N.ScalarTexture) == 16
+    assert ctypes.sizeof(N.SpectrumTexture) == 16
+    from oracle import ref
+
+    if ref.available():
+        lib = ref.load()
+        assert [lib.ref_sizeof(i) for i in range(6)] == [116, 144, 32, 16, 16, 16]
+
+
+def test_null_arguments_are_rejected():
+    lib = N.load()
+    assert lib.lambda_scene_upload(None, None) == 1
+    assert lib.lambda_render(None, None, None, None) == 1
+    assert lib.lambda_trace_closest(None, None, 0, None, None, None) == 1
+    assert lib.lambda_ctx_create(0, None) == 1
+
+
+def test_ctx_create_without_gpu_reports_error():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = N.load()
+    h = ctypes.c_void_p()
+    st = lib.lambda_ctx_create(0, ctypes.byref(h))
+    assert st in (4, 1)
+    assert lib.lambda_last_error(None)
+
+
+def test_cli_argument_errors(tmp_path):
+    exe = os.path.join(ROOT, "lambda_b200", "bin", "lambda")
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 1 and "invalid number of arguments" in r.stderr
+    r = subprocess.run([exe, "scene.txt"], capture_output=True, text=True)
+    assert r.returncode == 1 and r.stderr.strip() == "scene.txt: invalid file extension"
+    bad = tmp_path / "bad.lrd"
+    bad.write_text("Camera (0 0 0) (0 0 0) (1 0 0) (0 1 0)\n")
+    r = subprocess.run([exe, str(bad)], capture_output=True, text=True)
+    assert r.returncode == 1 and r.stderr.strip() == f'{bad}:1: expected "Render", got "Camera"'

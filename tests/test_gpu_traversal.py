@@ -6,7 +6,7 @@ import pytest
 
 import lambda_b200 as lb
 from lambda_b200 import scenes
-from oracle import ref
+from oracle import port, ref
 from tests.helpers import camera_rays, random_rays
 
 pytestmark = pytest.mark.gpu
@@ -34,14 +34,19 @@ def _ray_set(scene, n=20000):
     return np.concatenate([random_rays(n, center - ext, center + ext, 11), camera_rays(scene.settings, n, 12)])
 
 
+def _oracle_hit(sc, scene, rays):
+    if ref.available():
+        r_inst, r_obj, r_t, _, _ = ref.RefScene(sc.lrd).hit(rays)
+        return r_inst, r_obj, r_t
+    return port.hit(scene, rays)
+
+
 def test_closest_hit_ids_bit_exact(loaded, ctx):
     name, sc, scene = loaded
-    if not ref.available():
-        pytest.skip("reference harness not built")
     ctx.upload(scene)
     rays = _ray_set(scene)
     inst, obj, t = ctx.trace_closest(rays)
-    r_inst, r_obj, r_t, _, _ = ref.RefScene(sc.lrd).hit(rays)
+    r_inst, r_obj, r_t = _oracle_hit(sc, scene, rays)
     assert (inst == r_inst).all(), f"{name}: instance ids differ at {np.flatnonzero(inst != r_inst)[:10]}"
     assert (obj == r_obj).all(), f"{name}: object ids differ at {np.flatnonzero(obj != r_obj)[:10]}"
     assert (t.view(np.uint32) == r_t.view(np.uint32)).all(), f"{name}: t differs"
@@ -50,15 +55,13 @@ def test_closest_hit_ids_bit_exact(loaded, ctx):
 
 def test_shadow_bit_exact(loaded, ctx):
     name, sc, scene = loaded
-    if not ref.available():
-        pytest.skip("reference harness not built")
     ctx.upload(scene)
     rays = _ray_set(scene, 10000)
     li_all, lo_all = scene.light_instances, scene.light_objects
     pick = np.random.default_rng(5).integers(0, len(li_all), size=rays.shape[0])
     li, lo = li_all[pick], lo_all[pick]
     occ = ctx.trace_shadow(rays, li, lo)
-    r_occ = ref.RefScene(sc.lrd).shadow(rays, li, lo)
+    r_occ = ref.RefScene(sc.lrd).shadow(rays, li, lo) if ref.available() else port.shadow(scene, rays, li, lo)
     assert (occ == r_occ).all(), f"{name}: occlusion differs at {np.flatnonzero(occ != r_occ)[:10]}"
 
 
