@@ -271,11 +271,13 @@ typedef struct lambda_render_stats {
 lambda_status lambda_get_render_stats(const lambda_ctx *ctx, lambda_render_stats *stats);
 
 /* Per-stage device time of the last render made with LAMBDA_RENDER_PROFILE_STAGES.
- * Stages: 0 init, 1 wave prologue, 2 raygen, 3 intersect, 4 shade, 5 shadow,
- * 6 finish, 7 thin-film surrogate eval, 8 thin-film scatter. items = paths or rays
- * the stage processed over the whole render. No reference counterpart (the
- * reference's single kernel has no stages). */
-#define LAMBDA_NUM_STAGES 9
+ * Stages: 0 init, 1 wave prologue, 2 raygen, 3 intersect, 4 Lambertian shade,
+ * 5 mirror/dielectric shade, 6 thin-film shade (exact), 7 shadow rays, 8 finish,
+ * 9 thin-film surrogate inputs, 10 thin-film surrogate MLP (tensor cores),
+ * 11 thin-film surrogate scatter. items = paths or rays the stage processed over
+ * the whole render. No reference counterpart (the reference's single kernel has
+ * no stages). */
+#define LAMBDA_NUM_STAGES 12
 typedef struct lambda_stage_time {
     double ms;
     int64_t launches;
@@ -368,6 +370,14 @@ lambda_status lambda_surrogate_get(const lambda_ctx *ctx, float *params, lambda_
 
 /* Surrogate inference on the tensor cores: out [n][4] = (R_s, R_p, T_s, T_p). */
 lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, float *out);
+
+/* One forward/backward of the training kernel on caller data, for gradient
+ * checks: params [LAMBDA_MLP_PARAMS], x [n][5] inputs already normalised to
+ * [-1, 1], y [n][4] targets (host memory, n <= 65536). Writes the mean squared
+ * error over the 4 outputs and its gradient with respect to params. The forward
+ * pass rounds weights, inputs and hidden activations to BF16 as inference does. */
+lambda_status lambda_surrogate_grad(lambda_ctx *ctx, const float *params, const float *x, const float *y, int32_t n,
+                                    float *grad_out, float *loss_out);
 
 #ifdef __cplusplus
 }

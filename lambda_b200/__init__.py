@@ -338,9 +338,11 @@ def default_film_range() -> N.FilmRange:
 # structure-of-arrays words the stage must read and write (queue ids included),
 # not counting scene data, which is read-only and cache resident for small scenes.
 STAGE_BYTES = {
-    "raygen": 16 + 16 + 16 + 8 * 2 + 16 * 2 + 16 * 5 + 4,   # film rw, radiance r, lam rw, rng rw, ray/T/L writes, queue
-    "intersect": 4 + 32 + 48,                              # queue id, ray read, hit write
-    "shade": 4 + 32 + 48 + 16 * 3 + 8 * 2 + 32 + 4,        # queue, ray, hit, T/L/lam, rng rw, new ray, push
+    "raygen": 16 * 2 + 16 * 2 + 16 + 8 * 2 + 16 * 4 + 4,   # film rw, radiance rw, lam w, rng rw, ray/T w, queue
+    "intersect": 4 + 32 + 48 + 4,                          # queue id, ray read, hit write, material push
+    "shade_lambert": 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 64 + 8,  # queue, dir, hit, T/lam, rng rw, ray w, T w, NEE w, pushes
+    "shade_specular": 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
+    "shade_film": 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
     "shadow": 4 + 16 * 3 + 8 + 16 * 2,                     # queue, NEE ray + weights, light ids, radiance rw
     "finish": 16 * 3 + 12,
 }
@@ -364,7 +366,7 @@ def stage_profile(ctx: "Context", desc, out) -> dict:
 def roofline(stages: dict, hbm_gbs: float, bf16_tflops: float, peak_kind: str) -> dict:
     """Roofline entry for the stage with the largest device time."""
     name, s = max(((k, v) for k, v in stages.items() if v["ms"] > 0), key=lambda kv: kv[1]["ms"])
-    if name == "thinfilm_mlp":
+    if name == "film_mlp":
         flops = 17536.0 * s["items"] * 4  # 2*(5*64+64*64+64*64+64*4) per (hit, wavelength)
         achieved = flops / (s["ms"] / 1000.0) / 1e12
         return {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": bf16_tflops, "unit": "TFLOP/s",

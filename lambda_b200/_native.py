@@ -36,9 +36,9 @@ RENDER_THINFILM_EXACT = 0
 RENDER_THINFILM_SURROGATE = 1
 RENDER_OUTPUT_DEVICE = 2
 RENDER_PROFILE_STAGES = 4
-NUM_STAGES = 9
-STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade", "shadow", "finish", "thinfilm_mlp",
-               "thinfilm_scatter")
+NUM_STAGES = 12
+STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
+               "shadow", "finish", "film_inputs", "film_mlp", "film_scatter")
 
 
 class LambdaError(RuntimeError):
@@ -157,6 +157,7 @@ _SIGNATURES = {
     "lambda_surrogate_set": (C.c_int, [_P, _P, C.POINTER(FilmRange)]),
     "lambda_surrogate_get": (C.c_int, [_P, _P, C.POINTER(FilmRange)]),
     "lambda_surrogate_eval": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "lambda_surrogate_grad": (C.c_int, [_P, _P, _P, _P, C.c_int32, _P, _P]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

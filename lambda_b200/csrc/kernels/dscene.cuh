@@ -121,17 +121,35 @@ __device__ __forceinline__ f3 worley_feature(const DeviceScene &s, int cx, int c
               fract(float(sin(double(d))) * 43758.5453f));
 }
 
-// F1 Worley distance over the 27 neighbouring cells (utils.h:154-171).
+// F1 Worley distance over the 27 neighbouring cells (utils.h:154-171). The
+// minimum does not depend on visit order, so cells are visited nearest first and
+// a cell is skipped when every point of its box [c, c+1]^3 (where its feature
+// lies) is farther than the best distance so far, with a relative margin that
+// covers float rounding: the result equals the full 27-cell minimum.
+// Neighbour offsets ordered by |xo| + |yo| + |zo|, packed as (xo+1) | (yo+1) << 2 | (zo+1) << 4.
+__constant__ unsigned char kWorleyOrder[27] = {
+    0x15, 0x14, 0x16, 0x11, 0x19, 0x05, 0x25, 0x10, 0x18, 0x12, 0x1a, 0x04, 0x24, 0x06,
+    0x26, 0x01, 0x21, 0x09, 0x29, 0x00, 0x20, 0x08, 0x28, 0x02, 0x22, 0x0a, 0x2a};
+
 __device__ inline float worley_noise(const DeviceScene &s, f3 p) {
     const int xi = int(floorf(p.x)), yi = int(floorf(p.y)), zi = int(floorf(p.z));
     float distance = 9999;
-    for (int xo = -1; xo <= 1; xo++)
-        for (int yo = -1; yo <= 1; yo++)
-            for (int zo = -1; zo <= 1; zo++) {
-                const f3 cell = mk(float(xi + xo), float(yi + yo), float(zi + zo));
-                const f3 feature = worley_feature(s, xi + xo, yi + yo, zi + zo) + cell;
-                distance = fminf(distance, length(p - feature));
-            }
+    const float fx = p.x - float(xi), fy = p.y - float(yi), fz = p.z - float(zi);
+#pragma unroll 1
+    for (int c = 0; c < 27; c++) {
+        const int code = kWorleyOrder[c];
+        const int xo = (code & 3) - 1, yo = ((code >> 2) & 3) - 1, zo = ((code >> 4) & 3) - 1;
+        if (c > 0) {
+            const float gx = xo < 0 ? fx : (xo > 0 ? 1 - fx : 0);
+            const float gy = yo < 0 ? fy : (yo > 0 ? 1 - fy : 0);
+            const float gz = zo < 0 ? fz : (zo > 0 ? 1 - fz : 0);
+            const float lb2 = gx * gx + gy * gy + gz * gz;
+            if (lb2 > distance * distance * 1.0001f + 1e-6f) continue;
+        }
+        const f3 cell = mk(float(xi + xo), float(yi + yo), float(zi + zo));
+        const f3 feature = worley_feature(s, xi + xo, yi + yo, zi + zo) + cell;
+        distance = fminf(distance, length(p - feature));
+    }
     return distance;
 }
 
@@ -360,15 +378,54 @@ __device__ __forceinline__ void prim_attributes(const DeviceScene &s, int obj, c
     if (!h.front) h.normal = h.normal * -1.0f;
 }
 
+// Traversal stacks: 20 entries each (BVH_MAX_DEPTH, constants.h:10; the build
+// stops at depth 20, so a depth-first walk never holds more). LocalStack lives in
+// per-thread local memory; SharedStack is a slice of shared memory laid out
+// entry-major (entry i of thread t at base[i * stride + t]) so a warp's pushes
+// and pops hit 32 different banks.
+struct LocalStack {
+    int a[kStackDepth];
+    __device__ __forceinline__ int &operator[](int i) { return a[i]; }
+};
+struct SharedStack {
+    int *base;
+    int stride;
+    __device__ __forceinline__ int &operator[](int i) { return base[i * stride]; }
+};
+
+// World -> instance space (instance.h:50-52). An identity instance's transform
+// reduces exactly to adding +0 (which only turns -0 into +0), so it is done that way.
+__device__ __forceinline__ Ray3 to_local(const DeviceScene &s, int inst, const InstanceRef &ir, f3 o, f3 d) {
+    if (s.instance_flags[inst] & 1u) return make_ray(o + mk(0.0f, 0.0f, 0.0f), d + mk(0.0f, 0.0f, 0.0f));
+    float mi[16];
+    ir.load_m(mi, 1);
+    return make_ray(xform(mi, o, 1), xform(mi, d, 0));
+}
+
+// Instance space -> world for a hit (instance.h:42, :48).
+__device__ __forceinline__ void to_world(const DeviceScene &s, int inst, const InstanceRef &ir, Hit &h) {
+    if (s.instance_flags[inst] & 1u) {
+        h.normal = normalize(h.normal + mk(0.0f, 0.0f, 0.0f));
+        h.point = h.point + mk(0.0f, 0.0f, 0.0f);
+        return;
+    }
+    float m[16];
+    ir.load_m(m, 1);
+    h.normal = normalize(xform_t(m, h.normal, 0));
+    ir.load_m(m, 0);
+    h.point = xform(m, h.point, 1);
+}
+
 // Scene::hit in closest-hit mode (scene.h:51-124): two-level depth-first
-// traversal with 20-entry stacks, right child popped first, a TLAS leaf tests
-// only its first instance (scene.h:80), candidates accepted when t < best.
-// Returns false on a miss. `overflow` is set if a stack would overflow.
-__device__ inline bool closest_hit(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow) {
+// traversal, right child popped first, a TLAS leaf tests only its first instance
+// (scene.h:80), candidates accepted when t < best. Returns false on a miss.
+// `overflow` is set if a stack would overflow.
+template <class Stack>
+__device__ __forceinline__ bool closest_hit_t(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow, Stack stack,
+                                              Stack sub) {
     const Ray3 wr = make_ray(o, d);
     float best = kMax;
     int best_obj = -1, best_inst = -1;
-    int stack[kStackDepth];
     int sp = 0;
     stack[sp++] = 0;
     while (sp > 0) {
@@ -381,10 +438,7 @@ __device__ inline bool closest_hit(const DeviceScene &s, f3 o, f3 d, Hit &h, boo
             const int inst = __float_as_int(lo.w);
             const InstanceRef ir = instance_ref(s, inst);
             const int4 hd = ir.header();
-            float mi[16];
-            ir.load_m(mi, 1);
-            const Ray3 lr = make_ray(xform(mi, o, 1), xform(mi, d, 0));
-            int sub[kStackDepth];
+            const Ray3 lr = to_local(s, inst, ir, o, d);
             int ssp = 0;
             sub[ssp++] = hd.z;
             while (ssp > 0) {
@@ -427,17 +481,17 @@ __device__ inline bool closest_hit(const DeviceScene &s, f3 o, f3 d, Hit &h, boo
         return false;
     }
     const InstanceRef ir = instance_ref(s, best_inst);
-    float m[16];
-    ir.load_m(m, 1);
-    const f3 lo_ = xform(m, o, 1), ld = xform(m, d, 0);
-    prim_attributes(s, best_obj, load_prim(s, best_obj), lo_, ld, best, h);
+    const Ray3 lr = to_local(s, best_inst, ir, o, d);
+    prim_attributes(s, best_obj, load_prim(s, best_obj), lr.o, lr.d, best, h);
     h.instance = best_inst;
     h.object = best_obj;
-    // instance space -> world (instance.h:42, :48); m still holds M^-1
-    h.normal = normalize(xform_t(m, h.normal, 0));
-    ir.load_m(m, 0);
-    h.point = xform(m, h.point, 1);
+    to_world(s, best_inst, ir, h);
     return true;
+}
+
+__device__ inline bool closest_hit(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow) {
+    LocalStack a, b;
+    return closest_hit_t<LocalStack &>(s, o, d, h, overflow, a, b);
 }
 
 // Scene::hit in shadow mode (scene.h:51-124 with occludedInstance/Object): for a
@@ -445,26 +499,23 @@ __device__ inline bool closest_hit(const DeviceScene &s, f3 o, f3 d, Hit &h, boo
 // occluded), then any primitive other than the light closer than it occludes.
 // For the background light (-1, -1), any hit occludes. On a visible light,
 // `light` holds the light's hit record for its emission lookup.
-__device__ inline bool occluded(const DeviceScene &s, f3 o, f3 d, int light_inst, int light_obj, Hit &light, bool &overflow) {
+template <class Stack>
+__device__ __forceinline__ bool occluded_t(const DeviceScene &s, f3 o, f3 d, int light_inst, int light_obj, Hit &light,
+                                           bool &overflow, Stack stack, Stack sub) {
     const Ray3 wr = make_ray(o, d);
     float best = kMax;
     if (light_inst != -1) {
         const InstanceRef ir = instance_ref(s, light_inst);
-        float m[16];
-        ir.load_m(m, 1);
-        const f3 lo = xform(m, o, 1), ld = xform(m, d, 0);
+        const Ray3 lr = to_local(s, light_inst, ir, o, d);
         const Prim p = load_prim(s, light_obj);
-        const float t = intersect_t(p, make_ray(lo, ld), kMax);
+        const float t = intersect_t(p, lr, kMax);
         if (t < 0) return true;
-        prim_attributes(s, light_obj, p, lo, ld, t, light);
+        prim_attributes(s, light_obj, p, lr.o, lr.d, t, light);
         light.instance = light_inst;
         light.object = light_obj;
-        light.normal = normalize(xform_t(m, light.normal, 0));
-        ir.load_m(m, 0);
-        light.point = xform(m, light.point, 1);
+        to_world(s, light_inst, ir, light);
         best = t;
     }
-    int stack[kStackDepth];
     int sp = 0;
     stack[sp++] = 0;
     while (sp > 0) {
@@ -477,10 +528,7 @@ __device__ inline bool occluded(const DeviceScene &s, f3 o, f3 d, int light_inst
             const int inst = __float_as_int(lo.w);
             const InstanceRef ir = instance_ref(s, inst);
             const int4 hd = ir.header();
-            float mi[16];
-            ir.load_m(mi, 1);
-            const Ray3 lr = make_ray(xform(mi, o, 1), xform(mi, d, 0));
-            int sub[kStackDepth];
+            const Ray3 lr = to_local(s, inst, ir, o, d);
             int ssp = 0;
             sub[ssp++] = hd.z;
             while (ssp > 0) {
@@ -513,6 +561,19 @@ __device__ inline bool occluded(const DeviceScene &s, f3 o, f3 d, int light_inst
         }
     }
     return false;
+}
+
+__device__ inline bool occluded(const DeviceScene &s, f3 o, f3 d, int light_inst, int light_obj, Hit &light,
+                                bool &overflow) {
+    LocalStack a, b;
+    return occluded_t<LocalStack &>(s, o, d, light_inst, light_obj, light, overflow, a, b);
+}
+
+// Shared-memory stacks of one thread: 2 * kStackDepth ints per thread, entry-major.
+constexpr int kStackSmemPerThread = 2 * kStackDepth * 4;
+__device__ __forceinline__ void thread_stacks(int *smem, SharedStack &a, SharedStack &b) {
+    a = SharedStack{smem + threadIdx.x, int(blockDim.x)};
+    b = SharedStack{smem + kStackDepth * blockDim.x + threadIdx.x, int(blockDim.x)};
 }
 
 // ---------------------------------------------------------------------------

@@ -28,6 +28,7 @@ struct DeviceScene {
     const float *light_power;
     const float *light_cdf;      // running sums of light_power in list order
     const float *material_emission;  // per material: average emission (0 if not emissive)
+    const uint32_t *instance_flags;  // bit 0: transform and inverse are exactly the identity
     const float *cie;            // [471][3] as float
     const int *perm;             // [256]
     const float4 *worley_cells;  // feature offsets of lattice cells (xyz), cell-major
@@ -39,6 +40,7 @@ struct DeviceScene {
     int num_lights;
     float total_light_power;
     int background_texture;
+    uint32_t families;           // bit f set when some material of family f exists (0 Lambertian, 1 specular, 2 thin film)
 };
 
 struct RenderParams {
@@ -65,11 +67,16 @@ struct PathState {
     float4 *sh_a;         // throughput * BSDF * cos
     int2 *sh_light;       // light (instance, object)
     int *queue[2];        // active pixel ids, ping-pong by bounce parity
+    int *mat_queue[3];    // this bounce's Lambertian, mirror/dielectric and thin-film hits
     int *shadow_queue;    // pixel ids with a pending NEE ray
-    int *counts;          // [2 * (depth + 2)]: active paths per bounce, then NEE rays per bounce
+    int *counts;          // [kQueues * (depth + 2)], see queue_slot()
     int *wave;            // [2]: wave to run next, wave being run
     unsigned long long *stats;  // segments, shadow rays, thin-film hits
     int *error;           // bit 0: traversal stack overflow
 };
+
+// Counters per bounce: paths to trace, then the three material queues, then NEE rays.
+enum : int { kQActive = 0, kQLambert = 1, kQSpecular = 2, kQFilm = 3, kQShadow = 4, kQueues = 5 };
+__host__ __device__ inline int queue_slot(int bounce, int q) { return bounce * kQueues + q; }
 
 }  // namespace lambda_dev

@@ -411,6 +411,21 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     CK(b.cie.upload(cie.data(), cie.size() * sizeof(float), s), "upload CIE table");
     CK(b.perm.upload(kPerlinPermutation, sizeof(kPerlinPermutation), s), "upload permutation");
     CK(b.worley.upload(worley.data(), worley.size() * sizeof(float4), s), "upload Worley lattice");
+    std::vector<uint32_t> iflags(d.num_instances, 0);
+    for (int i = 0; i < d.num_instances; i++) {
+        bool ident = true;
+        for (int k = 0; k < 16; k++) {
+            const float e = (k % 5 == 0) ? 1.0f : 0.0f;
+            ident = ident && d.instances[i].transform[k] == e && d.instances[i].inverse_transform[k] == e;
+        }
+        iflags[i] = ident ? 1u : 0u;
+    }
+    CK(b.instance_flags.upload(iflags.data(), iflags.size() * sizeof(uint32_t), s), "upload instances");
+    uint32_t families = 0;
+    for (int i = 0; i < d.num_materials; i++) {
+        const int t = d.materials[i].type;
+        families |= t == LAMBDA_MATERIAL_LAMBERTIAN ? 1u : (t == LAMBDA_MATERIAL_THINFILM ? 4u : (t == LAMBDA_MATERIAL_EMISSIVE ? 0u : 2u));
+    }
     CK(cudaStreamSynchronize(s), "scene upload");
 
     DeviceScene &ds = ctx->dscene;
@@ -431,6 +446,8 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     ds.light_power = b.light_power.as<float>();
     ds.light_cdf = b.light_cdf.as<float>();
     ds.material_emission = b.material_emission.as<float>();
+    ds.instance_flags = b.instance_flags.as<uint32_t>();
+    ds.families = families;
     ds.cie = b.cie.as<float>();
     ds.perm = b.perm.as<int>();
     ds.worley_cells = b.worley.as<float4>();
@@ -533,7 +550,10 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     CK(r.q0.reserve(P * 4), "allocate queues");
     CK(r.q1.reserve(P * 4), "allocate queues");
     CK(r.qs.reserve(P * 4), "allocate queues");
-    CK(r.counts.reserve(size_t(2 * (depth + 2)) * 4), "allocate queues");
+    CK(r.qm0.reserve(P * 4), "allocate queues");
+    CK(r.qm1.reserve(P * 4), "allocate queues");
+    CK(r.qm2.reserve(P * 4), "allocate queues");
+    CK(r.counts.reserve(size_t(kQueues * (depth + 2)) * 4), "allocate queues");
     CK(r.wave.reserve(16), "allocate queues");
     CK(r.stats.reserve(8 * 8), "allocate statistics");
     CK(r.error.reserve(16), "allocate flags");
@@ -556,6 +576,9 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     ps.queue[0] = r.q0.as<int>();
     ps.queue[1] = r.q1.as<int>();
     ps.shadow_queue = r.qs.as<int>();
+    ps.mat_queue[0] = r.qm0.as<int>();
+    ps.mat_queue[1] = r.qm1.as<int>();
+    ps.mat_queue[2] = r.qm2.as<int>();
     ps.counts = r.counts.as<int>();
     ps.wave = r.wave.as<int>();
     ps.stats = r.stats.as<unsigned long long>();
@@ -602,17 +625,21 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
 
     lambda_status s = ctx->ensure_state(rp.num_pixels, rp.depth);
     if (s != LAMBDA_OK) return s;
+    if (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) {
+        s = ctx->ensure_surrogate_state(rp.num_pixels);
+        if (s != LAMBDA_OK) return s;
+    }
     cudaStream_t stream = ctx->stream;
     const PathState ps = ctx->pstate;
     const DeviceScene sc = ctx->dscene;
     const int P = rp.num_pixels;
     const int pix_blocks = (P + 255) / 256;
-    const int qgrid = std::min(pix_blocks, grid_for(ctx->sm_count, (const void *)k_shade, 256));
+    const int qgrid = std::min(pix_blocks, grid_for(ctx->sm_count, (const void *)k_shade_lambert, 256));
     const bool surrogate = (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) != 0;
 
     CK(cudaMemsetAsync(ps.stats, 0, 8 * 8, stream), "clear statistics");
     CK(cudaMemsetAsync(ps.error, 0, 16, stream), "clear flags");
-    CK(cudaMemsetAsync(ps.counts, 0, size_t(2 * (rp.depth + 2)) * 4, stream), "clear counters");
+    CK(cudaMemsetAsync(ps.counts, 0, size_t(kQueues * (rp.depth + 2)) * 4, stream), "clear counters");
     CK(cudaEventRecord(ctx->ev_start, stream), "event");
     k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps);
     CK(cudaGetLastError(), "launch init");
@@ -631,11 +658,16 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
         };
         timed(1, [&] { k_wave_prologue<<<1, 256, 0, stream>>>(rp.depth, ps); });
         timed(2, [&] { k_raygen<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
+        const size_t stack_smem = size_t(256) * kStackSmemPerThread;
         for (int b = 0; b <= rp.depth; b++) {
-            timed(3, [&] { k_intersect<<<qgrid, 256, 0, stream>>>(b, sc, ps); });
-            if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, qgrid, pr);
-            else timed(4, [&] { k_shade<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
-            timed(5, [&] { k_shadow<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+            timed(3, [&] { k_intersect<<<qgrid, 256, stack_smem, stream>>>(b, rp, sc, ps); });
+            if (sc.families & 1u) timed(4, [&] { k_shade_lambert<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+            if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+            if (sc.families & 4u) {
+                if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, qgrid, pr);
+                else timed(6, [&] { k_shade_film_exact<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+            }
+            if (sc.families & 1u) timed(7, [&] { k_shadow<<<qgrid, 256, stack_smem, stream>>>(b, rp, sc, ps); });
         }
         return n;
     };
@@ -703,16 +735,19 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
             ctx->stage_times[i].launches = prof.counts[i];
         }
         ctx->stage_times[0].launches = 1;
+        ctx->stage_times[0].items = P;
         ctx->stage_times[1].items = rp.samples;
         ctx->stage_times[2].items = int64_t(P) * rp.samples;
         ctx->stage_times[3].items = ctx->stats.segments;
-        ctx->stage_times[4].items = ctx->stats.segments;
-        ctx->stage_times[5].items = ctx->stats.shadow_rays;
-        ctx->stage_times[6].items = P;
-        ctx->stage_times[7].items = ctx->stats.thinfilm_hits;
-        ctx->stage_times[8].items = ctx->stats.thinfilm_hits;
+        ctx->stage_times[4].items = int64_t(stats[4]);
+        ctx->stage_times[5].items = int64_t(stats[5]);
+        ctx->stage_times[6].items = surrogate ? 0 : ctx->stats.thinfilm_hits;
+        ctx->stage_times[7].items = ctx->stats.shadow_rays;
+        ctx->stage_times[8].items = P;
+        for (int k = 9; k < 12; k++) ctx->stage_times[k].items = surrogate ? ctx->stats.thinfilm_hits : 0;
     }
     if (err[0] & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
+    if (err[0] & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
     return LAMBDA_OK;
 }
 

@@ -39,12 +39,12 @@ struct StageProfiler {
 struct SceneBuffers {
     DeviceBuffer nodes, prims, tri, instances, spectra, spectrum_flat, cspectra, cspectrum_flat, materials,
         material_props, scalar_tex, spectrum_tex, light_inst, light_obj, light_power, light_cdf, material_emission,
-        cie, perm, worley;
+        cie, perm, worley, instance_flags;
 };
 
 struct RenderBuffers {
     DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
-        q0, q1, qs, counts, wave, stats, error, out;
+        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out;
     // thin-film surrogate batch
     DeviceBuffer tf_queue, tf_in, tf_out;
 };
@@ -84,6 +84,7 @@ struct lambda_ctx {
     lambda_status cuda_fail(cudaError_t e, const char *what);
     lambda_status ensure_state(int pixels, int depth);
     lambda_status surrogate_ready();
+    lambda_status ensure_surrogate_state(int pixels);
     int launch_shade_surrogate(int bounce, const lambda_dev::RenderParams &rp, const lambda_dev::DeviceScene &sc,
                                const lambda_dev::PathState &ps, int grid, StageProfiler *prof);
 
@@ -92,9 +93,9 @@ struct lambda_ctx {
         RenderBuffers &r = rbuf;
         return {&s.nodes, &s.prims, &s.tri, &s.instances, &s.spectra, &s.spectrum_flat, &s.cspectra,
                 &s.cspectrum_flat, &s.materials, &s.material_props, &s.scalar_tex, &s.spectrum_tex, &s.light_inst,
-                &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley,
+                &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
-                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.counts, &r.wave,
+                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
                 &r.stats, &r.error, &r.out, &r.tf_queue, &r.tf_in, &r.tf_out, &sbuf.weights_bf16,
                 &sbuf.weights_f32, &sbuf.scratch};
     }

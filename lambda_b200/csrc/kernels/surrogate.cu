@@ -1,35 +1,891 @@
-// Thin-film surrogate MLP: training, weight install, tensor-core inference.
+// Thin-film surrogate: a 5 -> 64 -> 64 -> 64 -> 4 MLP (ReLU hidden layers) that maps
+// (lambda, cos theta, thickness, n_film, n_substrate) of a single film between air
+// and a substrate to (R_s, R_p, T_s, T_p), standing in for the transfer matrix of
+// Material::thinFilmReflectance (src/scene/material.h:263-309).
+//
+//   k_film_labels    training/audit data: uniform samples of the input box, labelled
+//                    by the FP64 transfer matrix (tmm.cuh)
+//   k_train_step     forward + backward of a minibatch on CUDA cores, forward rounded
+//                    to BF16 exactly as inference rounds it; per-CTA gradients are
+//                    summed with atomics
+//   k_adam           Adam update of the FP32 master weights
+//   k_mlp_tc         inference on the 5th-generation tensor cores: persistent CTAs of
+//                    4 warps, BF16 weights resident in shared memory (canonical K-major
+//                    layout, no swizzle), tcgen05.mma with FP32 accumulators in tensor
+//                    memory, tcgen05.ld epilogues (bias, ReLU, BF16) writing the next
+//                    layer's operand back to shared memory
+// In a render, thin-film hits are turned into four MLP rows each (one per hero
+// wavelength) by k_film_inputs, evaluated by k_mlp_tc, and consumed by
+// k_film_scatter; hits outside the trained domain take the exact FP32 path.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
 
 #include "engine.h"
 #include "lambda_gpu.h"
+#define LAMBDA_WAVEFRONT_HELPERS_ONLY
+#include "wavefront.cuh"
+
+using namespace lambda_dev;
+
+namespace mlp {
+
+constexpr int kIn = LAMBDA_MLP_IN, kH = LAMBDA_MLP_HIDDEN, kOut = LAMBDA_MLP_OUT;
+constexpr int kInPad = 16;   // K of layer 1 (bf16 MMA K = 16)
+constexpr int kOutPad = 16;  // N of layer 4 (M = 128 needs N % 16 == 0)
+constexpr int kParams = LAMBDA_MLP_PARAMS;
+// parameter offsets (row-major out x in)
+constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH * kH;
+constexpr int oW4 = oB3 + kH, oB4 = oW4 + kOut * kH;
+static_assert(oB4 + kOut == kParams, "parameter layout");
+
+constexpr int kTileM = 128;  // rows per MMA tile (TMEM lanes)
+constexpr int kRowStride = 8;  // floats per input row in the staging buffer
+
+// Byte offset of element (r, k) of a K-major bf16 operand with K columns, stored as
+// 8x8 core matrices (8 rows x 16 bytes, 128 contiguous bytes): core (r/8, k/8) at
+// ((r/8) * (K/8) + k/8) * 128. Consecutive core matrices along K are 128 bytes apart
+// (LBO), along M/N (K/8)*128 bytes apart (SBO).
+__host__ __device__ constexpr int core_offset(int r, int k, int K) {
+    return ((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// Shared-memory layout of k_mlp_tc (bytes).
+constexpr int sW1 = 0;                         // [64][16]
+constexpr int sW2 = sW1 + kH * kInPad * 2;     // [64][64]
+constexpr int sW3 = sW2 + kH * kH * 2;         // [64][64]
+constexpr int sW4 = sW3 + kH * kH * 2;         // [16][64]
+constexpr int sX = sW4 + kOutPad * kH * 2;     // [128][16]
+constexpr int sHid = sX + kTileM * kInPad * 2;  // [128][64]
+constexpr int sBias = sHid + kTileM * kH * 2;   // f32: b1[64] b2[64] b3[64] b4[16]
+constexpr int sBar = sBias + (3 * kH + kOutPad) * 4;
+constexpr int sTmem = sBar + 8;
+constexpr int kSmemBytes = sTmem + 8;
+constexpr int kPackedWeightBytes = sX;  // W1..W4 in their shared-memory layout
+constexpr int kTmemCols = 64;
+
+// Input normalisation to [-1, 1] over the trained box.
+struct Range {
+    float lo[kIn], hi[kIn];
+};
+
+__host__ __device__ inline float normalise(float v, float lo, float hi) { return 2.0f * (v - lo) / (hi - lo) - 1.0f; }
+
+__device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// ---------------------------------------------------------------------------
+// tcgen05 / mbarrier primitives (PTX ISA 8.7+, sm_100a)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor: start, leading-dimension (K) and stride (M/N)
+// byte offsets in 16-byte units, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M = 128.
+__host__ __device__ constexpr uint32_t instr_desc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(kTileM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Waits for phase `parity` of an mbarrier; gives up after `limit` polls and reports false.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core inference
+// ---------------------------------------------------------------------------
+
+// Writes 8 consecutive bf16 values (k = c*8 .. c*8+7 of row r) of a K-major operand.
+__device__ __forceinline__ void put8(uint8_t *smem, int base, int r, int c, int K, const float *v) {
+    __nv_bfloat162 p[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) p[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    *reinterpret_cast<uint4 *>(smem + base + core_offset(r, c * 8, K)) = *reinterpret_cast<uint4 *>(p);
+}
+
+// in: rows x kRowStride floats (normalised inputs); out: rows x 4 floats.
+// error bit 1 is set if an MMA completion wait timed out.
+__global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed, const float *__restrict__ bias,
+                                                const float *__restrict__ in, const int *__restrict__ row_count,
+                                                int row_multiplier, int rows_fixed, float4 *__restrict__ out,
+                                                int *error) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int rows = row_count ? (*row_count) * row_multiplier : rows_fixed;
+    const int tiles = (rows + kTileM - 1) / kTileM;
+    if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
+
+    // weights and biases once per CTA
+    for (int i = tid; i < kPackedWeightBytes / 16; i += blockDim.x) reinterpret_cast<uint4 *>(smem)[i] = packed[i];
+    float *sb = reinterpret_cast<float *>(smem + sBias);
+    for (int i = tid; i < 3 * kH + kOutPad; i += blockDim.x) sb[i] = bias[i];
+    const uint32_t bar = smem_u32(smem + sBar);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + sTmem);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_proxy_async();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = tmem + (uint32_t(warp * 32) << 16);
+    const uint32_t base = smem_u32(smem);
+    const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
+    uint32_t phase = 0;
+    bool ok = true;
+    const uint32_t kPoll = 1u << 22;
+
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const int r = warp * 32 + lane;  // this thread's row (its TMEM lane)
+        const int row = tile * kTileM + r;
+        // ---- layer 1 operand: normalised inputs, bf16, padded to K = 16
+        {
+            float x[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) x[i] = 0.0f;
+            if (row < rows) {
+                const float4 a = *reinterpret_cast<const float4 *>(in + size_t(row) * kRowStride);
+                const float b = in[size_t(row) * kRowStride + 4];
+                x[0] = a.x;
+                x[1] = a.y;
+                x[2] = a.z;
+                x[3] = a.w;
+                x[4] = b;
+            }
+            put8(smem, sX, r, 0, kInPad, x);
+            put8(smem, sX, r, 1, kInPad, x + 8);
+        }
+        // ---- four layers
+#pragma unroll 1
+        for (int layer = 0; layer < 4; layer++) {
+            fence_proxy_async();
+            fence_before();
+            __syncthreads();
+            if (tid == 0) {
+                fence_after();
+                if (layer == 0) {
+                    mma_bf16(tmem, smem_desc(base + sX, 128, 256), smem_desc(base + sW1, 128, 256), id64, 0);
+                } else {
+                    const int wofs = layer == 1 ? sW2 : (layer == 2 ? sW3 : sW4);
+                    const uint32_t idesc = layer == 3 ? id16 : id64;
+#pragma unroll
+                    for (int kk = 0; kk < kH / 16; kk++)
+                        mma_bf16(tmem, smem_desc(base + sHid + kk * 256, 128, 1024),
+                                 smem_desc(base + wofs + kk * 256, 128, 1024), idesc, kk > 0);
+                }
+                mma_commit(bar);
+            }
+            ok = mbar_wait(bar, phase, kPoll);
+            phase ^= 1u;
+            fence_after();
+            if (!ok) break;
+            if (layer < 3) {
+                const float *bl = sb + layer * kH;
+#pragma unroll
+                for (int c = 0; c < kH / 16; c++) {
+                    float v[16];
+                    tmem_ld16(lane_base + c * 16, v);
+#pragma unroll
+                    for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + bl[c * 16 + i], 0.0f);
+                    put8(smem, sHid, r, 2 * c, kH, v);
+                    put8(smem, sHid, r, 2 * c + 1, kH, v + 8);
+                }
+            } else {
+                float v[16];
+                tmem_ld16(lane_base, v);
+                if (row < rows) {
+                    const float *b4 = sb + 3 * kH;
+                    out[row] = make_float4(v[0] + b4[0], v[1] + b4[1], v[2] + b4[2], v[3] + b4[3]);
+                }
+            }
+        }
+    }
+    if (!ok && tid == 0) atomicOr(error, 2);
+    // all TMEM reads are complete (tcgen05.ld waits) before the columns are released
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Training
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint64_t splitmix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ double uniform01(uint64_t seed, uint64_t i, int dim) {
+    return double(splitmix(seed ^ splitmix(i * 8 + uint64_t(dim))) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Uniform samples of the input box labelled by the FP64 transfer matrix.
+// x: [n][kRowStride] normalised inputs; y: [n][4] (R_s, R_p, T_s, T_p).
+__global__ void k_film_labels(uint64_t seed, int64_t first, int n, Range rg, float *x, float *y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float v[kIn];
+    for (int d = 0; d < kIn; d++)
+        v[d] = float(rg.lo[d] + (rg.hi[d] - rg.lo[d]) * uniform01(seed, uint64_t(first + i), d));
+    cx<double> idx[3] = {cx<double>{1.0, 0.0}, cx<double>{double(v[3]), 0.0}, cx<double>{double(v[4]), 0.0}};
+    const double d = v[2];
+    const FilmResult<double> r = film_stack<double, 1>(1, idx, &d, double(v[1]), double(v[0]));
+    for (int k = 0; k < kIn; k++) x[size_t(i) * kRowStride + k] = normalise(v[k], rg.lo[k], rg.hi[k]);
+    for (int k = kIn; k < kRowStride; k++) x[size_t(i) * kRowStride + k] = 0.0f;
+    y[size_t(i) * 4] = float(r.rs);
+    y[size_t(i) * 4 + 1] = float(r.rp);
+    y[size_t(i) * 4 + 2] = float(r.ts);
+    y[size_t(i) * 4 + 3] = float(r.tp);
+}
+
+constexpr int kTrainRows = 64;
+constexpr int kTrainThreads = 256;
+// shared memory of k_train_step (floats)
+constexpr int tW = 0;                          // master weights rounded to bf16 (forward copy)
+constexpr int tX = tW + kParams;               // [64][5]
+constexpr int tH1 = tX + kTrainRows * kIn;     // [64][64]
+constexpr int tH2 = tH1 + kTrainRows * kH;
+constexpr int tH3 = tH2 + kTrainRows * kH;
+constexpr int tDY = tH3 + kTrainRows * kH;     // [64][4]
+constexpr int tDA = tDY + kTrainRows * kOut;   // [64][64]
+constexpr int tDB = tDA + kTrainRows * kH;
+constexpr int tLoss = tDB + kTrainRows * kH;
+constexpr int kTrainSmem = (tLoss + 8) * 4;
+
+// Dense layer on 64 rows: out[r][o] = act(sum_i in[r][i] * W[o][i] + b[o]), rounded to bf16.
+template <int NIN, int NOUT>
+__device__ __forceinline__ void fwd_layer(const float *W, const float *b, const float *in, float *out, bool relu) {
+    for (int e = threadIdx.x; e < kTrainRows * NOUT; e += blockDim.x) {
+        const int r = e / NOUT, o = e % NOUT;
+        float a = 0.0f;
+#pragma unroll 8
+        for (int i = 0; i < NIN; i++) a += in[r * NIN + i] * W[o * NIN + i];
+        a += b[o];
+        out[e] = relu ? bf16_round(fmaxf(a, 0.0f)) : a;
+    }
+}
+
+// grad W[o][i] += sum_r d[r][o] * in[r][i]; grad b[o] += sum_r d[r][o]
+template <int NIN, int NOUT>
+__device__ __forceinline__ void grad_w(const float *d, const float *in, float *gW, float *gb) {
+    for (int e = threadIdx.x; e < NOUT * NIN; e += blockDim.x) {
+        const int o = e / NIN, i = e % NIN;
+        float a = 0.0f;
+        for (int r = 0; r < kTrainRows; r++) a += d[r * NOUT + o] * in[r * NIN + i];
+        atomicAdd(&gW[e], a);
+    }
+    for (int o = threadIdx.x; o < NOUT; o += blockDim.x) {
+        float a = 0.0f;
+        for (int r = 0; r < kTrainRows; r++) a += d[r * NOUT + o];
+        atomicAdd(&gb[o], a);
+    }
+}
+
+// d_in[r][i] = (sum_o d[r][o] * W[o][i]) * (act[r][i] > 0)
+template <int NIN, int NOUT>
+__device__ __forceinline__ void back_act(const float *d, const float *W, const float *act, float *din) {
+    for (int e = threadIdx.x; e < kTrainRows * NIN; e += blockDim.x) {
+        const int r = e / NIN, i = e % NIN;
+        float a = 0.0f;
+#pragma unroll 8
+        for (int o = 0; o < NOUT; o++) a += d[r * NOUT + o] * W[o * NIN + i];
+        din[e] = act[e] > 0.0f ? a : 0.0f;
+    }
+}
+
+// One minibatch slice of 64 rows per CTA: forward (bf16-rounded like inference),
+// MSE loss over the 4 outputs, backward, gradients accumulated into `grad`.
+__global__ void __launch_bounds__(kTrainThreads) k_train_step(const float *params, const float *x, const float *y,
+                                                             int rows, float inv_count, float *grad, float *loss) {
+    extern __shared__ float ts[];
+    const int r0 = blockIdx.x * kTrainRows;
+    for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
+        const bool is_weight = !(i >= oB1 && i < oW2) && !(i >= oB2 && i < oW3) && !(i >= oB3 && i < oW4) && i < oB4;
+        ts[tW + i] = is_weight ? bf16_round(params[i]) : params[i];
+    }
+    for (int e = threadIdx.x; e < kTrainRows * kIn; e += blockDim.x) {
+        const int r = e / kIn, k = e % kIn;
+        ts[tX + e] = r0 + r < rows ? bf16_round(x[size_t(r0 + r) * kRowStride + k]) : 0.0f;
+    }
+    __syncthreads();
+    const float *W = ts + tW;
+    fwd_layer<kIn, kH>(W + oW1, W + oB1, ts + tX, ts + tH1, true);
+    __syncthreads();
+    fwd_layer<kH, kH>(W + oW2, W + oB2, ts + tH1, ts + tH2, true);
+    __syncthreads();
+    fwd_layer<kH, kH>(W + oW3, W + oB3, ts + tH2, ts + tH3, true);
+    __syncthreads();
+    // output layer, loss and its gradient
+    float lsum = 0.0f;
+    for (int e = threadIdx.x; e < kTrainRows * kOut; e += blockDim.x) {
+        const int r = e / kOut, o = e % kOut;
+        float a = W[oB4 + o];
+        for (int i = 0; i < kH; i++) a += ts[tH3 + r * kH + i] * W[oW4 + o * kH + i];
+        float dy = 0.0f;
+        if (r0 + r < rows) {
+            const float err = a - y[size_t(r0 + r) * 4 + o];
+            lsum += err * err * inv_count;
+            dy = 2.0f * err * inv_count;
+        }
+        ts[tDY + e] = dy;
+    }
+    atomicAdd(loss, lsum);
+    __syncthreads();
+    grad_w<kH, kOut>(ts + tDY, ts + tH3, grad + oW4, grad + oB4);
+    back_act<kH, kOut>(ts + tDY, W + oW4, ts + tH3, ts + tDA);
+    __syncthreads();
+    grad_w<kH, kH>(ts + tDA, ts + tH2, grad + oW3, grad + oB3);
+    back_act<kH, kH>(ts + tDA, W + oW3, ts + tH2, ts + tDB);
+    __syncthreads();
+    grad_w<kH, kH>(ts + tDB, ts + tH1, grad + oW2, grad + oB2);
+    back_act<kH, kH>(ts + tDB, W + oW2, ts + tH1, ts + tDA);
+    __syncthreads();
+    grad_w<kIn, kH>(ts + tDA, ts + tX, grad + oW1, grad + oB1);
+}
+
+__global__ void k_adam(float *p, float *g, float *m, float *v, int n, float lr, float b1, float b2, float eps, float c1,
+                       float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1 - b1) * gi;
+    const float vi = b2 * v[i] + (1 - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    g[i] = 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Render integration
+// ---------------------------------------------------------------------------
+
+struct FilmSurrogate {
+    Range rg;
+    float lam_lo, lam_hi, cos_lo, cos_hi, d_lo, d_hi, nf_lo, nf_hi, ns_lo, ns_hi;
+};
+
+// Writes four MLP rows per thin-film hit (one per hero wavelength) or marks the
+// hit for the exact path: the surrogate covers a single film with real indices
+// between air (index exactly 1) and a substrate, inside the trained box. Back-face
+// hits (light inside the substrate) are mapped to the equivalent incidence from air
+// by Snell's law, since a lossless stack reflects the same from both sides; total
+// internal reflection goes to the exact path.
+__global__ void __launch_bounds__(256) k_film_inputs(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
+                                                     FilmSurrogate fs, float *rows, int *fallback) {
+    const int n = ps.counts[queue_slot(bounce, kQFilm)];
+    const int stride = gridDim.x * blockDim.x;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
+        const int p = ps.mat_queue[2][idx];
+        const ShadeIn s = load_shade(ps, sc, p);
+        bool ok = s.m.y == 1;
+        float d = 0;
+        if (ok) {
+            d = scalar_texture(sc, sc.material_props[s.m.w], s.sp.point);
+            ok = d >= fs.d_lo && d <= fs.d_hi;
+        }
+        const float cos_in = dot(s.nrm, -s.d);
+        float nf[kHero], ns[kHero], c0[kHero];
+        for (int w = 0; w < kHero && ok; w++) {
+            const double2 a = cspectrum_at(sc, sc.material_props[s.m.z], s.lam.v[w]);
+            const double2 b = cspectrum_at(sc, sc.material_props[s.m.z + 1], s.lam.v[w]);
+            const double2 c = cspectrum_at(sc, sc.material_props[s.m.z + 2], s.lam.v[w]);
+            ok = a.x == 1.0 && a.y == 0.0 && b.y == 0.0 && c.y == 0.0;
+            nf[w] = float(b.x);
+            ns[w] = float(c.x);
+            if (s.front) {
+                c0[w] = cos_in;
+            } else {
+                const float sin2 = ns[w] * ns[w] * (1 - cos_in * cos_in);
+                ok = ok && sin2 < 1.0f;
+                c0[w] = sqrtf(fmaxf(1 - sin2, 0.0f));
+            }
+            ok = ok && nf[w] >= fs.nf_lo && nf[w] <= fs.nf_hi && ns[w] >= fs.ns_lo && ns[w] <= fs.ns_hi &&
+                 c0[w] >= fs.cos_lo && c0[w] <= fs.cos_hi && s.lam.v[w] >= fs.lam_lo && s.lam.v[w] <= fs.lam_hi;
+        }
+        fallback[idx] = ok ? 0 : 1;
+        if (!ok) atomicAdd(reinterpret_cast<unsigned long long *>(&ps.stats[3]), 1ull);
+        for (int w = 0; w < kHero; w++) {
+            float *row = rows + (size_t(idx) * kHero + w) * kRowStride;
+            if (ok) {
+                const float v[kIn] = {s.lam.v[w], c0[w], d, nf[w], ns[w]};
+                float4 a, b;
+                a.x = normalise(v[0], fs.rg.lo[0], fs.rg.hi[0]);
+                a.y = normalise(v[1], fs.rg.lo[1], fs.rg.hi[1]);
+                a.z = normalise(v[2], fs.rg.lo[2], fs.rg.hi[2]);
+                a.w = normalise(v[3], fs.rg.lo[3], fs.rg.hi[3]);
+                b = make_float4(normalise(v[4], fs.rg.lo[4], fs.rg.hi[4]), 0, 0, 0);
+                reinterpret_cast<float4 *>(row)[0] = a;
+                reinterpret_cast<float4 *>(row)[1] = b;
+            } else {
+                reinterpret_cast<float4 *>(row)[0] = make_float4(0, 0, 0, 0);
+                reinterpret_cast<float4 *>(row)[1] = make_float4(0, 0, 0, 0);
+            }
+        }
+    }
+}
+
+// Reflectances from the surrogate's (R_s + R_p) / 2 (or the exact path for hits
+// marked by k_film_inputs), then the thin-film scatter (material.h:228-261).
+__global__ void __launch_bounds__(256, 3) k_film_scatter(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
+                                                         const float4 *mlp_out, const int *fallback) {
+    const int n = ps.counts[queue_slot(bounce, kQFilm)];
+    const int *q = ps.mat_queue[2];
+    int *q_next = ps.queue[(bounce + 1) & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int idx = base + threadIdx.x;
+        bool alive = false;
+        int p = 0;
+        if (idx < n) {
+            p = q[idx];
+            const ShadeIn s = load_shade(ps, sc, p);
+            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            s4 R;
+            if (fallback[idx]) {
+                float thick[kMaxFilmLayers];
+                thin_film_thickness(sc, s, thick);
+                R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+            } else {
+                for (int w = 0; w < kHero; w++) {
+                    const float4 o = mlp_out[size_t(idx) * kHero + w];
+                    R.v[w] = clampf((o.x + o.y) * 0.5f, 0.0f, 1.0f);
+                }
+            }
+            s4 att;
+            f3 nd;
+            thin_film_scatter(sc, s, R, rng, att, nd);
+            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
+        }
+        const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
+        if (alive) q_next[slot] = p;
+    }
+}
+
+// Host: pack FP32 parameters into the bf16 shared-memory image and the bias vector.
+void pack_weights(const float *p, std::vector<uint8_t> &packed, std::vector<float> &bias) {
+    packed.assign(kPackedWeightBytes, 0);
+    auto put = [&](int region, int K, int r, int k, float v) {
+        const __nv_bfloat16 b = __float2bfloat16_rn(v);
+        std::memcpy(&packed[region + core_offset(r, k, K)], &b, 2);
+    };
+    for (int o = 0; o < kH; o++)
+        for (int i = 0; i < kInPad; i++) put(sW1, kInPad, o, i, i < kIn ? p[oW1 + o * kIn + i] : 0.0f);
+    for (int o = 0; o < kH; o++)
+        for (int i = 0; i < kH; i++) {
+            put(sW2, kH, o, i, p[oW2 + o * kH + i]);
+            put(sW3, kH, o, i, p[oW3 + o * kH + i]);
+        }
+    for (int o = 0; o < kOutPad; o++)
+        for (int i = 0; i < kH; i++) put(sW4, kH, o, i, o < kOut ? p[oW4 + o * kH + i] : 0.0f);
+    bias.assign(3 * kH + kOutPad, 0.0f);
+    for (int o = 0; o < kH; o++) {
+        bias[o] = p[oB1 + o];
+        bias[kH + o] = p[oB2 + o];
+        bias[2 * kH + o] = p[oB3 + o];
+    }
+    for (int o = 0; o < kOut; o++) bias[3 * kH + o] = p[oB4 + o];
+}
+
+Range to_range(const lambda_film_range &r) {
+    Range g;
+    const float *src[kIn] = {r.lambda_nm, r.cos_theta, r.thickness_nm, r.n_film, r.n_sub};
+    for (int k = 0; k < kIn; k++) {
+        g.lo[k] = src[k][0];
+        g.hi[k] = src[k][1];
+    }
+    return g;
+}
+
+bool range_ok(const lambda_film_range &r) {
+    const float *src[kIn] = {r.lambda_nm, r.cos_theta, r.thickness_nm, r.n_film, r.n_sub};
+    for (int k = 0; k < kIn; k++)
+        if (!(src[k][1] > src[k][0]) || !std::isfinite(src[k][0]) || !std::isfinite(src[k][1])) return false;
+    return r.n_film[0] > 0 && r.n_sub[0] > 0 && r.cos_theta[0] >= 0 && r.cos_theta[1] <= 1 && r.lambda_nm[0] > 0 &&
+           r.thickness_nm[0] >= 0;
+}
+
+}  // namespace mlp
+
+using namespace mlp;
+
+#define CK(call, what)                                          \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return ctx->cuda_fail(e_, what); \
+    } while (0)
 
 lambda_status lambda_ctx::surrogate_ready() {
-    if (!has_surrogate) return fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed (lambda_surrogate_train or lambda_surrogate_set)");
+    if (!has_surrogate)
+        return fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed (lambda_surrogate_train or lambda_surrogate_set)");
+    lambda_ctx *ctx = this;
+    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
     return LAMBDA_OK;
 }
 
-int lambda_ctx::launch_shade_surrogate(int, const lambda_dev::RenderParams &, const lambda_dev::DeviceScene &,
-                                       const lambda_dev::PathState &, int, StageProfiler *) {
-    return 0;
+namespace {
+
+// Installs FP32 parameters: master copy, packed bf16 tiles and biases.
+lambda_status install(lambda_ctx *ctx, const float *params_host, const lambda_film_range &r) {
+    std::vector<uint8_t> packed;
+    std::vector<float> bias;
+    pack_weights(params_host, packed, bias);
+    SurrogateBuffers &b = ctx->sbuf;
+    CK(b.weights_f32.upload(params_host, kParams * sizeof(float), ctx->stream), "upload surrogate");
+    CK(b.weights_bf16.reserve(packed.size() + bias.size() * 4), "upload surrogate");
+    CK(cudaMemcpyAsync(b.weights_bf16.ptr, packed.data(), packed.size(), cudaMemcpyHostToDevice, ctx->stream), "upload surrogate");
+    CK(cudaMemcpyAsync(static_cast<uint8_t *>(b.weights_bf16.ptr) + packed.size(), bias.data(), bias.size() * 4,
+                       cudaMemcpyHostToDevice, ctx->stream),
+       "upload surrogate");
+    CK(cudaStreamSynchronize(ctx->stream), "upload surrogate");
+    ctx->surrogate_range = r;
+    ctx->has_surrogate = true;
+    return LAMBDA_OK;
 }
 
-extern "C" lambda_status lambda_surrogate_train(lambda_ctx *ctx, const lambda_train_desc *, lambda_train_report *) {
-    if (!ctx) return LAMBDA_ERR_INVALID_ARGUMENT;
-    return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "surrogate training not built yet");
+int mlp_grid(lambda_ctx *ctx) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_tc, 128, kSmemBytes);
+    per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
+    return per_sm * ctx->sm_count;
 }
 
-extern "C" lambda_status lambda_surrogate_set(lambda_ctx *ctx, const float *, const lambda_film_range *) {
-    if (!ctx) return LAMBDA_ERR_INVALID_ARGUMENT;
-    return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "surrogate not built yet");
+lambda_status run_mlp(lambda_ctx *ctx, const float *rows_dev, int n_rows, float4 *out_dev) {
+    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+    CK(ctx->rbuf.error.reserve(16), "allocate flags");
+    int *err = ctx->rbuf.error.as<int>();
+    CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
+    const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
+    const int tiles = (n_rows + kTileM - 1) / kTileM;
+    const int grid = std::max(1, std::min(tiles, mlp_grid(ctx)));
+    k_mlp_tc<<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w),
+                                                     reinterpret_cast<const float *>(w + kPackedWeightBytes), rows_dev,
+                                                     nullptr, 0, n_rows, out_dev, err);
+    CK(cudaGetLastError(), "launch MLP kernel");
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");
+    CK(cudaStreamSynchronize(ctx->stream), "MLP inference");
+    if (herr & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
+    return LAMBDA_OK;
 }
 
-extern "C" lambda_status lambda_surrogate_get(const lambda_ctx *ctx, float *, lambda_film_range *) {
-    if (!ctx) return LAMBDA_ERR_INVALID_ARGUMENT;
-    return LAMBDA_ERR_UNSUPPORTED;
+}  // namespace
+
+int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const DeviceScene &sc, const PathState &ps,
+                                       int grid, StageProfiler *prof) {
+    const size_t P = size_t(rp.num_pixels);
+    FilmSurrogate fs;
+    fs.rg = to_range(surrogate_range);
+    fs.lam_lo = surrogate_range.lambda_nm[0];
+    fs.lam_hi = surrogate_range.lambda_nm[1];
+    fs.cos_lo = surrogate_range.cos_theta[0];
+    fs.cos_hi = surrogate_range.cos_theta[1];
+    fs.d_lo = surrogate_range.thickness_nm[0];
+    fs.d_hi = surrogate_range.thickness_nm[1];
+    fs.nf_lo = surrogate_range.n_film[0];
+    fs.nf_hi = surrogate_range.n_film[1];
+    fs.ns_lo = surrogate_range.n_sub[0];
+    fs.ns_hi = surrogate_range.n_sub[1];
+    float *rows = rbuf.tf_in.as<float>();
+    float4 *outv = rbuf.tf_out.as<float4>();
+    int *fb = rbuf.tf_queue.as<int>();
+    (void)P;
+    const uint8_t *w = static_cast<const uint8_t *>(sbuf.weights_bf16.ptr);
+    if (prof) prof->begin(9);
+    k_film_inputs<<<grid, 256, 0, stream>>>(bounce, rp, sc, ps, fs, rows, fb);
+    if (prof) prof->end();
+    if (prof) prof->begin(10);
+    k_mlp_tc<<<mlp_grid(this), 128, kSmemBytes, stream>>>(reinterpret_cast<const uint4 *>(w),
+                                                          reinterpret_cast<const float *>(w + kPackedWeightBytes), rows,
+                                                          ps.counts + queue_slot(bounce, kQFilm), kHero, 0, outv,
+                                                          ps.error);
+    if (prof) prof->end();
+    if (prof) prof->begin(11);
+    k_film_scatter<<<grid, 256, 0, stream>>>(bounce, rp, sc, ps, outv, fb);
+    if (prof) prof->end();
+    return 3;
 }
 
-extern "C" lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_film_query *, int32_t, float *) {
-    if (!ctx) return LAMBDA_ERR_INVALID_ARGUMENT;
-    return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "surrogate not built yet");
+lambda_status lambda_ctx::ensure_surrogate_state(int pixels) {
+    lambda_ctx *ctx = this;
+    const size_t P = size_t(pixels);
+    CK(rbuf.tf_in.reserve(P * kHero * kRowStride * sizeof(float)), "allocate surrogate batch");
+    CK(rbuf.tf_out.reserve(P * kHero * sizeof(float4)), "allocate surrogate batch");
+    CK(rbuf.tf_queue.reserve(P * sizeof(int)), "allocate surrogate batch");
+    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+    return LAMBDA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" lambda_status lambda_surrogate_set(lambda_ctx *ctx, const float *params, const lambda_film_range *range) {
+    if (!ctx || !params || !range) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (!range_ok(*range)) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "invalid surrogate input range");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    std::vector<float> p(kParams);
+    if (is_device_pointer(params)) CK(cudaMemcpy(p.data(), params, kParams * 4, cudaMemcpyDeviceToHost), "read parameters");
+    else std::memcpy(p.data(), params, kParams * 4);
+    for (float v : p)
+        if (!std::isfinite(v)) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "non-finite surrogate parameter");
+    return install(ctx, p.data(), *range);
+}
+
+extern "C" lambda_status lambda_surrogate_get(const lambda_ctx *cctx, float *params, lambda_film_range *range) {
+    if (!cctx || !params) return LAMBDA_ERR_INVALID_ARGUMENT;
+    lambda_ctx *ctx = const_cast<lambda_ctx *>(cctx);
+    if (!ctx->has_surrogate) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemcpy(params, ctx->sbuf.weights_f32.ptr, kParams * 4, cudaMemcpyDeviceToHost), "read parameters");
+    if (range) *range = ctx->surrogate_range;
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, float *out) {
+    if (!ctx || n < 0 || (n > 0 && (!q || !out))) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_surrogate) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed");
+    if (n == 0) return LAMBDA_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    std::vector<lambda_film_query> hq(n);
+    if (is_device_pointer(q)) CK(cudaMemcpy(hq.data(), q, sizeof(lambda_film_query) * n, cudaMemcpyDeviceToHost), "read queries");
+    else std::memcpy(hq.data(), q, sizeof(lambda_film_query) * n);
+    const Range rg = to_range(ctx->surrogate_range);
+    std::vector<float> rows(size_t(n) * kRowStride, 0.0f);
+    for (int i = 0; i < n; i++) {
+        const float v[kIn] = {hq[i].lambda_nm, hq[i].cos_theta, hq[i].thickness_nm, hq[i].n_film, hq[i].n_sub};
+        for (int k = 0; k < kIn; k++) rows[size_t(i) * kRowStride + k] = normalise(v[k], rg.lo[k], rg.hi[k]);
+    }
+    DeviceBuffer din, dout;
+    CK(din.upload(rows.data(), rows.size() * 4, ctx->stream), "stage queries");
+    CK(dout.reserve(size_t(n) * 16), "stage results");
+    lambda_status st = run_mlp(ctx, din.as<float>(), n, dout.as<float4>());
+    if (st == LAMBDA_OK) {
+        if (is_device_pointer(out)) CK(cudaMemcpy(out, dout.ptr, size_t(n) * 16, cudaMemcpyDeviceToDevice), "copy results");
+        else CK(cudaMemcpy(out, dout.ptr, size_t(n) * 16, cudaMemcpyDeviceToHost), "copy results");
+    }
+    din.release();
+    dout.release();
+    return st;
+}
+
+namespace {
+
+void init_params(std::vector<float> &p, uint64_t seed) {
+    p.assign(kParams, 0.0f);
+    uint64_t s = seed * 0x9E3779B97F4A7C15ull + 1;
+    auto uni = [&]() {
+        s = s * 6364136223846793005ull + 1442695040888963407ull;
+        return double(s >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    };
+    auto fill = [&](int off, int fan_out, int fan_in, double gain) {
+        const double a = gain * std::sqrt(6.0 / fan_in);
+        for (int i = 0; i < fan_out * fan_in; i++) p[off + i] = float(a * uni());
+    };
+    fill(oW1, kH, kIn, 1.0);
+    fill(oW2, kH, kH, 1.0);
+    fill(oW3, kH, kH, 1.0);
+    fill(oW4, kOut, kH, 0.5);
+}
+
+}  // namespace
+
+extern "C" lambda_status lambda_surrogate_train(lambda_ctx *ctx, const lambda_train_desc *desc,
+                                                lambda_train_report *report) {
+    if (!ctx || !desc) return LAMBDA_ERR_INVALID_ARGUMENT;
+    const lambda_train_desc &d = *desc;
+    if (d.samples < kTrainRows || d.samples > (int64_t(1) << 28) || d.epochs < 1 || d.batch < kTrainRows ||
+        d.batch % kTrainRows != 0 || !(d.learning_rate > 0) || !range_ok(d.range))
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "invalid training settings");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    const Range rg = to_range(d.range);
+    const int64_t N = d.samples;
+    const int audit_n = 1 << 18;
+    DeviceBuffer x, y, ax, ay, params, grad, m, v, loss, aout;
+    CK(x.reserve(size_t(N) * kRowStride * 4), "allocate training set");
+    CK(y.reserve(size_t(N) * 16), "allocate training set");
+    CK(ax.reserve(size_t(audit_n) * kRowStride * 4), "allocate audit set");
+    CK(ay.reserve(size_t(audit_n) * 16), "allocate audit set");
+    CK(aout.reserve(size_t(audit_n) * 16), "allocate audit set");
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    cudaEventRecord(e0, st);
+    for (int64_t first = 0; first < N; first += (1 << 22)) {
+        const int chunk = int(std::min<int64_t>(1 << 22, N - first));
+        k_film_labels<<<(chunk + 255) / 256, 256, 0, st>>>(d.seed, first, chunk, rg, x.as<float>() + first * kRowStride,
+                                                          y.as<float>() + first * 4);
+    }
+    k_film_labels<<<(audit_n + 255) / 256, 256, 0, st>>>(d.seed ^ 0xA5A5A5A5A5A5ull, 0, audit_n, rg, ax.as<float>(),
+                                                        ay.as<float>());
+    CK(cudaGetLastError(), "launch label kernel");
+    cudaEventRecord(e1, st);
+
+    std::vector<float> p;
+    init_params(p, d.seed);
+    CK(params.upload(p.data(), kParams * 4, st), "upload parameters");
+    CK(grad.reserve(kParams * 4), "allocate gradients");
+    CK(m.reserve(kParams * 4), "allocate optimiser state");
+    CK(v.reserve(kParams * 4), "allocate optimiser state");
+    CK(loss.reserve(64), "allocate loss");
+    CK(cudaMemsetAsync(grad.ptr, 0, kParams * 4, st), "clear gradients");
+    CK(cudaMemsetAsync(m.ptr, 0, kParams * 4, st), "clear optimiser state");
+    CK(cudaMemsetAsync(v.ptr, 0, kParams * 4, st), "clear optimiser state");
+    CK(cudaFuncSetAttribute(k_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem), "configure training kernel");
+    const int64_t steps_per_epoch = (N + d.batch - 1) / d.batch;
+    const int64_t total = steps_per_epoch * d.epochs;
+    int64_t t = 0;
+    float last_loss = 0;
+    for (int ep = 0; ep < d.epochs; ep++) {
+        CK(cudaMemsetAsync(loss.ptr, 0, 4, st), "clear loss");
+        for (int64_t s = 0; s < steps_per_epoch; s++, t++) {
+            const int64_t r0 = s * d.batch;
+            const int rows = int(std::min<int64_t>(d.batch, N - r0));
+            const int blocks = (rows + kTrainRows - 1) / kTrainRows;
+            k_train_step<<<blocks, kTrainThreads, kTrainSmem, st>>>(params.as<float>(), x.as<float>() + r0 * kRowStride,
+                                                                   y.as<float>() + r0 * 4, rows,
+                                                                   1.0f / float(rows * kOut), grad.as<float>(),
+                                                                   loss.as<float>());
+            // cosine decay to 2% of the base rate
+            const double frac = double(t) / double(std::max<int64_t>(1, total - 1));
+            const float lr = float(d.learning_rate * (0.02 + 0.98 * 0.5 * (1 + std::cos(3.14159265358979 * frac))));
+            const float c1 = float(1 - std::pow(0.9, double(t + 1))), c2 = float(1 - std::pow(0.999, double(t + 1)));
+            k_adam<<<(kParams + 255) / 256, 256, 0, st>>>(params.as<float>(), grad.as<float>(), m.as<float>(),
+                                                         v.as<float>(), kParams, lr, 0.9f, 0.999f, 1e-8f, c1, c2);
+        }
+        CK(cudaGetLastError(), "launch training kernels");
+        float h = 0;
+        CK(cudaMemcpyAsync(&h, loss.ptr, 4, cudaMemcpyDeviceToHost, st), "read loss");
+        CK(cudaStreamSynchronize(st), "training");
+        last_loss = h / float(steps_per_epoch);
+    }
+    cudaEventRecord(e2, st);
+    CK(cudaMemcpyAsync(p.data(), params.ptr, kParams * 4, cudaMemcpyDeviceToHost, st), "read parameters");
+    CK(cudaStreamSynchronize(st), "training");
+    lambda_status s = install(ctx, p.data(), d.range);
+    if (s != LAMBDA_OK) return s;
+    // audit: tensor-core inference against the FP64 labels
+    s = run_mlp(ctx, ax.as<float>(), audit_n, aout.as<float4>());
+    if (s != LAMBDA_OK) return s;
+    std::vector<float> got(size_t(audit_n) * 4), want(size_t(audit_n) * 4);
+    CK(cudaMemcpy(got.data(), aout.ptr, got.size() * 4, cudaMemcpyDeviceToHost), "read audit");
+    CK(cudaMemcpy(want.data(), ay.ptr, want.size() * 4, cudaMemcpyDeviceToHost), "read audit");
+    double mx = 0, mean = 0;
+    for (size_t i = 0; i < got.size(); i++) {
+        const double e = std::fabs(double(got[i]) - double(want[i]));
+        mx = std::max(mx, e);
+        mean += e;
+    }
+    mean /= double(got.size());
+    if (report) {
+        float lab = 0, tr = 0;
+        cudaEventElapsedTime(&lab, e0, e1);
+        cudaEventElapsedTime(&tr, e1, e2);
+        report->label_ms = lab;
+        report->train_ms = tr;
+        report->final_loss = last_loss;
+        report->max_abs_error = float(mx);
+        report->mean_abs_error = float(mean);
+        report->audit_samples = audit_n;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    for (DeviceBuffer *b : {&x, &y, &ax, &ay, &params, &grad, &m, &v, &loss, &aout}) b->release();
+    return LAMBDA_OK;
+}
+
+// One training-kernel forward/backward on caller data (for gradient checks):
+// x [n][5] normalised inputs, y [n][4] targets, n <= 64 * 1024; writes the mean
+// squared error and its gradient w.r.t. params.
+extern "C" lambda_status lambda_surrogate_grad(lambda_ctx *ctx, const float *params, const float *x, const float *y,
+                                               int32_t n, float *grad_out, float *loss_out) {
+    if (!ctx || !params || !x || !y || !grad_out || n <= 0 || n > (64 << 10)) return LAMBDA_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    std::vector<float> rows(size_t(n) * kRowStride, 0.0f);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < kIn; k++) rows[size_t(i) * kRowStride + k] = x[size_t(i) * kIn + k];
+    DeviceBuffer dp, dx, dy, dg, dl;
+    CK(dp.upload(params, kParams * 4, ctx->stream), "stage");
+    CK(dx.upload(rows.data(), rows.size() * 4, ctx->stream), "stage");
+    CK(dy.upload(y, size_t(n) * 16, ctx->stream), "stage");
+    CK(dg.reserve(kParams * 4), "stage");
+    CK(dl.reserve(16), "stage");
+    CK(cudaMemsetAsync(dg.ptr, 0, kParams * 4, ctx->stream), "stage");
+    CK(cudaMemsetAsync(dl.ptr, 0, 16, ctx->stream), "stage");
+    CK(cudaFuncSetAttribute(k_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem), "configure training kernel");
+    k_train_step<<<(n + kTrainRows - 1) / kTrainRows, kTrainThreads, kTrainSmem, ctx->stream>>>(
+        dp.as<float>(), dx.as<float>(), dy.as<float>(), n, 1.0f / float(n * kOut), dg.as<float>(), dl.as<float>());
+    CK(cudaGetLastError(), "launch training kernel");
+    CK(cudaMemcpyAsync(grad_out, dg.ptr, kParams * 4, cudaMemcpyDeviceToHost, ctx->stream), "read gradient");
+    float l = 0;
+    CK(cudaMemcpyAsync(&l, dl.ptr, 4, cudaMemcpyDeviceToHost, ctx->stream), "read loss");
+    CK(cudaStreamSynchronize(ctx->stream), "gradient");
+    if (loss_out) *loss_out = l;
+    for (DeviceBuffer *b : {&dp, &dx, &dy, &dg, &dl}) b->release();
+    return LAMBDA_OK;
 }

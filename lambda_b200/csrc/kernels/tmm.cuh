@@ -8,6 +8,11 @@
 // The reference returns only (R_s + R_p) / 2; this also gives the transmittances
 // T = Re(n_out cos_out) / Re(n_in cos_in) |1 / M00|^2 (conjugated indices for p),
 // which for real indices satisfy R + T = 1.
+//
+// The work splits in two: film_prepare() forms everything that depends only on
+// the indices and the incidence angle (Snell cosines, interface matrices), and
+// film_apply() multiplies in the layer phases for one wavelength. With
+// non-dispersive indices the four hero wavelengths of a hit share one prepare.
 // Templated on the real type: float for the render path, double for the
 // training-label generator and the error audit.
 #pragma once
@@ -26,16 +31,22 @@ template <typename R> __device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> 
     return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
 }
 template <typename R> __device__ __forceinline__ cx<R> operator*(cx<R> a, R s) { return cmk(a.re * s, a.im * s); }
+
+template <typename R> __device__ __forceinline__ R rdiv(R a, R b) {
+    if constexpr (sizeof(R) == 4) return __fdividef(a, b);  // 2 ulp: far inside the 1e-5 budget
+    else return a / b;
+}
+
 template <typename R> __device__ __forceinline__ cx<R> operator/(cx<R> a, cx<R> b) {
     // Smith's method: stable when one component of b dominates.
     if (fabs(b.re) >= fabs(b.im)) {
-        const R q = b.im / b.re;
+        const R q = rdiv(b.im, b.re);
         const R den = b.re + b.im * q;
-        return cmk((a.re + a.im * q) / den, (a.im - a.re * q) / den);
+        return cmk(rdiv(a.re + a.im * q, den), rdiv(a.im - a.re * q, den));
     }
-    const R q = b.re / b.im;
+    const R q = rdiv(b.re, b.im);
     const R den = b.re * q + b.im;
-    return cmk((a.re * q + a.im) / den, (a.im * q - a.re) / den);
+    return cmk(rdiv(a.re * q + a.im, den), rdiv(a.im * q - a.re, den));
 }
 template <typename R> __device__ __forceinline__ R cabs2(cx<R> a) { return a.re * a.re + a.im * a.im; }
 
@@ -46,11 +57,11 @@ template <typename R> __device__ __forceinline__ cx<R> csqrt_(cx<R> z) {
     if (r == R(0)) return cmk(R(0), z.im);
     if (z.re >= R(0)) {
         const R s = sqrt((r + z.re) * R(0.5));
-        return cmk(s, z.im / (R(2) * s));
+        return cmk(s, rdiv(z.im, R(2) * s));
     }
     R t = sqrt((r - z.re) * R(0.5));
     t = copysign(t, z.im);
-    return cmk(z.im / (R(2) * t), t);
+    return cmk(rdiv(z.im, R(2) * t), t);
 }
 
 template <typename R> __device__ __forceinline__ cx<R> cexp_(cx<R> z) {
@@ -75,6 +86,11 @@ template <typename R> __device__ __forceinline__ m2<R> mmul(const m2<R> &x, cons
     return m2<R>{x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c, x.c * y.b + x.d * y.d};
 }
 
+// diag(e_minus, e_plus) * y
+template <typename R> __device__ __forceinline__ m2<R> dmul(cx<R> em, cx<R> ep, const m2<R> &y) {
+    return m2<R>{em * y.a, em * y.b, ep * y.c, ep * y.d};
+}
+
 // Interface matrix (1/t) [[1, r], [r, 1]] (utils.h:173-191).
 template <typename R>
 __device__ __forceinline__ m2<R> interface_matrix(cx<R> n1, cx<R> n2, cx<R> c1, cx<R> c2, bool p_pol) {
@@ -86,10 +102,11 @@ __device__ __forceinline__ m2<R> interface_matrix(cx<R> n1, cx<R> n2, cx<R> c1, 
         num = n2 * c1 - n1 * c2;
         den = n2 * c1 + n1 * c2;
     }
-    const cx<R> r = num / den;
-    const cx<R> t = (cmk(R(2), R(0)) * n1 * c1) / den;
-    const cx<R> one = cmk(R(1), R(0));
-    return m2<R>{one / t, r / t, r / t, one / t};
+    // 1/t = den / (2 n1 c1) and r/t = num / (2 n1 c1)
+    const cx<R> two_n1c1 = cmk(R(2), R(0)) * n1 * c1;
+    const cx<R> inv_t = den / two_n1c1;
+    const cx<R> r_t = num / two_n1c1;
+    return m2<R>{inv_t, r_t, r_t, inv_t};
 }
 
 template <typename R>
@@ -97,46 +114,126 @@ struct FilmResult {
     R rs, rp, ts, tp;
 };
 
-// Multilayer stack: n[0] incidence medium, n[1..L] layers, n[L+1] exit medium;
-// d[0..L-1] layer thicknesses in nm, in the order the light meets them.
+// Everything of a stack of up to MAXL layers that does not depend on the
+// wavelength once the indices are fixed: n[0] incidence medium, n[1..L] layers,
+// n[L+1] exit medium.
 template <typename R, int MAXL>
-__device__ FilmResult<R> film_stack(int L, const cx<R> *n, const R *d, R cos0, R lambda) {
+struct FilmPrep {
+    int L;
+    m2<R> is[MAXL + 1], ip[MAXL + 1];
+    cx<R> n_layer[MAXL > 0 ? MAXL : 1];
+    cx<R> cos_layer[MAXL > 0 ? MAXL : 1];
+    cx<R> n_in, n_out, cos_out;
+    R cos0;
+};
+
+template <typename R, int MAXL>
+__device__ __forceinline__ void film_prepare(int L, const cx<R> *n, R cos0, FilmPrep<R, MAXL> &f) {
+    f.L = L < MAXL ? L : MAXL;
+    f.cos0 = cos0;
     cx<R> cos_cur = cmk(cos0, R(0));
     cx<R> sin_next = n[0] / n[1];
     sin_next = sin_next * (sin_next * (cmk(R(1), R(0)) - cos_cur * cos_cur));
     cx<R> cos_next = csqrt_(cmk(R(1), R(0)) - sin_next);
-    m2<R> ms = interface_matrix(n[0], n[1], cos_cur, cos_next, false);
-    m2<R> mp = interface_matrix(n[0], n[1], cos_cur, cos_next, true);
-    const R k = R(2) * R(3.14159265358979323846) / lambda;
-    for (int j = 0; j < L && j < MAXL; j++) {
-        const cx<R> a = n[j + 1], b = n[j + 2];
-        cos_cur = cos_next;
-        const cx<R> sin_cur = sin_next;
-        sin_next = a / b;
-        sin_next = sin_next * (sin_next * sin_cur);
-        cos_next = csqrt_(cmk(R(1), R(0)) - sin_next);
-        const m2<R> is = interface_matrix(a, b, cos_cur, cos_next, false);
-        const m2<R> ip = interface_matrix(a, b, cos_cur, cos_next, true);
-        const cx<R> phi = ((a * k) * d[j]) * cos_cur;
-        const cx<R> e_minus = cexp_(cmk(phi.im, -phi.re));   // exp(-i phi)
-        const cx<R> e_plus = cexp_(cmk(-phi.im, phi.re));    // exp(+i phi)
-        const cx<R> zero = cmk(R(0), R(0));
-        const m2<R> prop{e_minus, zero, zero, e_plus};
-        ms = mmul(ms, mmul(prop, is));
-        mp = mmul(mp, mmul(prop, ip));
+    f.is[0] = interface_matrix(n[0], n[1], cos_cur, cos_next, false);
+    f.ip[0] = interface_matrix(n[0], n[1], cos_cur, cos_next, true);
+#pragma unroll
+    for (int j = 0; j < MAXL; j++) {
+        if (j < f.L) {
+            const cx<R> a = n[j + 1], b = n[j + 2];
+            cos_cur = cos_next;
+            const cx<R> sin_cur = sin_next;
+            sin_next = a / b;
+            sin_next = sin_next * (sin_next * sin_cur);
+            cos_next = csqrt_(cmk(R(1), R(0)) - sin_next);
+            f.is[j + 1] = interface_matrix(a, b, cos_cur, cos_next, false);
+            f.ip[j + 1] = interface_matrix(a, b, cos_cur, cos_next, true);
+            f.n_layer[j] = a;
+            f.cos_layer[j] = cos_cur;
+        }
+    }
+    f.n_in = n[0];
+    f.n_out = n[f.L + 1];
+    f.cos_out = cos_next;
+}
+
+// Layer phases at one wavelength; k = 2 pi / lambda, d[j] in nm.
+template <typename R, int MAXL>
+__device__ __forceinline__ FilmResult<R> film_apply(const FilmPrep<R, MAXL> &f, const R *d, R k, bool want_t) {
+    m2<R> ms = f.is[0], mp = f.ip[0];
+#pragma unroll
+    for (int j = 0; j < MAXL; j++) {
+        if (j < f.L) {
+            const cx<R> phi = ((f.n_layer[j] * k) * d[j]) * f.cos_layer[j];
+            // exp(-i phi) = e^{Im phi} (cos Re phi - i sin Re phi), exp(+i phi) = e^{-Im phi} (cos + i sin)
+            R sn, cs, g;
+            if constexpr (sizeof(R) == 4) {
+                sincosf(phi.re, &sn, &cs);
+                g = expf(phi.im);
+            } else {
+                sincos(phi.re, &sn, &cs);
+                g = exp(phi.im);
+            }
+            const R ginv = R(1) / g;
+            const cx<R> e_minus = cmk(g * cs, -(g * sn));
+            const cx<R> e_plus = cmk(ginv * cs, ginv * sn);
+            ms = mmul(ms, dmul(e_minus, e_plus, f.is[j + 1]));
+            mp = mmul(mp, dmul(e_minus, e_plus, f.ip[j + 1]));
+        }
     }
     FilmResult<R> out;
     out.rs = cabs2(ms.b / ms.a);
     out.rp = cabs2(mp.b / mp.a);
-    const cx<R> n_in = n[0], n_out = n[L + 1];
-    const cx<R> c_in = cmk(cos0, R(0));
-    const R s_num = (n_out * cos_next).re, s_den = (n_in * c_in).re;
-    const R p_num = (cmk(n_out.re, -n_out.im) * cos_next).re, p_den = (cmk(n_in.re, -n_in.im) * c_in).re;
-    const cx<R> one = cmk(R(1), R(0));
-    const R ts_amp = cabs2(one / ms.a), tp_amp = cabs2(one / mp.a);
-    out.ts = s_den != R(0) ? s_num / s_den * ts_amp : R(0);
-    out.tp = p_den != R(0) ? p_num / p_den * tp_amp : R(0);
+    out.ts = out.tp = R(0);
+    if (want_t) {
+        const cx<R> c_in = cmk(f.cos0, R(0));
+        const R s_num = (f.n_out * f.cos_out).re, s_den = (f.n_in * c_in).re;
+        const R p_num = (cmk(f.n_out.re, -f.n_out.im) * f.cos_out).re, p_den = (cmk(f.n_in.re, -f.n_in.im) * c_in).re;
+        const R ts_amp = R(1) / cabs2(ms.a), tp_amp = R(1) / cabs2(mp.a);
+        out.ts = s_den != R(0) ? s_num / s_den * ts_amp : R(0);
+        out.tp = p_den != R(0) ? p_num / p_den * tp_amp : R(0);
+    }
     return out;
+}
+
+template <typename R, int MAXL>
+__device__ __forceinline__ FilmResult<R> film_stack(int L, const cx<R> *n, const R *d, R cos0, R lambda) {
+    FilmPrep<R, MAXL> f;
+    film_prepare<R, MAXL>(L, n, cos0, f);
+    return film_apply<R, MAXL>(f, d, R(2) * R(3.14159265358979323846) / lambda, true);
+}
+
+// The same product formed one interface at a time (any number of layers, no
+// per-layer arrays): index_of(j) gives n[j], d[j] the layer thicknesses.
+template <typename R, class IndexOf>
+__device__ __forceinline__ R film_reflectance_stream(int L, IndexOf index_of, const R *d, R cos0, R k) {
+    cx<R> n0 = index_of(0), n1 = index_of(1);
+    cx<R> cos_cur = cmk(cos0, R(0));
+    cx<R> sin_next = n0 / n1;
+    sin_next = sin_next * (sin_next * (cmk(R(1), R(0)) - cos_cur * cos_cur));
+    cx<R> cos_next = csqrt_(cmk(R(1), R(0)) - sin_next);
+    m2<R> ms = interface_matrix(n0, n1, cos_cur, cos_next, false);
+    m2<R> mp = interface_matrix(n0, n1, cos_cur, cos_next, true);
+#pragma unroll 1
+    for (int j = 0; j < L; j++) {
+        const cx<R> a = n1;
+        n1 = index_of(j + 2);
+        cos_cur = cos_next;
+        const cx<R> sin_cur = sin_next;
+        sin_next = a / n1;
+        sin_next = sin_next * (sin_next * sin_cur);
+        cos_next = csqrt_(cmk(R(1), R(0)) - sin_next);
+        const cx<R> phi = ((a * k) * d[j]) * cos_cur;
+        R sn, cs;
+        if constexpr (sizeof(R) == 4) sincosf(phi.re, &sn, &cs);
+        else sincos(phi.re, &sn, &cs);
+        const R g = sizeof(R) == 4 ? R(expf(float(phi.im))) : R(exp(double(phi.im)));
+        const R ginv = R(1) / g;
+        const cx<R> e_minus = cmk(g * cs, -(g * sn)), e_plus = cmk(ginv * cs, ginv * sn);
+        ms = mmul(ms, dmul(e_minus, e_plus, interface_matrix(a, n1, cos_cur, cos_next, false)));
+        mp = mmul(mp, dmul(e_minus, e_plus, interface_matrix(a, n1, cos_cur, cos_next, true)));
+    }
+    return (cabs2(ms.b / ms.a) + cabs2(mp.b / mp.a)) * R(0.5);
 }
 
 }  // namespace lambda_dev

@@ -4,12 +4,16 @@
 // consumed in the reference's order (renderer.h:64-92, :94-195), so each pixel
 // must finish sample s before it starts s+1, and the wave is the unit of
 // parallelism (W*H paths in flight). Per bounce i the stages are
-//   intersect  closest hit of every active path            (scene.h:51)
-//   shade      miss/emitter terms, NEE light sampling, BSDF scatter, Russian
-//              roulette; survivors and shadow rays are pushed to queues with one
-//              atomic per warp (ballot + popc)                (renderer.h:101-191)
-//   shadow     occlusion of the NEE rays and their radiance  (renderer.h:166-173)
-// All path state is structure-of-arrays indexed by pixel; queues hold pixel ids.
+//   intersect   closest hit of every active path (scene.h:51); misses and emitter
+//               hits are finished on the spot (renderer.h:105-131), the rest are
+//               pushed to one queue per material family
+//   lambert     NEE light sampling + cosine scatter + Russian roulette (renderer.h:133-191)
+//   specular    mirror and dielectric scatter + Russian roulette
+//   thin film   transfer-matrix reflectance of the four hero wavelengths, scatter
+//   shadow      occlusion of the NEE rays and their radiance (renderer.h:166-173)
+// so every kernel runs one material's code over a coherent batch. Queue pushes
+// cost one atomic per warp (ballot + popc). All path state is structure-of-arrays
+// indexed by pixel; queues hold pixel ids.
 #pragma once
 
 #include <cstdint>
@@ -18,6 +22,14 @@
 #include "tmm.cuh"
 
 namespace lambda_dev {
+
+// Translation units that only need the device helpers define
+// LAMBDA_WAVEFRONT_HELPERS_ONLY; the kernels then get internal linkage there.
+#ifdef LAMBDA_WAVEFRONT_HELPERS_ONLY
+#define LAMBDA_KERNEL static __global__
+#else
+#define LAMBDA_KERNEL __global__
+#endif
 
 // Queue push with one atomic per warp. Must be reached by all 32 lanes.
 __device__ __forceinline__ int warp_push(int *counter, bool want) {
@@ -39,7 +51,7 @@ __device__ __forceinline__ s4 hero_wavelengths(const RenderParams &rp, float lam
 }
 
 // Every pixel: seed its stream, zero film and radiance.
-__global__ void k_init(RenderParams rp, PathState ps) {
+LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= rp.num_pixels) return;
     ps.rng[p] = lambda_rng::pcg_seed(rp.seed, uint64_t(p));
@@ -54,24 +66,21 @@ __global__ void k_init(RenderParams rp, PathState ps) {
 
 // Wave prologue (one block): fold the last wave's queue sizes into the
 // statistics, clear the counters, advance the wave index.
-__global__ void k_wave_prologue(int depth, PathState ps) {
-    const int n = 2 * (depth + 2);
-    __shared__ unsigned long long seg, sh;
-    if (threadIdx.x == 0) {
-        seg = 0;
-        sh = 0;
-    }
+LAMBDA_KERNEL void k_wave_prologue(int depth, PathState ps) {
+    const int n = kQueues * (depth + 2);
+    __shared__ unsigned long long tot[kQueues];
+    if (threadIdx.x < kQueues) tot[threadIdx.x] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int c = ps.counts[i];
-        if (i < depth + 2) atomicAdd(&seg, (unsigned long long)c);
-        else atomicAdd(&sh, (unsigned long long)c);
-    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&tot[i % kQueues], (unsigned long long)ps.counts[i]);
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) ps.counts[i] = 0;
     if (threadIdx.x == 0) {
-        ps.stats[0] += seg;
-        ps.stats[1] += sh;
+        // stats: segments, NEE rays, thin-film hits, (fallback), Lambertian hits, specular hits
+        ps.stats[0] += tot[kQActive];
+        ps.stats[1] += tot[kQShadow];
+        ps.stats[2] += tot[kQFilm];
+        ps.stats[4] += tot[kQLambert];
+        ps.stats[5] += tot[kQSpecular];
         ps.wave[1] = ps.wave[0];
         ps.wave[0] += 1;
     }
@@ -79,7 +88,7 @@ __global__ void k_wave_prologue(int depth, PathState ps) {
 
 // Film += linear sRGB of the finished sample (renderer.h:84), then start the
 // next sample: stratified jitter, hero wavelength, camera ray (renderer.h:69-81).
-__global__ void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
+LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= rp.num_pixels) return;
     const int s = ps.wave[1];
@@ -107,27 +116,7 @@ __global__ void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
     ps.throughput[p] = make_float4(1, 1, 1, 1);
     ps.radiance[p] = make_float4(0, 0, 0, 0);
     ps.queue[0][p] = p;
-    if (p == 0) ps.counts[0] = rp.num_pixels;
-}
-
-__global__ void __launch_bounds__(256) k_intersect(int bounce, DeviceScene sc, PathState ps) {
-    const int n = ps.counts[bounce];
-    const int *q = ps.queue[bounce & 1];
-    const int stride = gridDim.x * blockDim.x;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
-        const int p = q[idx];
-        const float4 o = ps.ray_o[p], d = ps.ray_d[p];
-        Hit h;
-        bool overflow = false;
-        if (closest_hit(sc, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), h, overflow)) {
-            ps.hit_p[p] = make_float4(h.point.x, h.point.y, h.point.z, h.u);
-            ps.hit_n[p] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.v);
-            ps.hit_id[p] = make_int4(h.instance, h.object, h.front ? 1 : 0, 0);
-        } else {
-            ps.hit_id[p] = make_int4(-1, -1, 0, 0);
-        }
-        if (overflow) atomicOr(ps.error, 1);
-    }
+    if (p == 0) ps.counts[queue_slot(0, kQActive)] = rp.num_pixels;
 }
 
 // Material index of object `obj` in instance `inst` (instance.h:38).
@@ -135,21 +124,199 @@ __device__ __forceinline__ int material_of(const DeviceScene &sc, int inst_mater
     return inst_material >= 0 ? inst_material : prim_material(load_prim(sc, obj));
 }
 
-// Thin-film reflectance (R_s + R_p) / 2 at one wavelength (material.h:263-309),
-// FP32 transfer matrix. Layer order and thicknesses reverse on back-face hits.
-__device__ inline float thin_film_r(const DeviceScene &sc, const int4 &m, bool front, float cos0, float lambda,
-                             const float *thickness) {
-    const int L = m.y < kMaxFilmLayers ? m.y : kMaxFilmLayers;
-    cx<float> n[kMaxFilmLayers + 2];
-    float d[kMaxFilmLayers];
-    for (int k = 0; k < L + 2; k++) {
-        const int src = front ? k : L + 1 - k;
-        const double2 c = cspectrum_at(sc, sc.material_props[m.z + src], lambda);
-        n[k] = cx<float>{float(c.x), float(c.y)};
+// Closest hit; misses and emitter hits add their radiance and end the path
+// (renderer.h:105-131); other hits go to their material's queue.
+LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    extern __shared__ int stack_smem[];
+    SharedStack st_a, st_b;
+    thread_stacks(stack_smem, st_a, st_b);
+    const int n = ps.counts[queue_slot(bounce, kQActive)];
+    const int *q = ps.queue[bounce & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int idx = base + threadIdx.x;
+        int p = 0, family = -1;
+        if (idx < n) {
+            p = q[idx];
+            const float4 o4 = ps.ray_o[p], d4 = ps.ray_d[p];
+            const f3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
+            Hit h;
+            bool overflow = false;
+            const bool hit = closest_hit_t(sc, o, d, h, overflow, st_a, st_b);
+            if (overflow) atomicOr(ps.error, 1);
+            const bool specular = d4.w != 0.0f;
+            const float prev_pdf = o4.w;
+            const bool lights = sc.total_light_power > 0;
+            if (!hit) {
+                const s4 lam = from_f4(ps.lam[p]);
+                float w = 1;
+                if (!specular && lights)
+                    w = power_heuristic(prev_pdf, (1 / (4 * kPi)) * sc.light_power[sc.num_lights - 1] / sc.total_light_power);
+                const s4 T = from_f4(ps.throughput[p]);
+                ps.radiance[p] = to_f4(from_f4(ps.radiance[p]) + T * background_eval(sc, d, lam) * w);
+            } else {
+                const InstanceRef ir = instance_ref(sc, h.instance);
+                const int4 ih = ir.header();
+                const int mat = material_of(sc, ih.w, h.object);
+                const int4 m = __ldg(&sc.materials[mat]);
+                if (m.x == kEmissive) {
+                    float w = 1;
+                    if (!specular && lights) {
+                        float M[16], Mi[16];
+                        ir.load_m(M, 0);
+                        ir.load_m(Mi, 1);
+                        const Prim pr = load_prim(sc, h.object);
+                        const f3 c0 = mk(M[0], M[4], M[8]);
+                        const float light_power = prim_area(pr) * length_sq(c0) * sc.material_emission[mat];
+                        const float pdf = prim_pdf(pr, xform(Mi, o, 1), normalize(xform(Mi, d, 0)));
+                        w = power_heuristic(prev_pdf, pdf * light_power / sc.total_light_power);
+                    }
+                    ShadePoint sp;
+                    sp.point = h.point;
+                    sp.u = h.u;
+                    sp.v = h.v;
+                    const s4 lam = from_f4(ps.lam[p]);
+                    const s4 T = from_f4(ps.throughput[p]);
+                    ps.radiance[p] = to_f4(from_f4(ps.radiance[p]) + T * spectrum_texture4(sc, m.y, sp, lam) * w);
+                } else {
+                    ps.hit_p[p] = make_float4(h.point.x, h.point.y, h.point.z, h.u);
+                    ps.hit_n[p] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.v);
+                    ps.hit_id[p] = make_int4(mat, h.object, h.front ? 1 : 0, h.instance);
+                    family = m.x == kLambertian ? 0 : (m.x == kThinFilm ? 2 : 1);
+                }
+            }
+        }
+        for (int f = 0; f < 3; f++) {
+            const int slot = warp_push(&ps.counts[queue_slot(bounce, kQLambert + f)], family == f);
+            if (family == f) ps.mat_queue[f][slot] = p;
+        }
     }
-    for (int k = 0; k < L; k++) d[k] = thickness[front ? k : L - 1 - k];
-    const FilmResult<float> r = film_stack<float, kMaxFilmLayers>(L, n, d, cos0, lambda);
-    return (r.rs + r.rp) * 0.5f;
+}
+
+// Per-path state a shade kernel works on.
+struct ShadeIn {
+    int p;
+    f3 d;
+    ShadePoint sp;
+    f3 nrm;
+    bool front;
+    int4 m;
+    s4 T, lam;
+};
+
+__device__ __forceinline__ ShadeIn load_shade(const PathState &ps, const DeviceScene &sc, int p) {
+    ShadeIn s;
+    s.p = p;
+    const float4 d4 = ps.ray_d[p];
+    s.d = mk(d4.x, d4.y, d4.z);
+    const float4 hp = ps.hit_p[p], hn = ps.hit_n[p];
+    const int4 id = ps.hit_id[p];
+    s.sp.point = mk(hp.x, hp.y, hp.z);
+    s.sp.u = hp.w;
+    s.sp.v = hn.w;
+    s.nrm = mk(hn.x, hn.y, hn.z);
+    s.front = id.z != 0;
+    s.m = __ldg(&sc.materials[id.x]);
+    s.T = from_f4(ps.throughput[p]);
+    s.lam = from_f4(ps.lam[p]);
+    return s;
+}
+
+// Throughput update, Russian roulette and the depth limit (renderer.h:177-191);
+// writes the scattered ray and returns whether the path continues.
+__device__ __forceinline__ bool finish_scatter(const RenderParams &rp, const PathState &ps, const ShadeIn &s, Rng &rng,
+                                               int bounce, s4 att, f3 nd, float pdf, bool spec) {
+    s4 T = s.T;
+    if (spec) T = T * att;
+    else T = T * ((att * dot(s.nrm, nd)) / pdf);
+    bool alive = true;
+    if (bounce >= kRrStartDepth) {
+        const float qq = 1 - clampf(s4_max(T), 0.05f, 0.95f);
+        if (rng.next() < qq) alive = false;
+        else T = T / (1 - qq);
+    }
+    if (bounce >= rp.depth) alive = false;
+    ps.rng[s.p] = rng.state;
+    ps.throughput[s.p] = to_f4(T);
+    ps.ray_o[s.p] = make_float4(s.sp.point.x, s.sp.point.y, s.sp.point.z, pdf);
+    ps.ray_d[s.p] = make_float4(nd.x, nd.y, nd.z, spec ? 1.0f : 0.0f);
+    return alive;
+}
+
+// Lambertian: next-event estimation (renderer.h:133-175), then cosine-weighted
+// scatter (material.h:151-172).
+LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_lambert(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    const int n = ps.counts[queue_slot(bounce, kQLambert)];
+    const int *q = ps.mat_queue[0];
+    int *q_next = ps.queue[(bounce + 1) & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int idx = base + threadIdx.x;
+        bool alive = false, nee = false;
+        int p = 0;
+        if (idx < n) {
+            p = q[idx];
+            const ShadeIn s = load_shade(ps, sc, p);
+            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            const s4 albedo = spectrum_texture4(sc, s.m.y, s.sp, s.lam);
+            if (sc.total_light_power > 0) {
+                const float target = sc.total_light_power * rng.next();
+                int li = sc.light_inst[0], lo = sc.light_obj[0];
+                float lp = sc.light_power[0];
+                for (int j = 0; j < sc.num_lights; j++) {
+                    if (sc.light_cdf[j] >= target) {
+                        li = sc.light_inst[j];
+                        lo = sc.light_obj[j];
+                        lp = sc.light_power[j];
+                        break;
+                    }
+                }
+                f3 ldir;
+                float lpdf;
+                if (li != -1) {
+                    const Prim pr = load_prim(sc, lo);
+                    if (sc.instance_flags[li] & 1u) {
+                        const f3 zero = mk(0.0f, 0.0f, 0.0f);
+                        const f3 local = s.sp.point + zero;
+                        ldir = normalize(prim_sample(pr, local, rng) + zero);
+                        lpdf = prim_pdf(pr, local, normalize(ldir + zero));
+                    } else {
+                        const InstanceRef lr = instance_ref(sc, li);
+                        float M[16], Mi[16];
+                        lr.load_m(M, 0);
+                        lr.load_m(Mi, 1);
+                        const f3 local = xform(Mi, s.sp.point, 1);
+                        ldir = normalize(xform(M, prim_sample(pr, local, rng), 0));
+                        lpdf = prim_pdf(pr, local, normalize(xform(Mi, ldir, 0)));
+                    }
+                } else {
+                    ldir = random_unit_vector(rng);
+                    lpdf = 1 / (4 * kPi);
+                }
+                const float cos_t = dot(s.nrm, ldir);
+                if (lpdf > 0 && cos_t > 0) {
+                    lpdf *= lp / sc.total_light_power;
+                    const s4 att = cos_t <= 0 ? s4_fill(0) : albedo / kPi;
+                    const float spdf = cos_t > 0 ? cos_t / kPi : 0;
+                    const float w = power_heuristic(lpdf, spdf);
+                    ps.sh_o[p] = make_float4(s.sp.point.x, s.sp.point.y, s.sp.point.z, w);
+                    ps.sh_d[p] = make_float4(ldir.x, ldir.y, ldir.z, lpdf);
+                    ps.sh_a[p] = to_f4((s.T * att) * cos_t);
+                    ps.sh_light[p] = make_int2(li, lo);
+                    nee = true;
+                }
+            }
+            const f3 nd = random_in_hemisphere(s.nrm, rng);
+            const float cl = dot(s.nrm, nd);
+            const s4 att = cl <= 0 ? s4_fill(0) : albedo / kPi;
+            const float pdf = cl > 0 ? cl / kPi : 0;
+            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, pdf, false);
+        }
+        const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
+        if (alive) q_next[slot] = p;
+        const int sslot = warp_push(&ps.counts[queue_slot(bounce, kQShadow)], nee);
+        if (nee) ps.shadow_queue[sslot] = p;
+    }
 }
 
 // powf(x, 5) of the dielectric's Schlick factor (material.h:186), formed in double
@@ -159,190 +326,152 @@ __device__ __forceinline__ float pow5(float x) {
     return float(x2 * x2 * double(x));
 }
 
-__global__ void __launch_bounds__(256) k_shade(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
-    const int n = ps.counts[bounce];
-    const int *q = ps.queue[bounce & 1];
+// Mirror and dielectric (material.h:174-226).
+LAMBDA_KERNEL void __launch_bounds__(256) k_shade_specular(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    const int n = ps.counts[queue_slot(bounce, kQSpecular)];
+    const int *q = ps.mat_queue[1];
     int *q_next = ps.queue[(bounce + 1) & 1];
     const int stride = gridDim.x * blockDim.x;
-    // uniform trip count per warp so that the queue pushes below see all lanes
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const int idx = base + threadIdx.x;
-        bool alive = false, nee = false;
+        bool alive = false;
         int p = 0;
         if (idx < n) {
             p = q[idx];
-            const int4 id = ps.hit_id[p];
-            float4 o4 = ps.ray_o[p], d4 = ps.ray_d[p];
-            const f3 d = mk(d4.x, d4.y, d4.z);
-            const float prev_pdf = o4.w;
-            const bool specular = d4.w != 0.0f;
-            s4 T = from_f4(ps.throughput[p]);
-            s4 L = from_f4(ps.radiance[p]);
-            const s4 lam = from_f4(ps.lam[p]);
-            const bool lights = sc.total_light_power > 0;
-            if (id.x < 0) {
-                // miss: background with MIS against its NEE pdf (renderer.h:105-113)
-                float w = 1;
-                if (!specular && lights)
-                    w = power_heuristic(prev_pdf, (1 / (4 * kPi)) * sc.light_power[sc.num_lights - 1] / sc.total_light_power);
-                L = L + T * background_eval(sc, d, lam) * w;
-                ps.radiance[p] = to_f4(L);
+            const ShadeIn s = load_shade(ps, sc, p);
+            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            s4 att;
+            f3 nd;
+            if (s.m.x == kMirror) {
+                nd = reflected(s.d, s.nrm);
+                att = spectrum_texture4(sc, s.m.y, s.sp, s.lam);
             } else {
-                const float4 hp = ps.hit_p[p], hn = ps.hit_n[p];
-                ShadePoint sp;
-                sp.point = mk(hp.x, hp.y, hp.z);
-                sp.u = hp.w;
-                sp.v = hn.w;
-                const f3 nrm = mk(hn.x, hn.y, hn.z);
-                const bool front = id.z != 0;
-                const InstanceRef ir = instance_ref(sc, id.x);
-                const int4 ih = ir.header();
-                const int mat = material_of(sc, ih.w, id.y);
-                const int4 m = __ldg(&sc.materials[mat]);
-                if (m.x == kEmissive) {
-                    // emitter hit (renderer.h:119-131)
-                    float w = 1;
-                    if (!specular && lights) {
-                        float M[16], Mi[16];
-                        ir.load_m(M, 0);
-                        ir.load_m(Mi, 1);
-                        const Prim pr = load_prim(sc, id.y);
-                        const f3 c0 = mk(M[0], M[4], M[8]);
-                        const float light_power = prim_area(pr) * length_sq(c0) * sc.material_emission[mat];
-                        const f3 o = mk(o4.x, o4.y, o4.z);
-                        const float pdf = prim_pdf(pr, xform(Mi, o, 1), normalize(xform(Mi, d, 0)));
-                        w = power_heuristic(prev_pdf, pdf * light_power / sc.total_light_power);
-                    }
-                    L = L + T * spectrum_texture4(sc, m.y, sp, lam) * w;
-                    ps.radiance[p] = to_f4(L);
-                } else {
-                    Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
-                    s4 albedo = s4_fill(0);
-                    if (m.x == kLambertian || m.x == kMirror) albedo = spectrum_texture4(sc, m.y, sp, lam);
-                    // next-event estimation (renderer.h:133-175)
-                    if (m.x == kLambertian && lights) {
-                        const float target = sc.total_light_power * rng.next();
-                        int li = sc.light_inst[0], lo = sc.light_obj[0];
-                        float lp = sc.light_power[0];
-                        for (int j = 0; j < sc.num_lights; j++) {
-                            if (sc.light_cdf[j] >= target) {
-                                li = sc.light_inst[j];
-                                lo = sc.light_obj[j];
-                                lp = sc.light_power[j];
-                                break;
-                            }
-                        }
-                        f3 ldir;
-                        float lpdf;
-                        if (li != -1) {
-                            const InstanceRef lr = instance_ref(sc, li);
-                            float M[16], Mi[16];
-                            lr.load_m(M, 0);
-                            lr.load_m(Mi, 1);
-                            const Prim pr = load_prim(sc, lo);
-                            const f3 lp_local = xform(Mi, sp.point, 1);
-                            ldir = normalize(xform(M, prim_sample(pr, lp_local, rng), 0));
-                            lpdf = prim_pdf(pr, lp_local, normalize(xform(Mi, ldir, 0)));
-                        } else {
-                            ldir = random_unit_vector(rng);
-                            lpdf = 1 / (4 * kPi);
-                        }
-                        const float cos_t = dot(nrm, ldir);
-                        if (lpdf > 0 && cos_t > 0) {
-                            lpdf *= lp / sc.total_light_power;
-                            // Lambertian evaluate/pdf toward the light (material.h:151-166)
-                            const float cl = dot(nrm, ldir);
-                            const s4 att = cl <= 0 ? s4_fill(0) : albedo / kPi;
-                            const float spdf = cl > 0 ? cl / kPi : 0;
-                            const float w = power_heuristic(lpdf, spdf);
-                            const s4 a = (T * att) * cos_t;
-                            ps.sh_o[p] = make_float4(sp.point.x, sp.point.y, sp.point.z, w);
-                            ps.sh_d[p] = make_float4(ldir.x, ldir.y, ldir.z, lpdf);
-                            ps.sh_a[p] = to_f4(a);
-                            ps.sh_light[p] = make_int2(li, lo);
-                            nee = true;
-                        }
-                    }
-                    // BSDF sampling (material.h:117-261)
-                    s4 att;
-                    f3 nd;
-                    float pdf = 0;
-                    bool spec = true;
-                    if (m.x == kLambertian) {
-                        nd = random_in_hemisphere(nrm, rng);
-                        const float cl = dot(nrm, nd);
-                        att = cl <= 0 ? s4_fill(0) : albedo / kPi;
-                        pdf = cl > 0 ? cl / kPi : 0;
-                        spec = false;
-                    } else if (m.x == kMirror) {
-                        nd = reflected(d, nrm);
-                        att = albedo;
-                    } else if (m.x == kDielectric) {
-                        const float factor = pow5(1 + dot(d, nrm));
-                        const float n0h = spectrum_at(sc, m.y, lam.v[0]);
-                        const float n1h = spectrum_at(sc, m.z, lam.v[0]);
-                        const float ratio = front ? n0h / n1h : n1h / n0h;
-                        float r0 = (n0h - n1h) / (n0h + n1h);
-                        r0 *= r0;
-                        const float rh = r0 + (1 - r0) * factor;
-                        const bool refl = rng.next() < rh;
-                        nd = refl ? reflected(d, nrm) : refracted(d, nrm, ratio);
-                        att.v[0] = 1;
-                        for (int k = 1; k < kHero; k++) {
-                            const float a0 = spectrum_at(sc, m.y, lam.v[k]);
-                            const float a1 = spectrum_at(sc, m.z, lam.v[k]);
-                            float rr = (a0 - a1) / (a0 + a1);
-                            rr *= rr;
-                            const float r = rr + (1 - rr) * factor;
-                            att.v[k] = refl ? r / rh
-                                            : (fabsf(a0 - n0h) < kEps && fabsf(a1 - n1h) < kEps) ? (1 - r) / (1 - rh) : 0;
-                        }
-                    } else {  // thin film (material.h:228-261)
-                        const int Lc = m.y < kMaxFilmLayers ? m.y : kMaxFilmLayers;
-                        float thick[kMaxFilmLayers];
-                        for (int k = 0; k < Lc; k++) thick[k] = scalar_texture(sc, sc.material_props[m.w + k], sp.point);
-                        const float cos0 = dot(nrm, -d);
-                        const int outer = sc.material_props[m.z], sub = sc.material_props[m.z + m.y + 1];
-                        const float n0h = float(cspectrum_at(sc, outer, lam.v[0]).x);
-                        const float n1h = float(cspectrum_at(sc, sub, lam.v[0]).x);
-                        const float ratio = front ? n0h / n1h : n1h / n0h;
-                        const float rh = thin_film_r(sc, m, front, cos0, lam.v[0], thick);
-                        const bool refl = rng.next() < rh;
-                        nd = refl ? reflected(d, nrm) : refracted(d, nrm, ratio);
-                        att.v[0] = 1;
-                        for (int k = 1; k < kHero; k++) {
-                            const float a0 = float(cspectrum_at(sc, outer, lam.v[k]).x);
-                            const float a1 = float(cspectrum_at(sc, sub, lam.v[k]).x);
-                            const float r = thin_film_r(sc, m, front, cos0, lam.v[k], thick);
-                            att.v[k] = refl ? r / rh
-                                            : (fabsf(a0 - n0h) < kEps && fabsf(a1 - n1h) < kEps) ? (1 - r) / (1 - rh) : 0;
-                        }
-                    }
-                    if (spec) T = T * att;
-                    else T = T * ((att * dot(nrm, nd)) / pdf);
-                    alive = true;
-                    if (bounce >= kRrStartDepth) {
-                        const float qq = 1 - clampf(s4_max(T), 0.05f, 0.95f);
-                        if (rng.next() < qq) alive = false;
-                        else T = T / (1 - qq);
-                    }
-                    if (bounce >= rp.depth) alive = false;
-                    ps.rng[p] = rng.state;
-                    ps.throughput[p] = to_f4(T);
-                    ps.ray_o[p] = make_float4(sp.point.x, sp.point.y, sp.point.z, pdf);
-                    ps.ray_d[p] = make_float4(nd.x, nd.y, nd.z, spec ? 1.0f : 0.0f);
+                const float factor = pow5(1 + dot(s.d, s.nrm));
+                const float n0h = spectrum_at(sc, s.m.y, s.lam.v[0]);
+                const float n1h = spectrum_at(sc, s.m.z, s.lam.v[0]);
+                const float ratio = s.front ? n0h / n1h : n1h / n0h;
+                float r0 = (n0h - n1h) / (n0h + n1h);
+                r0 *= r0;
+                const float rh = r0 + (1 - r0) * factor;
+                const bool refl = rng.next() < rh;
+                nd = refl ? reflected(s.d, s.nrm) : refracted(s.d, s.nrm, ratio);
+                att.v[0] = 1;
+                for (int k = 1; k < kHero; k++) {
+                    const float a0 = spectrum_at(sc, s.m.y, s.lam.v[k]);
+                    const float a1 = spectrum_at(sc, s.m.z, s.lam.v[k]);
+                    float rr = (a0 - a1) / (a0 + a1);
+                    rr *= rr;
+                    const float r = rr + (1 - rr) * factor;
+                    att.v[k] = refl ? r / rh : (fabsf(a0 - n0h) < kEps && fabsf(a1 - n1h) < kEps) ? (1 - r) / (1 - rh) : 0;
                 }
             }
+            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
         }
-        const int slot = warp_push(&ps.counts[bounce + 1], alive);
+        const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
-        const int sslot = warp_push(&ps.counts[rp.depth + 2 + bounce], nee);
-        if (nee) ps.shadow_queue[sslot] = p;
     }
 }
 
-__global__ void __launch_bounds__(256) k_shadow(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
-    const int n = ps.counts[rp.depth + 2 + bounce];
+// Thin-film reflectance (R_s + R_p) / 2 at the four hero wavelengths
+// (material.h:263-309), FP32 transfer matrix. Layer order and thicknesses
+// reverse on back-face hits. With non-dispersive indices the interfaces are
+// formed once for all four wavelengths.
+__device__ inline s4 thin_film_r4(const DeviceScene &sc, const int4 &m, bool front, float cos0, const s4 &lam,
+                                  const float *thickness) {
+    const int L = m.y < kMaxFilmLayers ? m.y : kMaxFilmLayers;
+    bool flat = true;
+    for (int k = 0; k < L + 2; k++) flat = flat && sc.cspectrum_flat[sc.material_props[m.z + k]];
+    s4 R;
+    if (flat && L <= 1) {
+        cx<float> n[3];
+        for (int k = 0; k < L + 2; k++) {
+            const int src = front ? k : L + 1 - k;
+            const double2 c = cspectrum_at(sc, sc.material_props[m.z + src], lam.v[0]);
+            n[k] = cx<float>{float(c.x), float(c.y)};
+        }
+        FilmPrep<float, 1> f;
+        film_prepare<float, 1>(L, n, cos0, f);
+#pragma unroll 1
+        for (int w = 0; w < kHero; w++) {
+            const FilmResult<float> r = film_apply<float, 1>(f, thickness, (2 * kPi) / lam.v[w], false);
+            R.v[w] = (r.rs + r.rp) * 0.5f;
+        }
+        return R;
+    }
+    float d[kMaxFilmLayers];
+    for (int k = 0; k < L; k++) d[k] = thickness[front ? k : L - 1 - k];
+#pragma unroll 1
+    for (int w = 0; w < kHero; w++) {
+        const float lambda = lam.v[w];
+        auto index_of = [&](int k) {
+            const int src = front ? k : L + 1 - k;
+            const double2 c = cspectrum_at(sc, sc.material_props[m.z + src], lambda);
+            return cx<float>{float(c.x), float(c.y)};
+        };
+        R.v[w] = film_reflectance_stream<float>(L, index_of, d, cos0, (2 * kPi) / lambda);
+    }
+    return R;
+}
+
+// Hero-wavelength reflect/refract choice and secondary-wavelength weights of the
+// thin film (material.h:228-261), given the four reflectances.
+__device__ __forceinline__ void thin_film_scatter(const DeviceScene &sc, const ShadeIn &s, const s4 &R, Rng &rng,
+                                                  s4 &att, f3 &nd) {
+    const int outer = sc.material_props[s.m.z], sub = sc.material_props[s.m.z + s.m.y + 1];
+    const float n0h = float(cspectrum_at(sc, outer, s.lam.v[0]).x);
+    const float n1h = float(cspectrum_at(sc, sub, s.lam.v[0]).x);
+    const float ratio = s.front ? n0h / n1h : n1h / n0h;
+    const float rh = R.v[0];
+    const bool refl = rng.next() < rh;
+    nd = refl ? reflected(s.d, s.nrm) : refracted(s.d, s.nrm, ratio);
+    att.v[0] = 1;
+    for (int k = 1; k < kHero; k++) {
+        const float a0 = float(cspectrum_at(sc, outer, s.lam.v[k]).x);
+        const float a1 = float(cspectrum_at(sc, sub, s.lam.v[k]).x);
+        const float r = R.v[k];
+        att.v[k] = refl ? r / rh : (fabsf(a0 - n0h) < kEps && fabsf(a1 - n1h) < kEps) ? (1 - r) / (1 - rh) : 0;
+    }
+}
+
+// Layer thicknesses of a thin-film hit: the thickness textures are evaluated once
+// per hit (the reference evaluates them once per wavelength at the same point).
+__device__ __forceinline__ void thin_film_thickness(const DeviceScene &sc, const ShadeIn &s, float *thick) {
+    const int L = s.m.y < kMaxFilmLayers ? s.m.y : kMaxFilmLayers;
+    for (int k = 0; k < L; k++) thick[k] = scalar_texture(sc, sc.material_props[s.m.w + k], s.sp.point);
+}
+
+// Thin film with the exact FP32 transfer matrix.
+LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    const int n = ps.counts[queue_slot(bounce, kQFilm)];
+    const int *q = ps.mat_queue[2];
+    int *q_next = ps.queue[(bounce + 1) & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int idx = base + threadIdx.x;
+        bool alive = false;
+        int p = 0;
+        if (idx < n) {
+            p = q[idx];
+            const ShadeIn s = load_shade(ps, sc, p);
+            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            float thick[kMaxFilmLayers];
+            thin_film_thickness(sc, s, thick);
+            const s4 R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+            s4 att;
+            f3 nd;
+            thin_film_scatter(sc, s, R, rng, att, nd);
+            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
+        }
+        const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
+        if (alive) q_next[slot] = p;
+    }
+}
+
+LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    extern __shared__ int stack_smem[];
+    SharedStack st_a, st_b;
+    thread_stacks(stack_smem, st_a, st_b);
+    const int n = ps.counts[queue_slot(bounce, kQShadow)];
     const int stride = gridDim.x * blockDim.x;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
         const int p = ps.shadow_queue[idx];
@@ -351,7 +480,7 @@ __global__ void __launch_bounds__(256) k_shadow(int bounce, RenderParams rp, Dev
         const f3 d = mk(dd.x, dd.y, dd.z);
         Hit lh;
         bool overflow = false;
-        if (!occluded(sc, mk(o.x, o.y, o.z), d, light.x, light.y, lh, overflow)) {
+        if (!occluded_t(sc, mk(o.x, o.y, o.z), d, light.x, light.y, lh, overflow, st_a, st_b)) {
             const s4 lam = from_f4(ps.lam[p]);
             s4 e;
             if (light.x != -1) {
@@ -375,7 +504,7 @@ __global__ void __launch_bounds__(256) k_shadow(int bounce, RenderParams rp, Dev
 }
 
 // Last sample into the film, then the average (renderer.h:84-91).
-__global__ void k_finish(RenderParams rp, DeviceScene sc, PathState ps, float *out) {
+LAMBDA_KERNEL void k_finish(RenderParams rp, DeviceScene sc, PathState ps, float *out) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= rp.num_pixels) return;
     const f3 rgb = spectrum_to_rgb(sc, from_f4(ps.radiance[p]), from_f4(ps.lam[p]), rp.lambda_range);

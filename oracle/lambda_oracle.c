@@ -845,11 +845,27 @@ void oracle_pcg(uint64_t seed, uint64_t stream, int n, float *out) {
 #define H 64
 static const int kIn = 5, kOut = 4;
 
+/* Round to the nearest BF16 value (ties to even), as the tensor-core path stores
+ * weights, inputs and hidden activations. */
+static double bf16(double v) {
+    float f = (float)v;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+static int g_round_bf16 = 0;
+
+void oracle_mlp_set_bf16(int on) { g_round_bf16 = on; }
+
 static void layer(const double *W, const double *b, const double *x, int nin, int nout, double *y, int relu) {
     for (int o = 0; o < nout; o++) {
         double a = b[o];
-        for (int i = 0; i < nin; i++) a += W[o * nin + i] * x[i];
-        y[o] = relu && a < 0 ? 0 : a;
+        for (int i = 0; i < nin; i++) a += (g_round_bf16 ? bf16(W[o * nin + i]) : W[o * nin + i]) * x[i];
+        a = relu && a < 0 ? 0 : a;
+        y[o] = relu && g_round_bf16 ? bf16(a) : a;
     }
 }
 
@@ -857,8 +873,9 @@ void oracle_mlp_forward(const double *p, const double *x, int n, double *y) {
     const double *W1 = p, *b1 = W1 + H * kIn, *W2 = b1 + H, *b2 = W2 + H * H, *W3 = b2 + H, *b3 = W3 + H * H;
     const double *W4 = b3 + H, *b4 = W4 + kOut * H;
     for (int r = 0; r < n; r++) {
-        double h1[H], h2[H], h3[H];
-        layer(W1, b1, x + kIn * r, kIn, H, h1, 1);
+        double h1[H], h2[H], h3[H], xr[5];
+        for (int i = 0; i < kIn; i++) xr[i] = g_round_bf16 ? bf16(x[kIn * r + i]) : x[kIn * r + i];
+        layer(W1, b1, xr, kIn, H, h1, 1);
         layer(W2, b2, h1, H, H, h2, 1);
         layer(W3, b3, h2, H, H, h3, 1);
         layer(W4, b4, h3, H, kOut, y + kOut * r, 0);
@@ -876,7 +893,8 @@ double oracle_mlp_grad(const double *p, const double *x, const double *t, int n,
     double loss = 0;
     const double scale = 1.0 / ((double)n * kOut);
     for (int r = 0; r < n; r++) {
-        const double *in = x + kIn * r;
+        double in[5];
+        for (int i = 0; i < kIn; i++) in[i] = g_round_bf16 ? bf16(x[kIn * r + i]) : x[kIn * r + i];
         double h1[H], h2[H], h3[H], y[4], dy[4], d3[H], d2[H], d1[H];
         layer(W1, b1, in, kIn, H, h1, 1);
         layer(W2, b2, h1, H, H, h2, 1);
@@ -893,7 +911,7 @@ double oracle_mlp_grad(const double *p, const double *x, const double *t, int n,
         }
         for (int i = 0; i < H; i++) {
             double a = 0;
-            for (int o = 0; o < kOut; o++) a += W4[o * H + i] * dy[o];
+            for (int o = 0; o < kOut; o++) a += (g_round_bf16 ? bf16(W4[o * H + i]) : W4[o * H + i]) * dy[o];
             d3[i] = h3[i] > 0 ? a : 0;
         }
         for (int o = 0; o < H; o++) {
@@ -902,7 +920,7 @@ double oracle_mlp_grad(const double *p, const double *x, const double *t, int n,
         }
         for (int i = 0; i < H; i++) {
             double a = 0;
-            for (int o = 0; o < H; o++) a += W3[o * H + i] * d3[o];
+            for (int o = 0; o < H; o++) a += (g_round_bf16 ? bf16(W3[o * H + i]) : W3[o * H + i]) * d3[o];
             d2[i] = h2[i] > 0 ? a : 0;
         }
         for (int o = 0; o < H; o++) {
@@ -911,7 +929,7 @@ double oracle_mlp_grad(const double *p, const double *x, const double *t, int n,
         }
         for (int i = 0; i < H; i++) {
             double a = 0;
-            for (int o = 0; o < H; o++) a += W2[o * H + i] * d2[o];
+            for (int o = 0; o < H; o++) a += (g_round_bf16 ? bf16(W2[o * H + i]) : W2[o * H + i]) * d2[o];
             d1[i] = h1[i] > 0 ? a : 0;
         }
         for (int o = 0; o < H; o++) {

@@ -36,6 +36,7 @@ def load():
         lib.oracle_mlp_forward.argtypes = [P, P, C.c_int, P]
         lib.oracle_mlp_grad.restype = C.c_double
         lib.oracle_mlp_grad.argtypes = [P, P, P, C.c_int, P]
+        lib.oracle_mlp_set_bf16.argtypes = [C.c_int]
         _lib = lib
     return _lib
 
@@ -96,7 +97,10 @@ def pcg(seed, stream, n) -> np.ndarray:
     return out
 
 
-def mlp_forward(params, x) -> np.ndarray:
+def mlp_forward(params, x, bf16: bool = False) -> np.ndarray:
+    """FP64 forward; bf16=True rounds weights, inputs and hidden activations to BF16
+    as the tensor-core kernel does (output layer weights too; biases stay FP32)."""
+    load().oracle_mlp_set_bf16(1 if bf16 else 0)
     p = np.ascontiguousarray(params, np.float64)
     x = np.ascontiguousarray(x, np.float64).reshape(-1, 5)
     y = np.empty((x.shape[0], 4), np.float64)
@@ -104,7 +108,8 @@ def mlp_forward(params, x) -> np.ndarray:
     return y
 
 
-def mlp_grad(params, x, t):
+def mlp_grad(params, x, t, bf16: bool = False):
+    load().oracle_mlp_set_bf16(1 if bf16 else 0)
     p = np.ascontiguousarray(params, np.float64)
     x = np.ascontiguousarray(x, np.float64).reshape(-1, 5)
     t = np.ascontiguousarray(t, np.float64).reshape(-1, 4)
