@@ -322,7 +322,11 @@ lambda_status lambda_thinfilm_exact(lambda_ctx *ctx, const lambda_film_query *q,
 /* FP64 transfer matrix (the training labeller and error audit): out [n][4] doubles. */
 lambda_status lambda_thinfilm_fp64(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, double *out);
 
-/* Surrogate MLP 5->64->64->64->4 (ReLU hidden layers), BF16 weights. */
+/* Surrogate MLP 5->64->64->64->4 (ReLU hidden layers), BF16 weights. A query
+ * (lambda, cos theta, d, n_film, n_sub) enters encoded as (cos 2delta, sin 2delta,
+ * cos theta, n_film, n_sub), with 2delta = 4 pi n_film d cos(theta_film) / lambda
+ * the film's round-trip phase and the last three normalised to [-1, 1] over the
+ * trained range. */
 #define LAMBDA_MLP_IN 5
 #define LAMBDA_MLP_HIDDEN 64
 #define LAMBDA_MLP_OUT 4
@@ -372,8 +376,8 @@ lambda_status lambda_surrogate_get(const lambda_ctx *ctx, float *params, lambda_
 lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, float *out);
 
 /* One forward/backward of the training kernel on caller data, for gradient
- * checks: params [LAMBDA_MLP_PARAMS], x [n][5] inputs already normalised to
- * [-1, 1], y [n][4] targets (host memory, n <= 65536). Writes the mean squared
+ * checks: params [LAMBDA_MLP_PARAMS], x [n][5] already-encoded inputs,
+ * y [n][4] targets (host memory, n <= 65536). Writes the mean squared
  * error over the 4 outputs and its gradient with respect to params. The forward
  * pass rounds weights, inputs and hidden activations to BF16 as inference does. */
 lambda_status lambda_surrogate_grad(lambda_ctx *ctx, const float *params, const float *x, const float *y, int32_t n,

@@ -76,6 +76,27 @@ struct Range {
 
 __host__ __device__ inline float normalise(float v, float lo, float hi) { return 2.0f * (v - lo) / (hi - lo) - 1.0f; }
 
+// Input encoding of one film query (lambda, cos theta in air, thickness, n_film,
+// n_sub): the film's round-trip phase 2 delta = 4 pi n_f d cos(theta_f) / lambda
+// (Snell: sin theta_f = sin theta / n_f) enters as (cos 2 delta, sin 2 delta), so
+// the network sees the interference term as a smooth periodic feature; the angle
+// and the two indices are normalised to [-1, 1]. The wavelength and thickness
+// ranges bound the trained domain (and the phase), not the encoding.
+__host__ __device__ inline void encode(const float *v, const Range &rg, float *x) {
+    const float c0 = v[1], nf = v[3];
+    const float cf = sqrtf(fmaxf(1.0f - (1.0f - c0 * c0) / (nf * nf), 0.0f));
+    const float two_delta = 4.0f * 3.14159265358979f * nf * v[2] * cf / v[0];
+#ifdef __CUDA_ARCH__
+    sincosf(two_delta, &x[1], &x[0]);
+#else
+    x[0] = std::cos(two_delta);
+    x[1] = std::sin(two_delta);
+#endif
+    x[2] = normalise(c0, rg.lo[1], rg.hi[1]);
+    x[3] = normalise(nf, rg.lo[3], rg.hi[3]);
+    x[4] = normalise(v[4], rg.lo[4], rg.hi[4]);
+}
+
 __device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 // ---------------------------------------------------------------------------
@@ -292,7 +313,9 @@ __global__ void k_film_labels(uint64_t seed, int64_t first, int n, Range rg, flo
     cx<double> idx[3] = {cx<double>{1.0, 0.0}, cx<double>{double(v[3]), 0.0}, cx<double>{double(v[4]), 0.0}};
     const double d = v[2];
     const FilmResult<double> r = film_stack<double, 1>(1, idx, &d, double(v[1]), double(v[0]));
-    for (int k = 0; k < kIn; k++) x[size_t(i) * kRowStride + k] = normalise(v[k], rg.lo[k], rg.hi[k]);
+    float e[kIn];
+    encode(v, rg, e);
+    for (int k = 0; k < kIn; k++) x[size_t(i) * kRowStride + k] = e[k];
     for (int k = kIn; k < kRowStride; k++) x[size_t(i) * kRowStride + k] = 0.0f;
     y[size_t(i) * 4] = float(r.rs);
     y[size_t(i) * 4 + 1] = float(r.rp);
@@ -471,14 +494,10 @@ __global__ void __launch_bounds__(256) k_film_inputs(int bounce, RenderParams rp
             float *row = rows + (size_t(idx) * kHero + w) * kRowStride;
             if (ok) {
                 const float v[kIn] = {s.lam.v[w], c0[w], d, nf[w], ns[w]};
-                float4 a, b;
-                a.x = normalise(v[0], fs.rg.lo[0], fs.rg.hi[0]);
-                a.y = normalise(v[1], fs.rg.lo[1], fs.rg.hi[1]);
-                a.z = normalise(v[2], fs.rg.lo[2], fs.rg.hi[2]);
-                a.w = normalise(v[3], fs.rg.lo[3], fs.rg.hi[3]);
-                b = make_float4(normalise(v[4], fs.rg.lo[4], fs.rg.hi[4]), 0, 0, 0);
-                reinterpret_cast<float4 *>(row)[0] = a;
-                reinterpret_cast<float4 *>(row)[1] = b;
+                float e[kIn];
+                encode(v, fs.rg, e);
+                reinterpret_cast<float4 *>(row)[0] = make_float4(e[0], e[1], e[2], e[3]);
+                reinterpret_cast<float4 *>(row)[1] = make_float4(e[4], 0, 0, 0);
             } else {
                 reinterpret_cast<float4 *>(row)[0] = make_float4(0, 0, 0, 0);
                 reinterpret_cast<float4 *>(row)[1] = make_float4(0, 0, 0, 0);
@@ -716,7 +735,7 @@ extern "C" lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_fil
     std::vector<float> rows(size_t(n) * kRowStride, 0.0f);
     for (int i = 0; i < n; i++) {
         const float v[kIn] = {hq[i].lambda_nm, hq[i].cos_theta, hq[i].thickness_nm, hq[i].n_film, hq[i].n_sub};
-        for (int k = 0; k < kIn; k++) rows[size_t(i) * kRowStride + k] = normalise(v[k], rg.lo[k], rg.hi[k]);
+        encode(v, rg, &rows[size_t(i) * kRowStride]);
     }
     DeviceBuffer din, dout;
     CK(din.upload(rows.data(), rows.size() * 4, ctx->stream), "stage queries");
@@ -860,7 +879,7 @@ extern "C" lambda_status lambda_surrogate_train(lambda_ctx *ctx, const lambda_tr
 }
 
 // One training-kernel forward/backward on caller data (for gradient checks):
-// x [n][5] normalised inputs, y [n][4] targets, n <= 64 * 1024; writes the mean
+// x [n][5] encoded inputs, y [n][4] targets, n <= 64 * 1024; writes the mean
 // squared error and its gradient w.r.t. params.
 extern "C" lambda_status lambda_surrogate_grad(lambda_ctx *ctx, const float *params, const float *x, const float *y,
                                                int32_t n, float *grad_out, float *loss_out) {

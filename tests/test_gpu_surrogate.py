@@ -10,7 +10,7 @@ import pytest
 
 import lambda_b200 as lb
 from lambda_b200 import _native as N
-from lambda_b200 import scenes
+from lambda_b200 import scenes, surrogate
 from oracle import port
 from tests.helpers import rel_rmse
 
@@ -49,10 +49,7 @@ def test_tensor_core_inference_matches_fp64_forward(ctx):
     q = np.stack([rng.uniform(380, 780, 5000), rng.uniform(0, 1, 5000), rng.uniform(150, 850, 5000),
                   rng.uniform(1.2, 1.8, 5000), rng.uniform(1.0, 2.0, 5000)], 1).astype(np.float32)
     got = ctx.surrogate_eval(q)
-    r = lb.default_film_range()
-    lo = np.array([r.lambda_nm[0], r.cos_theta[0], r.thickness_nm[0], r.n_film[0], r.n_sub[0]], np.float32)
-    hi = np.array([r.lambda_nm[1], r.cos_theta[1], r.thickness_nm[1], r.n_film[1], r.n_sub[1]], np.float32)
-    x = (2.0 * (q - lo) / (hi - lo) - 1.0).astype(np.float32)
+    x = surrogate.encode(q, lb.default_film_range())
     want = port.mlp_forward(p.astype(np.float64), x, bf16=True)
     err = np.abs(got - want)
     scale = np.abs(want).max()
@@ -65,30 +62,54 @@ def test_tensor_core_inference_matches_fp64_forward(ctx):
 
 @pytest.fixture(scope="module")
 def trained(ctx):
-    rep = ctx.surrogate_train(samples=1 << 21, epochs=4, batch=4096, lr=3e-3, seed=11)
+    rep = ctx.surrogate_train(samples=1 << 21, epochs=4, batch=8192, lr=3e-3, seed=11)
     print(f"train {rep.train_ms:.0f} ms, labels {rep.label_ms:.0f} ms, loss {rep.final_loss:.3e}, "
           f"audit max {rep.max_abs_error:.3e} mean {rep.mean_abs_error:.3e}")
     return rep
 
 
 def test_short_training_run(trained, ctx):
-    assert trained.final_loss < 1e-3
+    """The training kernels learn: 1024 Adam steps on 2^21 samples."""
+    # a short run (1024 Adam steps); the shipped weights train 24 epochs of 2^24 samples
+    assert trained.final_loss < 2e-3
     assert trained.mean_abs_error < 0.02
     q = np.array([[550, 0.8, 400, 1.33, 1.5]], np.float32)
     out = ctx.surrogate_eval(q)
     want = ctx.thinfilm_fp64(q)
     assert np.abs(out - want).max() < 0.1
+    assert trained.audit_samples == 1 << 18
 
 
-def test_surrogate_render_close_to_exact(trained, scene_dir, ctx):
-    sc = scenes.thinfilm_spheres(scene_dir, 96, 54, 16, name="s_thinfilm.lrd")
+def test_trained_weights_accuracy(ctx):
+    """The shipped weights (lambda_b200/data) against the FP64 transfer matrix."""
+    surrogate.install(ctx)
+    rng = np.random.default_rng(5)
+    n = 100000
+    q = np.stack([rng.uniform(380, 780, n), rng.uniform(0, 1, n), rng.uniform(150, 850, n),
+                  rng.uniform(1.2, 1.8, n), rng.uniform(1.0, 2.0, n)], 1).astype(np.float32)
+    a, b = ctx.surrogate_eval(q), ctx.thinfilm_fp64(q)
+    e = np.abs((a[:, 0] + a[:, 1]) / 2 - (b[:, 0] + b[:, 1]) / 2)
+    print(f"R error vs FP64: mean {e.mean():.2e}, p99 {np.quantile(e, 0.99):.2e}, max {e.max():.2e}")
+    assert e.mean() < 3e-3 and np.quantile(e, 0.99) < 2e-2
+
+
+def test_surrogate_render_unbiased(scene_dir, ctx):
+    """A noisy render differs from the exact form's by no more than a second exact
+    render (another seed) does, plus 1%; the image means agree within 2%."""
+    surrogate.install(ctx)
+    sc = scenes.thinfilm_spheres(scene_dir, 96, 54, 256, name="s_thinfilm.lrd")
     scene = lb.HostScene.parse(sc.lrd)
     ctx.upload(scene)
-    exact = ctx.render(scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_EXACT))
-    sur = ctx.render(scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_SURROGATE))
+    exact_a = ctx.render(scene.render_desc(seed=3, flags=lb.RENDER_THINFILM_EXACT))
+    exact_b = ctx.render(scene.render_desc(seed=4, flags=lb.RENDER_THINFILM_EXACT))
+    sur_b = ctx.render(scene.render_desc(seed=4, flags=lb.RENDER_THINFILM_SURROGATE))
     st = ctx.stats()
-    err = rel_rmse(sur, exact)
-    print(f"surrogate vs exact relRMSE {err:.3e}; thin-film hits {st.thinfilm_hits}, exact fallback {st.thinfilm_fallback}")
-    assert np.isfinite(sur).all()
-    assert st.thinfilm_hits > 0 and st.thinfilm_fallback < st.thinfilm_hits
-    assert err < 0.05
+    floor = rel_rmse(exact_b, exact_a)
+    err = rel_rmse(sur_b, exact_a)
+    ratio = float(sur_b.mean() / exact_b.mean())
+    print(f"relRMSE vs exact(seed 3): surrogate {err:.4f}, exact(seed 4) {floor:.4f}; mean ratio {ratio:.4f}; "
+          f"thin-film hits {st.thinfilm_hits}, exact fallback {st.thinfilm_fallback}")
+    assert np.isfinite(sur_b).all()
+    assert st.thinfilm_hits > 0 and st.thinfilm_fallback < 0.05 * st.thinfilm_hits
+    assert err <= floor + 0.01
+    assert abs(ratio - 1) < 0.02
