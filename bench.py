@@ -209,6 +209,58 @@ def run_reference(args):
 # GPU arm
 # ---------------------------------------------------------------------------
 
+def _xyz(img):
+    from tests.helpers import to_xyz
+
+    return to_xyz(img)
+
+
+def image_quality(ctx, scene, dev_out) -> dict:
+    """relRMSE (linear XYZ) of surrogate and exact frames against an exact frame of
+    another seed, at full resolution (noise-dominated at 256 spp) and averaged over
+    8x8 pixel blocks (noise /8, so the remainder estimates bias)."""
+    import lambda_b200 as lb
+
+    frames = {}
+    for name, seed, flags in (("exact_a", 3, lb.RENDER_THINFILM_EXACT), ("exact_b", 4, lb.RENDER_THINFILM_EXACT),
+                              ("surrogate_b", 4, lb.RENDER_THINFILM_SURROGATE)):
+        ctx.render(scene.render_desc(seed=seed, flags=flags | lb.RENDER_OUTPUT_DEVICE), out=dev_out)
+        frames[name] = dev_out.cpu().numpy().copy()
+
+    finite = np.isfinite(frames["exact_a"]).all(2) & np.isfinite(frames["exact_b"]).all(2) & \
+        np.isfinite(frames["surrogate_b"]).all(2)
+    for f in frames.values():
+        f[~finite] = 0.0  # the reference also yields 0/0 on the rare tangent-plane cosine sample
+
+    def rel(a, b, block=1):
+        if block > 1:
+            h, w = (a.shape[0] // block) * block, (a.shape[1] // block) * block
+            a = a[:h, :w].reshape(h // block, block, w // block, block, 3).mean((1, 3))
+            b = b[:h, :w].reshape(h // block, block, w // block, block, 3).mean((1, 3))
+        xa, xb = _xyz(a), _xyz(b)
+        return float(np.linalg.norm(xa - xb) / np.linalg.norm(xb))
+
+    ea, eb, sb = frames["exact_a"], frames["exact_b"], frames["surrogate_b"]
+    return {"relrmse_surrogate_vs_exact": rel(sb, ea), "relrmse_exact_vs_exact_noise_floor": rel(eb, ea),
+            "relrmse_surrogate_vs_exact_8x8": rel(sb, ea, 8), "relrmse_exact_vs_exact_8x8": rel(eb, ea, 8),
+            "mean_ratio_surrogate_over_exact": float(sb.mean() / eb.mean()),
+            "non_finite_pixels_excluded": int((~finite).sum()),
+            "note": "different seeds; the exact-vs-exact figures are the noise floor of one 256-spp frame"}
+
+
+def surrogate_error(ctx) -> dict:
+    """Per-result error of R = (R_s + R_p)/2 against the FP64 transfer matrix."""
+    rng = np.random.default_rng(5)
+    n = 1 << 18
+    q = np.stack([rng.uniform(380, 780, n), rng.uniform(0, 1, n), rng.uniform(150, 850, n),
+                  rng.uniform(1.2, 1.8, n), rng.uniform(1.0, 2.0, n)], 1).astype(np.float32)
+    a, b = ctx.surrogate_eval(q), ctx.thinfilm_fp64(q)
+    e = np.abs((a[:, 0] + a[:, 1]) / 2 - (b[:, 0] + b[:, 1]) / 2)
+    eo = np.abs(a - b)
+    return {"samples": n, "R_mean_abs": float(e.mean()), "R_p99_abs": float(np.quantile(e, 0.99)),
+            "R_max_abs": float(e.max()), "outputs_mean_abs": float(eo.mean()), "outputs_max_abs": float(eo.max())}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -218,6 +270,7 @@ def main():
     ap.add_argument("--mode", default="auto", choices=["auto", "surrogate", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--no-compare", action="store_true", help="skip the exact-form comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -280,6 +333,24 @@ def main():
     # per-stage kernel times (CUDA events inside the library) for the roofline
     stage = lb.stage_profile(ctx, desc, dev_out)
 
+    # the exact transfer-matrix form over the same steps, and image quality
+    comparison = None
+    if mode == "surrogate" and not args.no_compare:
+        exact_desc = scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_EXACT | lb.RENDER_OUTPUT_DEVICE)
+        ctx.render(exact_desc, out=dev_out)
+        ex_ms = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ctx.render(exact_desc, out=dev_out)
+            ex_ms += ctx.stats().render_ms
+        ex_ms = max_over_ranks(ex_ms, world)
+        ex_value = world * paths_per_step * args.steps / (ex_ms / 1000.0)
+        comparison = {"exact_tmm_value": ex_value, "exact_tmm_ms_per_step": ex_ms / args.steps,
+                      "surrogate_over_exact": value / ex_value}
+        if rank == 0:
+            comparison["quality"] = image_quality(ctx, scene, dev_out)
+
     # end to end through the C ABI with host buffers
     host_out = torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy()
     e2e_desc = scene.render_desc(seed=sc.seed, flags=flags)
@@ -312,7 +383,13 @@ def main():
             "roofline": roof,
             "stages": stage,
             "segments_per_path": stats[-1].segments / stats[-1].paths,
+            "thinfilm": {"hits_per_step": stats[-1].thinfilm_hits,
+                         "exact_fallback_per_step": stats[-1].thinfilm_fallback},
         }
+        if comparison is not None:
+            out["surrogate_vs_exact"] = comparison
+            if mode == "surrogate":
+                out["surrogate_error_vs_fp64"] = surrogate_error(ctx)
         if not args.no_cpu_baseline:
             cb = cpu_baseline(sc.lrd, sc.seed)
             if cb is not None:
