@@ -375,6 +375,22 @@ lambda_status lambda_surrogate_get(const lambda_ctx *ctx, float *params, lambda_
 /* Surrogate inference on the tensor cores: out [n][4] = (R_s, R_p, T_s, T_p). */
 lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_film_query *q, int32_t n, float *out);
 
+/* Allocation-free surrogate evaluation, for callers that must not allocate device
+ * memory where they evaluate films (a host renderer whose device memory belongs to
+ * its own pool allocator, such as a game engine or plug-in host, and whose render
+ * thread may not call cudaMalloc, which can synchronise the device and fail under
+ * the host's memory budget). It has no counterpart in the reference.
+ * queries [n] and out [n][4] = (R_s, R_p, T_s, T_p) are caller-owned DEVICE
+ * memory (out 16-byte aligned); results equal lambda_surrogate_eval's. The only
+ * scratch is a fixed array of LAMBDA_SURROGATE_STATIC_MAX_QUERIES encoded queries
+ * (4 MiB) compiled into the library, held by every GPU that loads it until the
+ * process exits; n above the limit returns LAMBDA_ERR_INVALID_ARGUMENT. The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture. Every call shares the array:
+ * calls that overlap on the GPU race. The call blocks until `out` is written. */
+#define LAMBDA_SURROGATE_STATIC_MAX_QUERIES 131072
+lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lambda_film_query *queries, int32_t n, float *out);
+
 /* One forward/backward of the training kernel on caller data, for gradient
  * checks: params [LAMBDA_MLP_PARAMS], x [n][5] already-encoded inputs,
  * y [n][4] targets (host memory, n <= 65536). Writes the mean squared

@@ -158,6 +158,7 @@ _SIGNATURES = {
     "lambda_surrogate_get": (C.c_int, [_P, _P, C.POINTER(FilmRange)]),
     "lambda_surrogate_eval": (C.c_int, [_P, _P, C.c_int32, _P]),
     "lambda_surrogate_grad": (C.c_int, [_P, _P, _P, _P, C.c_int32, _P, _P]),
+    "lambda_surrogate_eval_static": (C.c_int, [_P, _P, C.c_int32, _P]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "engine.h"
@@ -906,5 +907,103 @@ extern "C" lambda_status lambda_surrogate_grad(lambda_ctx *ctx, const float *par
     CK(cudaStreamSynchronize(ctx->stream), "gradient");
     if (loss_out) *loss_out = l;
     for (DeviceBuffer *b : {&dp, &dx, &dy, &dg, &dl}) b->release();
+    return LAMBDA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free surrogate evaluation.
+//
+// Some callers cannot call cudaMalloc at the point where they evaluate films: a
+// host renderer whose device memory belongs to its own pool allocator (a game
+// engine, a DCC plug-in host) and whose render thread must not allocate, because
+// cudaMalloc can synchronise the device and can fail under the host's memory
+// budget. For them, lambda_surrogate_eval_static takes caller-owned device
+// buffers and keeps its only scratch, the encoded network inputs, in a fixed
+// array compiled into this library: kStaticMaxQueries queries (4 MiB), held by
+// every GPU that loads the library until the process exits. The array is shared
+// by all calls and keeps the last call's contents; calls that overlap on the GPU
+// (other streams, other threads, other contexts on the same device) race on it.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kStaticMaxQueries = LAMBDA_SURROGATE_STATIC_MAX_QUERIES;
+static_assert(kStaticMaxQueries == 131072, "header and library disagree");
+
+static __device__ __align__(256) float g_static_rows[kStaticMaxQueries * mlp::kRowStride];
+static __device__ __align__(256) int g_static_error[4];
+
+// Device addresses of the two arrays, looked up once per device. In host code the
+// array names are host-side stand-ins, never device addresses.
+struct StaticScratch {
+    float *rows = nullptr;
+    int *error = nullptr;
+    bool ready = false;
+};
+constexpr int kMaxDevices = 64;
+StaticScratch g_static_scratch[kMaxDevices];
+std::mutex g_static_mutex;
+
+lambda_status static_scratch(lambda_ctx *ctx, StaticScratch &out) {
+    if (ctx->device < 0 || ctx->device >= kMaxDevices) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "device index too large");
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    StaticScratch &s = g_static_scratch[ctx->device];
+    if (!s.ready) {
+        CK(cudaSetDevice(ctx->device), "cudaSetDevice");  // the lookup is per device: this device must be current
+        void *rows = nullptr, *err = nullptr;
+        CK(cudaGetSymbolAddress(&rows, g_static_rows), "look up the static scratch array");
+        CK(cudaGetSymbolAddress(&err, g_static_error), "look up the static error word");
+        s.rows = static_cast<float *>(rows);
+        s.error = static_cast<int *>(err);
+        s.ready = true;
+    }
+    out = s;
+    return LAMBDA_OK;
+}
+
+__global__ void k_encode_queries(const lambda_film_query *q, int n, mlp::Range rg, float *rows) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v[mlp::kIn] = {q[i].lambda_nm, q[i].cos_theta, q[i].thickness_nm, q[i].n_film, q[i].n_sub};
+    float e[mlp::kIn];
+    mlp::encode(v, rg, e);
+    float *row = rows + size_t(i) * mlp::kRowStride;
+    reinterpret_cast<float4 *>(row)[0] = make_float4(e[0], e[1], e[2], e[3]);
+    reinterpret_cast<float4 *>(row)[1] = make_float4(e[4], 0.0f, 0.0f, 0.0f);
+}
+
+}  // namespace
+
+extern "C" lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lambda_film_query *queries, int32_t n,
+                                                      float *out) {
+    if (!ctx) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (n < 0 || n > kStaticMaxQueries)
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT,
+                         "lambda_surrogate_eval_static: n must be in [0, 131072] (LAMBDA_SURROGATE_STATIC_MAX_QUERIES); "
+                         "split larger batches into several calls");
+    if (!ctx->has_surrogate) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed");
+    if (n == 0) return LAMBDA_OK;
+    if (!queries || !out || !is_device_pointer(queries) || !is_device_pointer(out))
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "lambda_surrogate_eval_static takes device pointers only");
+    if (reinterpret_cast<uintptr_t>(out) % 16 != 0)
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "lambda_surrogate_eval_static: out must be 16-byte aligned");
+    StaticScratch sc;
+    lambda_status st = static_scratch(ctx, sc);
+    if (st != LAMBDA_OK) return st;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+    CK(cudaMemsetAsync(sc.error, 0, sizeof(int) * 4, ctx->stream), "clear the static error word");
+    k_encode_queries<<<(n + 255) / 256, 256, 0, ctx->stream>>>(queries, n, to_range(ctx->surrogate_range), sc.rows);
+    const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
+    const int tiles = (n + kTileM - 1) / kTileM;
+    const int grid = std::max(1, std::min(tiles, mlp_grid(ctx)));
+    k_mlp_tc<<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w),
+                                                     reinterpret_cast<const float *>(w + kPackedWeightBytes), sc.rows,
+                                                     nullptr, 0, n, reinterpret_cast<float4 *>(out), sc.error);
+    CK(cudaGetLastError(), "launch MLP kernel");
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, sc.error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "read the static error word");
+    CK(cudaStreamSynchronize(ctx->stream), "MLP inference");
+    if (herr & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
     return LAMBDA_OK;
 }
