@@ -384,7 +384,8 @@ def main():
             "stages": stage,
             "segments_per_path": stats[-1].segments / stats[-1].paths,
             "thinfilm": {"hits_per_step": stats[-1].thinfilm_hits,
-                         "exact_fallback_per_step": stats[-1].thinfilm_fallback},
+                         "exact_fallback_per_step": stats[-1].thinfilm_fallback,
+                         "surrogate_ctas_per_sm": stats[-1].surrogate_ctas_per_sm},
         }
         if comparison is not None:
             out["surrogate_vs_exact"] = comparison

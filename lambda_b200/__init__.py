@@ -179,6 +179,7 @@ class RenderStats:
     thinfilm_fallback: int
     kernel_launches: int
     waves: int
+    surrogate_ctas_per_sm: int
 
 
 def _ptr(a) -> int:
@@ -240,7 +241,7 @@ class Context:
         st = N.RenderStats()
         self._check(self._lib.lambda_get_render_stats(self._h, C.byref(st)))
         return RenderStats(st.render_ms, st.paths, st.segments, st.shadow_rays, st.thinfilm_hits,
-                           st.thinfilm_fallback, st.kernel_launches, st.waves)
+                           st.thinfilm_fallback, st.kernel_launches, st.waves, st.surrogate_ctas_per_sm)
 
     def stage_times(self) -> dict:
         arr = (N.StageTime * N.NUM_STAGES)()
@@ -366,7 +367,7 @@ def stage_profile(ctx: "Context", desc, out) -> dict:
 def roofline(stages: dict, hbm_gbs: float, bf16_tflops: float, peak_kind: str) -> dict:
     """Roofline entry for the stage with the largest device time."""
     name, s = max(((k, v) for k, v in stages.items() if v["ms"] > 0), key=lambda kv: kv[1]["ms"])
-    if name == "film_mlp":
+    if name == "film_surrogate":
         flops = 17536.0 * s["items"] * 4  # 2*(5*64+64*64+64*64+64*4) per (hit, wavelength)
         achieved = flops / (s["ms"] / 1000.0) / 1e12
         return {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": bf16_tflops, "unit": "TFLOP/s",

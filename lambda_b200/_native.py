@@ -38,7 +38,7 @@ RENDER_OUTPUT_DEVICE = 2
 RENDER_PROFILE_STAGES = 4
 NUM_STAGES = 12
 STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
-               "shadow", "finish", "film_inputs", "film_mlp", "film_scatter")
+               "shadow", "finish", "film_surrogate", "film_fallback", "unused")
 
 
 class LambdaError(RuntimeError):
@@ -108,7 +108,8 @@ class RenderDesc(C.Structure):
 class RenderStats(C.Structure):
     _fields_ = [("render_ms", C.c_double), ("paths", C.c_int64), ("segments", C.c_int64),
                 ("shadow_rays", C.c_int64), ("thinfilm_hits", C.c_int64), ("thinfilm_fallback", C.c_int64),
-                ("kernel_launches", C.c_int32), ("waves", C.c_int32)]
+                ("kernel_launches", C.c_int32), ("waves", C.c_int32), ("surrogate_ctas_per_sm", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class StageTime(C.Structure):

@@ -553,6 +553,7 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     CK(r.qm0.reserve(P * 4), "allocate queues");
     CK(r.qm1.reserve(P * 4), "allocate queues");
     CK(r.qm2.reserve(P * 4), "allocate queues");
+    CK(r.qm3.reserve(P * 4), "allocate queues");
     CK(r.counts.reserve(size_t(kQueues * (depth + 2)) * 4), "allocate queues");
     CK(r.wave.reserve(16), "allocate queues");
     CK(r.stats.reserve(8 * 8), "allocate statistics");
@@ -579,6 +580,7 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     ps.mat_queue[0] = r.qm0.as<int>();
     ps.mat_queue[1] = r.qm1.as<int>();
     ps.mat_queue[2] = r.qm2.as<int>();
+    ps.mat_queue[3] = r.qm3.as<int>();
     ps.counts = r.counts.as<int>();
     ps.wave = r.wave.as<int>();
     ps.stats = r.stats.as<unsigned long long>();
@@ -665,7 +667,7 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
             if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
             if (sc.families & 4u) {
                 if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, qgrid, pr);
-                else timed(6, [&] { k_shade_film_exact<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+                else timed(6, [&] { k_shade_film_exact<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps, false); });
             }
             if (sc.families & 1u) timed(7, [&] { k_shadow<<<qgrid, 256, stack_smem, stream>>>(b, rp, sc, ps); });
         }
@@ -728,6 +730,7 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
     ctx->stats.thinfilm_fallback = int64_t(stats[3]);
     ctx->stats.kernel_launches = launches;
     ctx->stats.waves = rp.samples;
+    ctx->stats.surrogate_ctas_per_sm = surrogate ? ctx->mlp_ctas_per_sm : 0;
     if (profile) {
         prof.totals[0] = 0;
         for (int i = 0; i < LAMBDA_NUM_STAGES; i++) {
@@ -744,7 +747,8 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
         ctx->stage_times[6].items = surrogate ? 0 : ctx->stats.thinfilm_hits;
         ctx->stage_times[7].items = ctx->stats.shadow_rays;
         ctx->stage_times[8].items = P;
-        for (int k = 9; k < 12; k++) ctx->stage_times[k].items = surrogate ? ctx->stats.thinfilm_hits : 0;
+        ctx->stage_times[9].items = surrogate ? ctx->stats.thinfilm_hits : 0;
+        ctx->stage_times[10].items = surrogate ? ctx->stats.thinfilm_fallback : 0;
     }
     if (err[0] & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
     if (err[0] & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");

@@ -44,7 +44,7 @@ struct SceneBuffers {
 
 struct RenderBuffers {
     DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
-        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out;
+        q0, q1, qs, qm0, qm1, qm2, qm3, counts, wave, stats, error, out;
     // thin-film surrogate batch
     DeviceBuffer tf_queue, tf_in, tf_out;
 };
@@ -75,6 +75,7 @@ struct lambda_ctx {
 
     // surrogate
     bool has_surrogate = false;
+    int mlp_ctas_per_sm = 0;  // resident CTAs of the tensor-core MLP kernel per SM
     lambda_film_range surrogate_range{};
     SurrogateBuffers sbuf;
 
@@ -95,7 +96,7 @@ struct lambda_ctx {
                 &s.cspectrum_flat, &s.materials, &s.material_props, &s.scalar_tex, &s.spectrum_tex, &s.light_inst,
                 &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
-                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
+                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.qm3, &r.counts, &r.wave,
                 &r.stats, &r.error, &r.out, &r.tf_queue, &r.tf_in, &r.tf_out, &sbuf.weights_bf16,
                 &sbuf.weights_f32, &sbuf.scratch};
     }

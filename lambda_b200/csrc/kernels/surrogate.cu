@@ -14,9 +14,10 @@
 //                    layout, no swizzle), tcgen05.mma with FP32 accumulators in tensor
 //                    memory, tcgen05.ld epilogues (bias, ReLU, BF16) writing the next
 //                    layer's operand back to shared memory
-// In a render, thin-film hits are turned into four MLP rows each (one per hero
-// wavelength) by k_film_inputs, evaluated by k_mlp_tc, and consumed by
-// k_film_scatter; hits outside the trained domain take the exact FP32 path.
+//   k_film_fused     the render's thin-film shade: rows of four hero wavelengths per
+//                    hit built in shared memory, the same tensor-core MLP tile, and
+//                    the scatter, in one kernel; hits outside the trained domain go
+//                    to the exact FP32 path's queue
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -175,26 +176,31 @@ __device__ __forceinline__ void put8(uint8_t *smem, int base, int r, int c, int 
     *reinterpret_cast<uint4 *>(smem + base + core_offset(r, c * 8, K)) = *reinterpret_cast<uint4 *>(p);
 }
 
-// in: rows x kRowStride floats (normalised inputs); out: rows x 4 floats.
-// error bit 1 is set if an MMA completion wait timed out.
-__global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed, const float *__restrict__ bias,
-                                                const float *__restrict__ in, const int *__restrict__ row_count,
-                                                int row_multiplier, int rows_fixed, float4 *__restrict__ out,
-                                                int *error) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int rows = row_count ? (*row_count) * row_multiplier : rows_fixed;
-    const int tiles = (rows + kTileM - 1) / kTileM;
-    if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
+// Sets up one CTA of a tensor-core MLP kernel: weights and biases into shared
+// memory, the completion mbarrier, and kTmemCols TMEM columns (warp 0 allocates).
+struct TileCtx {
+    uint32_t base;       // shared-memory address of smem[0]
+    uint32_t bar;        // MMA completion mbarrier
+    uint32_t tmem;       // TMEM accumulator base (lane 0, column 0)
+    uint32_t lane_base;  // this warp's 32 TMEM lanes
+    uint32_t phase;
+    const float *bias;   // b1 b2 b3 (64 each) b4 (16) in shared memory
+};
 
-    // weights and biases once per CTA
+__device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__restrict__ packed,
+                                              const float *__restrict__ bias) {
+    const int tid = threadIdx.x, warp = tid >> 5;
     for (int i = tid; i < kPackedWeightBytes / 16; i += blockDim.x) reinterpret_cast<uint4 *>(smem)[i] = packed[i];
     float *sb = reinterpret_cast<float *>(smem + sBias);
     for (int i = tid; i < 3 * kH + kOutPad; i += blockDim.x) sb[i] = bias[i];
-    const uint32_t bar = smem_u32(smem + sBar);
+    TileCtx t;
+    t.base = smem_u32(smem);
+    t.bar = smem_u32(smem + sBar);
+    t.phase = 0;
+    t.bias = sb;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + sTmem);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(t.bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -207,85 +213,111 @@ __global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t lane_base = tmem + (uint32_t(warp * 32) << 16);
-    const uint32_t base = smem_u32(smem);
-    const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
-    uint32_t phase = 0;
-    bool ok = true;
-    const uint32_t kPoll = 1u << 22;
+    t.tmem = *tmem_slot;
+    t.lane_base = t.tmem + (uint32_t(warp * 32) << 16);
+    return t;
+}
 
-    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const int r = warp * 32 + lane;  // this thread's row (its TMEM lane)
-        const int row = tile * kTileM + r;
-        // ---- layer 1 operand: normalised inputs, bf16, padded to K = 16
-        {
-            float x[16];
-#pragma unroll
-            for (int i = 0; i < 16; i++) x[i] = 0.0f;
-            if (row < rows) {
-                const float4 a = *reinterpret_cast<const float4 *>(in + size_t(row) * kRowStride);
-                const float b = in[size_t(row) * kRowStride + 4];
-                x[0] = a.x;
-                x[1] = a.y;
-                x[2] = a.z;
-                x[3] = a.w;
-                x[4] = b;
-            }
-            put8(smem, sX, r, 0, kInPad, x);
-            put8(smem, sX, r, 1, kInPad, x + 8);
-        }
-        // ---- four layers
-#pragma unroll 1
-        for (int layer = 0; layer < 4; layer++) {
-            fence_proxy_async();
-            fence_before();
-            __syncthreads();
-            if (tid == 0) {
-                fence_after();
-                if (layer == 0) {
-                    mma_bf16(tmem, smem_desc(base + sX, 128, 256), smem_desc(base + sW1, 128, 256), id64, 0);
-                } else {
-                    const int wofs = layer == 1 ? sW2 : (layer == 2 ? sW3 : sW4);
-                    const uint32_t idesc = layer == 3 ? id16 : id64;
-#pragma unroll
-                    for (int kk = 0; kk < kH / 16; kk++)
-                        mma_bf16(tmem, smem_desc(base + sHid + kk * 256, 128, 1024),
-                                 smem_desc(base + wofs + kk * 256, 128, 1024), idesc, kk > 0);
-                }
-                mma_commit(bar);
-            }
-            ok = mbar_wait(bar, phase, kPoll);
-            phase ^= 1u;
-            fence_after();
-            if (!ok) break;
-            if (layer < 3) {
-                const float *bl = sb + layer * kH;
-#pragma unroll
-                for (int c = 0; c < kH / 16; c++) {
-                    float v[16];
-                    tmem_ld16(lane_base + c * 16, v);
-#pragma unroll
-                    for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + bl[c * 16 + i], 0.0f);
-                    put8(smem, sHid, r, 2 * c, kH, v);
-                    put8(smem, sHid, r, 2 * c + 1, kH, v + 8);
-                }
-            } else {
-                float v[16];
-                tmem_ld16(lane_base, v);
-                if (row < rows) {
-                    const float *b4 = sb + 3 * kH;
-                    out[row] = make_float4(v[0] + b4[0], v[1] + b4[1], v[2] + b4[2], v[3] + b4[3]);
-                }
-            }
-        }
-    }
-    if (!ok && tid == 0) atomicOr(error, 2);
-    // all TMEM reads are complete (tcgen05.ld waits) before the columns are released
+__device__ __forceinline__ void tile_teardown(const TileCtx &t) {
+    // every TMEM read has completed (tcgen05.ld waits) before the columns are released
     fence_before();
     __syncthreads();
     fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem), "r"(kTmemCols) : "memory");
+}
+
+// Four layers over the 128-row operand already stored in sX (row r = thread r).
+// On return y holds this thread's four outputs (bias included). Returns false,
+// uniformly across the CTA, if an MMA completion wait timed out.
+__device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
+    const int tid = threadIdx.x;
+    const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
+    const uint32_t kPoll = 1u << 22;
+#pragma unroll 1
+    for (int layer = 0; layer < 4; layer++) {
+        fence_proxy_async();
+        fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after();
+            if (layer == 0) {
+                mma_bf16(t.tmem, smem_desc(t.base + sX, 128, 256), smem_desc(t.base + sW1, 128, 256), id64, 0);
+            } else {
+                const int wofs = layer == 1 ? sW2 : (layer == 2 ? sW3 : sW4);
+                const uint32_t idesc = layer == 3 ? id16 : id64;
+#pragma unroll
+                for (int kk = 0; kk < kH / 16; kk++)
+                    mma_bf16(t.tmem, smem_desc(t.base + sHid + kk * 256, 128, 1024),
+                             smem_desc(t.base + wofs + kk * 256, 128, 1024), idesc, kk > 0);
+            }
+            mma_commit(t.bar);
+        }
+        const bool done = mbar_wait(t.bar, t.phase, kPoll);
+        t.phase ^= 1u;
+        fence_after();
+        if (!__syncthreads_and(done)) return false;
+        if (layer < 3) {
+            const float *bl = t.bias + layer * kH;
+#pragma unroll
+            for (int c = 0; c < kH / 16; c++) {
+                float v[16];
+                tmem_ld16(t.lane_base + c * 16, v);
+#pragma unroll
+                for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + bl[c * 16 + i], 0.0f);
+                put8(smem, sHid, tid, 2 * c, kH, v);
+                put8(smem, sHid, tid, 2 * c + 1, kH, v + 8);
+            }
+        } else {
+            float v[16];
+            tmem_ld16(t.lane_base, v);
+            const float *b4 = t.bias + 3 * kH;
+            for (int i = 0; i < kOut; i++) y[i] = v[i] + b4[i];
+        }
+    }
+    return true;
+}
+
+// Stores one encoded row (5 features, zero-padded to K = 16) as row r of sX.
+__device__ __forceinline__ void put_row(uint8_t *smem, int r, const float *e) {
+    float x[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) x[i] = i < kIn ? e[i] : 0.0f;
+    put8(smem, sX, r, 0, kInPad, x);
+    put8(smem, sX, r, 1, kInPad, x + 8);
+}
+
+// in: rows x kRowStride floats (encoded inputs); out: rows x 4 floats.
+// error bit 1 is set if an MMA completion wait timed out.
+__global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed, const float *__restrict__ bias,
+                                                const float *__restrict__ in, const int *__restrict__ row_count,
+                                                int row_multiplier, int rows_fixed, float4 *__restrict__ out,
+                                                int *error) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int tid = threadIdx.x;
+    const int rows = row_count ? (*row_count) * row_multiplier : rows_fixed;
+    const int tiles = (rows + kTileM - 1) / kTileM;
+    if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
+    TileCtx t = tile_setup(smem, packed, bias);
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const int row = tile * kTileM + tid;
+        float e[kIn] = {0, 0, 0, 0, 0};
+        if (row < rows) {
+            const float4 a = *reinterpret_cast<const float4 *>(in + size_t(row) * kRowStride);
+            e[0] = a.x;
+            e[1] = a.y;
+            e[2] = a.z;
+            e[3] = a.w;
+            e[4] = in[size_t(row) * kRowStride + 4];
+        }
+        put_row(smem, tid, e);
+        float y[kOut];
+        ok = mlp_tile(smem, t, y);
+        if (ok && row < rows) out[row] = make_float4(y[0], y[1], y[2], y[3]);
+    }
+    if (!ok && tid == 0) atomicOr(error, 2);
+    tile_teardown(t);
 }
 
 // ---------------------------------------------------------------------------
@@ -451,97 +483,97 @@ struct FilmSurrogate {
     float lam_lo, lam_hi, cos_lo, cos_hi, d_lo, d_hi, nf_lo, nf_hi, ns_lo, ns_hi;
 };
 
-// Writes four MLP rows per thin-film hit (one per hero wavelength) or marks the
-// hit for the exact path: the surrogate covers a single film with real indices
-// between air (index exactly 1) and a substrate, inside the trained box. Back-face
-// hits (light inside the substrate) are mapped to the equivalent incidence from air
-// by Snell's law, since a lossless stack reflects the same from both sides; total
-// internal reflection goes to the exact path.
-__global__ void __launch_bounds__(256) k_film_inputs(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
-                                                     FilmSurrogate fs, float *rows, int *fallback) {
+// Thin-film shade with the surrogate, one kernel per bounce: persistent CTAs of
+// four warps take 128 thin-film hits at a time, one per thread. Each thread loads
+// its hit, evaluates the film thickness and encodes the four hero-wavelength
+// queries (lambda, cos, thickness, n_film, n_sub) in registers; the CTA then runs
+// four 128-row tiles through the tensor-core MLP, tile k holding every hit's
+// wavelength k, so thread t reads its own four (R_s + R_p)/2 back from TMEM lane t;
+// finally each thread makes its hit's thin-film scatter (material.h:228-261) and
+// Russian roulette. The surrogate covers a single film with real indices between
+// air (index exactly 1) and a substrate inside the trained box. A back-face hit
+// (light inside the substrate) is mapped to the equivalent incidence from air by
+// Snell's law, since a lossless stack reflects the same from both sides. Hits
+// outside the domain or with total internal reflection go to the exact path's queue.
+__global__ void __launch_bounds__(128) k_film_fused(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
+                                                    FilmSurrogate fs, const uint4 *__restrict__ packed,
+                                                    const float *__restrict__ bias) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int tid = threadIdx.x;
     const int n = ps.counts[queue_slot(bounce, kQFilm)];
-    const int stride = gridDim.x * blockDim.x;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
-        const int p = ps.mat_queue[2][idx];
-        const ShadeIn s = load_shade(ps, sc, p);
-        bool ok = s.m.y == 1;
-        float d = 0;
-        if (ok) {
-            d = scalar_texture(sc, sc.material_props[s.m.w], s.sp.point);
-            ok = d >= fs.d_lo && d <= fs.d_hi;
-        }
-        const float cos_in = dot(s.nrm, -s.d);
-        float nf[kHero], ns[kHero], c0[kHero];
-        for (int w = 0; w < kHero && ok; w++) {
-            const double2 a = cspectrum_at(sc, sc.material_props[s.m.z], s.lam.v[w]);
-            const double2 b = cspectrum_at(sc, sc.material_props[s.m.z + 1], s.lam.v[w]);
-            const double2 c = cspectrum_at(sc, sc.material_props[s.m.z + 2], s.lam.v[w]);
-            ok = a.x == 1.0 && a.y == 0.0 && b.y == 0.0 && c.y == 0.0;
-            nf[w] = float(b.x);
-            ns[w] = float(c.x);
-            if (s.front) {
-                c0[w] = cos_in;
-            } else {
-                const float sin2 = ns[w] * ns[w] * (1 - cos_in * cos_in);
-                ok = ok && sin2 < 1.0f;
-                c0[w] = sqrtf(fmaxf(1 - sin2, 0.0f));
-            }
-            ok = ok && nf[w] >= fs.nf_lo && nf[w] <= fs.nf_hi && ns[w] >= fs.ns_lo && ns[w] <= fs.ns_hi &&
-                 c0[w] >= fs.cos_lo && c0[w] <= fs.cos_hi && s.lam.v[w] >= fs.lam_lo && s.lam.v[w] <= fs.lam_hi;
-        }
-        fallback[idx] = ok ? 0 : 1;
-        if (!ok) atomicAdd(reinterpret_cast<unsigned long long *>(&ps.stats[3]), 1ull);
-        for (int w = 0; w < kHero; w++) {
-            float *row = rows + (size_t(idx) * kHero + w) * kRowStride;
-            if (ok) {
-                const float v[kIn] = {s.lam.v[w], c0[w], d, nf[w], ns[w]};
-                float e[kIn];
-                encode(v, fs.rg, e);
-                reinterpret_cast<float4 *>(row)[0] = make_float4(e[0], e[1], e[2], e[3]);
-                reinterpret_cast<float4 *>(row)[1] = make_float4(e[4], 0, 0, 0);
-            } else {
-                reinterpret_cast<float4 *>(row)[0] = make_float4(0, 0, 0, 0);
-                reinterpret_cast<float4 *>(row)[1] = make_float4(0, 0, 0, 0);
-            }
-        }
-    }
-}
-
-// Reflectances from the surrogate's (R_s + R_p) / 2 (or the exact path for hits
-// marked by k_film_inputs), then the thin-film scatter (material.h:228-261).
-__global__ void __launch_bounds__(256, 3) k_film_scatter(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
-                                                         const float4 *mlp_out, const int *fallback) {
-    const int n = ps.counts[queue_slot(bounce, kQFilm)];
+    const int tiles = (n + kTileM - 1) / kTileM;
+    if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
     const int *q = ps.mat_queue[2];
     int *q_next = ps.queue[(bounce + 1) & 1];
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-        const int idx = base + threadIdx.x;
-        bool alive = false;
+    int *q_exact = ps.mat_queue[3];
+    TileCtx t = tile_setup(smem, packed, bias);
+    bool ok_tc = true;
+    for (int tile = blockIdx.x; tile < tiles && ok_tc; tile += gridDim.x) {
+        const int idx = tile * kTileM + tid;
+        const bool valid = idx < n;
         int p = 0;
-        if (idx < n) {
+        ShadeIn s;
+        bool ok = false;
+        float e[kHero][kIn];
+        if (valid) {
             p = q[idx];
-            const ShadeIn s = load_shade(ps, sc, p);
-            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
-            s4 R;
-            if (fallback[idx]) {
-                float thick[kMaxFilmLayers];
-                thin_film_thickness(sc, s, thick);
-                R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
-            } else {
-                for (int w = 0; w < kHero; w++) {
-                    const float4 o = mlp_out[size_t(idx) * kHero + w];
-                    R.v[w] = clampf((o.x + o.y) * 0.5f, 0.0f, 1.0f);
+            s = load_shade(ps, sc, p);
+            ok = s.m.y == 1;
+        }
+        if (ok) {
+            const float d = scalar_texture(sc, sc.material_props[s.m.w], s.sp.point);
+            const float cos_in = dot(s.nrm, -s.d);
+            ok = d >= fs.d_lo && d <= fs.d_hi;
+#pragma unroll
+            for (int w = 0; w < kHero; w++) {
+                const float lam = s.lam.v[w];
+                const double2 a = cspectrum_at(sc, sc.material_props[s.m.z], lam);
+                const double2 b = cspectrum_at(sc, sc.material_props[s.m.z + 1], lam);
+                const double2 c = cspectrum_at(sc, sc.material_props[s.m.z + 2], lam);
+                const float nf = float(b.x), ns = float(c.x);
+                float c0 = cos_in;
+                if (!s.front) {
+                    const float sin2 = ns * ns * (1 - cos_in * cos_in);
+                    ok = ok && sin2 < 1.0f;
+                    c0 = sqrtf(fmaxf(1 - sin2, 0.0f));
                 }
+                ok = ok && a.x == 1.0 && a.y == 0.0 && b.y == 0.0 && c.y == 0.0 && nf >= fs.nf_lo && nf <= fs.nf_hi &&
+                     ns >= fs.ns_lo && ns <= fs.ns_hi && c0 >= fs.cos_lo && c0 <= fs.cos_hi && lam >= fs.lam_lo &&
+                     lam <= fs.lam_hi;
+                const float v[kIn] = {lam, c0, d, nf, ns};
+                encode(v, fs.rg, e[w]);
             }
-            s4 att;
-            f3 nd;
-            thin_film_scatter(sc, s, R, rng, att, nd);
-            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
+        }
+        s4 R = s4_fill(0.0f);
+#pragma unroll 1
+        for (int w = 0; w < kHero && ok_tc; w++) {
+            float row[kIn];
+#pragma unroll
+            for (int k = 0; k < kIn; k++) row[k] = ok ? e[w][k] : 0.0f;
+            put_row(smem, tid, row);
+            float y[kOut];
+            ok_tc = mlp_tile(smem, t, y);
+            R.v[w] = clampf((y[0] + y[1]) * 0.5f, 0.0f, 1.0f);
+        }
+        bool alive = false, to_exact = false;
+        if (valid && ok_tc) {
+            if (ok) {
+                Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+                s4 att;
+                f3 nd;
+                thin_film_scatter(sc, s, R, rng, att, nd);
+                alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
+            } else {
+                to_exact = true;
+            }
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
+        const int xslot = warp_push(&ps.counts[queue_slot(bounce, kQFilmExact)], to_exact);
+        if (to_exact) q_exact[xslot] = p;
     }
+    if (!ok_tc && tid == 0) atomicOr(ps.error, 2);
+    tile_teardown(t);
 }
 
 // Host: pack FP32 parameters into the bf16 shared-memory image and the bias vector.
@@ -625,11 +657,38 @@ lambda_status install(lambda_ctx *ctx, const float *params_host, const lambda_fi
     return LAMBDA_OK;
 }
 
+// CTAs of 128 threads with kSmemBytes of dynamic shared memory that one SM holds
+// at once, from the kernel's registers and shared memory and the SM's register
+// file, shared memory and thread limits (registers are allocated per thread in
+// multiples of 8; every CTA also holds the SM's per-block reservation).
+int resident_ctas(const void *fn, int device) {
+    cudaFuncAttributes fa{};
+    int smem_sm = 0, regs_sm = 0, threads_sm = 0, reserved = 0;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const int regs = (std::max(fa.numRegs, 1) + 7) / 8 * 8;
+    const int by_regs = regs_sm / (128 * regs);
+    const int by_smem = smem_sm / int(kSmemBytes + fa.sharedSizeBytes + reserved);
+    const int by_threads = threads_sm / 128;
+    return std::max(1, std::min({by_regs, by_smem, by_threads}));
+}
+
+// Resident CTAs per SM of the tensor-core MLP kernels, capped so their TMEM
+// columns fit the SM's 512 and no allocation ever waits. Computed outside stream
+// capture and cached on the context.
 int mlp_grid(lambda_ctx *ctx) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_tc, 128, kSmemBytes);
-    per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
-    return per_sm * ctx->sm_count;
+    if (ctx->mlp_ctas_per_sm <= 0) {
+        const int per_sm = std::min(resident_ctas((const void *)k_mlp_tc, ctx->device),
+                                    resident_ctas((const void *)k_film_fused, ctx->device));
+        ctx->mlp_ctas_per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
+    }
+    return ctx->mlp_ctas_per_sm * ctx->sm_count;
 }
 
 lambda_status run_mlp(lambda_ctx *ctx, const float *rows_dev, int n_rows, float4 *out_dev) {
@@ -655,7 +714,6 @@ lambda_status run_mlp(lambda_ctx *ctx, const float *rows_dev, int n_rows, float4
 
 int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const DeviceScene &sc, const PathState &ps,
                                        int grid, StageProfiler *prof) {
-    const size_t P = size_t(rp.num_pixels);
     FilmSurrogate fs;
     fs.rg = to_range(surrogate_range);
     fs.lam_lo = surrogate_range.lambda_nm[0];
@@ -668,33 +726,24 @@ int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const
     fs.nf_hi = surrogate_range.n_film[1];
     fs.ns_lo = surrogate_range.n_sub[0];
     fs.ns_hi = surrogate_range.n_sub[1];
-    float *rows = rbuf.tf_in.as<float>();
-    float4 *outv = rbuf.tf_out.as<float4>();
-    int *fb = rbuf.tf_queue.as<int>();
-    (void)P;
     const uint8_t *w = static_cast<const uint8_t *>(sbuf.weights_bf16.ptr);
     if (prof) prof->begin(9);
-    k_film_inputs<<<grid, 256, 0, stream>>>(bounce, rp, sc, ps, fs, rows, fb);
+    k_film_fused<<<mlp_grid(this), 128, kSmemBytes, stream>>>(bounce, rp, sc, ps, fs, reinterpret_cast<const uint4 *>(w),
+                                                              reinterpret_cast<const float *>(w + kPackedWeightBytes));
     if (prof) prof->end();
     if (prof) prof->begin(10);
-    k_mlp_tc<<<mlp_grid(this), 128, kSmemBytes, stream>>>(reinterpret_cast<const uint4 *>(w),
-                                                          reinterpret_cast<const float *>(w + kPackedWeightBytes), rows,
-                                                          ps.counts + queue_slot(bounce, kQFilm), kHero, 0, outv,
-                                                          ps.error);
+    k_shade_film_exact<<<grid, 256, 0, stream>>>(bounce, rp, sc, ps, true);
     if (prof) prof->end();
-    if (prof) prof->begin(11);
-    k_film_scatter<<<grid, 256, 0, stream>>>(bounce, rp, sc, ps, outv, fb);
-    if (prof) prof->end();
-    return 3;
+    return 2;
 }
 
 lambda_status lambda_ctx::ensure_surrogate_state(int pixels) {
     lambda_ctx *ctx = this;
     const size_t P = size_t(pixels);
-    CK(rbuf.tf_in.reserve(P * kHero * kRowStride * sizeof(float)), "allocate surrogate batch");
-    CK(rbuf.tf_out.reserve(P * kHero * sizeof(float4)), "allocate surrogate batch");
-    CK(rbuf.tf_queue.reserve(P * sizeof(int)), "allocate surrogate batch");
+    (void)P;
     CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+    CK(cudaFuncSetAttribute(k_film_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+    mlp_grid(this);  // before any stream capture
     return LAMBDA_OK;
 }
 
