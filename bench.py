@@ -5,7 +5,7 @@ grid, seed 3; film n = [1 1.33 1.5], Worley thickness 200-800 nm at frequency 3)
 Lambertian ground (0.5), one quad light (10); 1920x1080, depth 16, 256 spp,
 380-780 nm, render seed 3. 530,841,600 spectral paths per step.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode surrogate|exact]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode exact|surrogate]
   python bench.py --impl reference ...   (the reference's CPU renderer, same workload)
 
 `value` is device time (CUDA events on the library's stream) with the image left
@@ -13,6 +13,12 @@ in HBM; `e2e` goes through the C ABI with host buffers every step (scene upload
 H2D, image D2H). Between timed steps L2 is flushed by writing 256 MB. For N > 1
 each rank renders its own frame (replicas, weak scaling) and the slowest rank's
 time counts.
+
+The headline mode is the exact FP32 transfer matrix (the reference's algorithm,
+and the faster of the two here); the BF16 surrogate is rendered over the same
+steps and reported beside it (`surrogate_vs_exact`: throughput ratio, image
+quality against the exact frames, per-query error against FP64, and a
+query-level comparison of the two film evaluators on device-resident batches).
 """
 
 from __future__ import annotations
@@ -36,6 +42,14 @@ UNIT = "spectral paths/s"
 WORKLOAD = ("thinfilm_spheres 1920x1080 depth16 256spp 380-780nm: 64 spheres r=0.4 jittered 8x8 (seed 3), "
             "thinfilm [1 1.33 1.5] worley 200-800nm freq 3, lambertian ground 0.5, quad light 10, render seed 3")
 W, H, SPP, DEPTH = 1920, 1080, 256, 16
+
+# DRAM bytes per processed item and issue-slot utilisation of a kernel, from the ncu
+# capture summarised in the named profile (one launch of the same kernel on the same
+# scene); the JSON line scales the bytes to the average launch as `traffic`.
+PROFILED = {
+    "intersect": {"dram_bytes_per_item": (96.653824e6 + 49.102080e6) / 2073600, "issue_slot_utilisation": 0.5889,
+                  "profile": "profiles/k_intersect_thinfilm_1080p.md"},
+}
 
 
 def peaks():
@@ -261,16 +275,42 @@ def surrogate_error(ctx) -> dict:
             "R_max_abs": float(e.max()), "outputs_mean_abs": float(eo.mean()), "outputs_max_abs": float(eo.max())}
 
 
+def film_queries(ctx, local: int, n: int = 1 << 24, reps: int = 5) -> dict:
+    """Film evaluations per second of the two evaluators on device-resident batches
+    of n queries (wall time of the blocking C-ABI call, best of reps): the exact
+    FP32 transfer matrix (R_s, R_p, T_s, T_p) and the tensor-core surrogate."""
+    import torch
+
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(7)
+    lo = torch.tensor([380.0, 0.05, 150.0, 1.2, 1.0], device=f"cuda:{local}")
+    hi = torch.tensor([780.0, 1.0, 850.0, 1.8, 2.0], device=f"cuda:{local}")
+    q = lo + (hi - lo) * torch.rand((n, 5), generator=g, device=f"cuda:{local}")
+    out = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
+    res = {}
+    for name, fn in (("exact_tmm", ctx.thinfilm_exact), ("surrogate", ctx.surrogate_eval)):
+        best = float("inf")
+        for _ in range(reps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn(q, out)
+            t1 = time.perf_counter()
+            best = min(best, t1 - t0)
+        res[f"{name}_queries_per_s"] = n / best
+    res["surrogate_over_exact"] = res["surrogate_queries_per_s"] / res["exact_tmm_queries_per_s"]
+    res["batch"] = n
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lambda_b200", choices=["lambda_b200", "reference"])
-    ap.add_argument("--mode", default="auto", choices=["auto", "surrogate", "exact"])
+    ap.add_argument("--mode", default="exact", choices=["exact", "surrogate"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
-    ap.add_argument("--no-compare", action="store_true", help="skip the exact-form comparison")
+    ap.add_argument("--no-compare", action="store_true", help="skip the surrogate/exact comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -290,18 +330,17 @@ def main():
     ctx.upload(scene)
 
     mode = args.mode
-    if mode in ("auto", "surrogate"):
-        try:
-            from lambda_b200 import surrogate as lbs
+    have_surrogate = True
+    try:
+        from lambda_b200 import surrogate as lbs
 
-            lbs.install(ctx)
-            mode = "surrogate"
-        except Exception as e:  # no trained weights: the exact form is what can run
-            if args.mode == "surrogate":
-                raise
-            mode = "exact"
-            if rank == 0:
-                print(f"# surrogate unavailable ({e}); measuring the exact transfer matrix", file=sys.stderr)
+        lbs.install(ctx)
+    except Exception as e:  # no trained weights: only the exact form can run
+        if mode == "surrogate":
+            raise
+        have_surrogate = False
+        if rank == 0:
+            print(f"# surrogate unavailable ({e}); no surrogate comparison", file=sys.stderr)
     flags = lb.RENDER_THINFILM_SURROGATE if mode == "surrogate" else lb.RENDER_THINFILM_EXACT
     dev_out = torch.empty((H, W, 3), dtype=torch.float32, device=f"cuda:{local}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -333,23 +372,32 @@ def main():
     # per-stage kernel times (CUDA events inside the library) for the roofline
     stage = lb.stage_profile(ctx, desc, dev_out)
 
-    # the exact transfer-matrix form over the same steps, and image quality
+    # the other thin-film evaluator over the same steps, and image quality
     comparison = None
-    if mode == "surrogate" and not args.no_compare:
-        exact_desc = scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_EXACT | lb.RENDER_OUTPUT_DEVICE)
-        ctx.render(exact_desc, out=dev_out)
-        ex_ms = 0.0
+    if have_surrogate and not args.no_compare:
+        other = "exact" if mode == "surrogate" else "surrogate"
+        oflags = lb.RENDER_THINFILM_EXACT if other == "exact" else lb.RENDER_THINFILM_SURROGATE
+        other_desc = scene.render_desc(seed=sc.seed, flags=oflags | lb.RENDER_OUTPUT_DEVICE)
+        ctx.render(other_desc, out=dev_out)
+        o_ms = 0.0
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            ctx.render(exact_desc, out=dev_out)
-            ex_ms += ctx.stats().render_ms
-        ex_ms = max_over_ranks(ex_ms, world)
-        ex_value = world * paths_per_step * args.steps / (ex_ms / 1000.0)
-        comparison = {"exact_tmm_value": ex_value, "exact_tmm_ms_per_step": ex_ms / args.steps,
-                      "surrogate_over_exact": value / ex_value}
+            ctx.render(other_desc, out=dev_out)
+            o_ms += ctx.stats().render_ms
+        o_ms = max_over_ranks(o_ms, world)
+        o_value = world * paths_per_step * args.steps / (o_ms / 1000.0)
+        ex_value, su_value = (value, o_value) if mode == "exact" else (o_value, value)
+        comparison = {"exact_tmm_value": ex_value, "surrogate_value": su_value,
+                      "exact_tmm_ms_per_step": (max_ms if mode == "exact" else o_ms) / args.steps,
+                      "surrogate_ms_per_step": (o_ms if mode == "exact" else max_ms) / args.steps,
+                      "surrogate_over_exact": su_value / ex_value,
+                      "surrogate_ctas_per_sm": ctx.stats().surrogate_ctas_per_sm if other == "surrogate"
+                      else stats[-1].surrogate_ctas_per_sm}
         if rank == 0:
             comparison["quality"] = image_quality(ctx, scene, dev_out)
+            comparison["surrogate_error_vs_fp64"] = surrogate_error(ctx)
+            comparison["film_queries"] = film_queries(ctx, local)
 
     # end to end through the C ABI with host buffers
     host_out = torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy()
@@ -368,6 +416,13 @@ def main():
     if rank == 0:
         hbm, tf, tf_sus, peak_kind = peaks()
         roof = lb.roofline(stage, hbm, tf, peak_kind)
+        prof = PROFILED.get(roof.get("kernel"))
+        if prof is not None:
+            launches_k = stage[roof["kernel"]]["launches"]
+            roof["traffic"] = prof["dram_bytes_per_item"] * roof["items"] / max(launches_k, 1)
+            roof["achieved_bytes_per_launch"] = roof["bytes_per_item"] * roof["items"] / max(launches_k, 1)
+            roof["issue_slot_utilisation"] = prof["issue_slot_utilisation"]
+            roof["traffic_source"] = prof["profile"]
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -384,13 +439,10 @@ def main():
             "stages": stage,
             "segments_per_path": stats[-1].segments / stats[-1].paths,
             "thinfilm": {"hits_per_step": stats[-1].thinfilm_hits,
-                         "exact_fallback_per_step": stats[-1].thinfilm_fallback,
-                         "surrogate_ctas_per_sm": stats[-1].surrogate_ctas_per_sm},
+                         "surrogate_exact_fallback_per_step": stats[-1].thinfilm_fallback},
         }
         if comparison is not None:
             out["surrogate_vs_exact"] = comparison
-            if mode == "surrogate":
-                out["surrogate_error_vs_fp64"] = surrogate_error(ctx)
         if not args.no_cpu_baseline:
             cb = cpu_baseline(sc.lrd, sc.seed)
             if cb is not None:

@@ -274,24 +274,34 @@ class Context:
         q = np.ascontiguousarray(q, dtype=np.float32).reshape(-1, 5)
         return q
 
-    def thinfilm_exact(self, q: np.ndarray) -> np.ndarray:
-        """q: [n, 5] = (lambda_nm, cos_theta, thickness_nm, n_film, n_sub) -> [n, 4] (Rs, Rp, Ts, Tp)."""
+    def _film(self, fn, q, out, dtype):
+        """Film queries: q [n, 5] = (lambda_nm, cos_theta, thickness_nm, n_film, n_sub).
+        A numpy q returns a new numpy [n, 4]; a contiguous float32 CUDA tensor q is
+        evaluated in place into `out` (a [n, 4] CUDA tensor), with no host staging."""
+        if not isinstance(q, np.ndarray) and getattr(q, "is_cuda", False):
+            if out is None or not q.is_contiguous() or not out.is_contiguous() or q.shape[-1] != 5:
+                raise ValueError("device queries need a contiguous [n, 5] tensor and a contiguous [n, 4] out")
+            n = q.numel() // 5
+            if out.numel() != 4 * n:
+                raise ValueError("out must hold [n, 4] results")
+            self._check(fn(self._h, _ptr(q), n, _ptr(out)))
+            return out
         q = self._queries(q)
-        out = np.empty((q.shape[0], 4), np.float32)
-        self._check(self._lib.lambda_thinfilm_exact(self._h, q.ctypes.data, q.shape[0], out.ctypes.data))
-        return out
+        res = np.empty((q.shape[0], 4), dtype)
+        self._check(fn(self._h, q.ctypes.data, q.shape[0], res.ctypes.data))
+        return res
 
-    def thinfilm_fp64(self, q: np.ndarray) -> np.ndarray:
-        q = self._queries(q)
-        out = np.empty((q.shape[0], 4), np.float64)
-        self._check(self._lib.lambda_thinfilm_fp64(self._h, q.ctypes.data, q.shape[0], out.ctypes.data))
-        return out
+    def thinfilm_exact(self, q, out=None):
+        """Exact FP32 transfer matrix: (R_s, R_p, T_s, T_p) per query."""
+        return self._film(self._lib.lambda_thinfilm_exact, q, out, np.float32)
 
-    def surrogate_eval(self, q: np.ndarray) -> np.ndarray:
-        q = self._queries(q)
-        out = np.empty((q.shape[0], 4), np.float32)
-        self._check(self._lib.lambda_surrogate_eval(self._h, q.ctypes.data, q.shape[0], out.ctypes.data))
-        return out
+    def thinfilm_fp64(self, q, out=None):
+        """FP64 transfer matrix (the training labeller)."""
+        return self._film(self._lib.lambda_thinfilm_fp64, q, out, np.float64)
+
+    def surrogate_eval(self, q, out=None):
+        """Tensor-core surrogate: (R_s, R_p, T_s, T_p) per query."""
+        return self._film(self._lib.lambda_surrogate_eval, q, out, np.float32)
 
     def surrogate_train(self, samples: int = 1 << 24, epochs: int = 8, batch: int = 8192, lr: float = 2e-3,
                         seed: int = 7, film_range=None) -> N.TrainReport:

@@ -38,7 +38,7 @@ RENDER_OUTPUT_DEVICE = 2
 RENDER_PROFILE_STAGES = 4
 NUM_STAGES = 12
 STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
-               "shadow", "finish", "film_surrogate", "film_fallback", "unused")
+               "shadow", "finish", "film_surrogate", "unused10", "unused11")
 
 
 class LambdaError(RuntimeError):

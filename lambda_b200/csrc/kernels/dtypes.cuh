@@ -67,8 +67,7 @@ struct PathState {
     float4 *sh_a;         // throughput * BSDF * cos
     int2 *sh_light;       // light (instance, object)
     int *queue[2];        // active pixel ids, ping-pong by bounce parity
-    int *mat_queue[4];    // this bounce's Lambertian, mirror/dielectric and thin-film hits, and the
-                          // thin-film hits the surrogate hands to the exact path
+    int *mat_queue[3];    // this bounce's Lambertian, mirror/dielectric and thin-film hits
     int *shadow_queue;    // pixel ids with a pending NEE ray
     int *counts;          // [kQueues * (depth + 2)], see queue_slot()
     int *wave;            // [2]: wave to run next, wave being run
@@ -76,8 +75,9 @@ struct PathState {
     int *error;           // bit 0: traversal stack overflow
 };
 
-// Counters per bounce: paths to trace, then the three material queues, then NEE rays.
-enum : int { kQActive = 0, kQLambert = 1, kQSpecular = 2, kQFilm = 3, kQShadow = 4, kQFilmExact = 5, kQueues = 6 };
+// Counters per bounce: paths to trace, then the three material queues, then NEE rays,
+// then the thin-film hits the surrogate left to the exact transfer matrix (a count).
+enum : int { kQActive = 0, kQLambert = 1, kQSpecular = 2, kQFilm = 3, kQShadow = 4, kQFilmFallback = 5, kQueues = 6 };
 __host__ __device__ inline int queue_slot(int bounce, int q) { return bounce * kQueues + q; }
 
 }  // namespace lambda_dev

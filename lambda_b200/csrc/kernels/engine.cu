@@ -553,7 +553,6 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     CK(r.qm0.reserve(P * 4), "allocate queues");
     CK(r.qm1.reserve(P * 4), "allocate queues");
     CK(r.qm2.reserve(P * 4), "allocate queues");
-    CK(r.qm3.reserve(P * 4), "allocate queues");
     CK(r.counts.reserve(size_t(kQueues * (depth + 2)) * 4), "allocate queues");
     CK(r.wave.reserve(16), "allocate queues");
     CK(r.stats.reserve(8 * 8), "allocate statistics");
@@ -580,7 +579,6 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     ps.mat_queue[0] = r.qm0.as<int>();
     ps.mat_queue[1] = r.qm1.as<int>();
     ps.mat_queue[2] = r.qm2.as<int>();
-    ps.mat_queue[3] = r.qm3.as<int>();
     ps.counts = r.counts.as<int>();
     ps.wave = r.wave.as<int>();
     ps.stats = r.stats.as<unsigned long long>();
@@ -628,7 +626,7 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
     lambda_status s = ctx->ensure_state(rp.num_pixels, rp.depth);
     if (s != LAMBDA_OK) return s;
     if (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) {
-        s = ctx->ensure_surrogate_state(rp.num_pixels);
+        s = ctx->ensure_surrogate_state();
         if (s != LAMBDA_OK) return s;
     }
     cudaStream_t stream = ctx->stream;
@@ -666,8 +664,8 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
             if (sc.families & 1u) timed(4, [&] { k_shade_lambert<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
             if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
             if (sc.families & 4u) {
-                if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, qgrid, pr);
-                else timed(6, [&] { k_shade_film_exact<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps, false); });
+                if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, pr);
+                else timed(6, [&] { k_shade_film_exact<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
             }
             if (sc.families & 1u) timed(7, [&] { k_shadow<<<qgrid, 256, stack_smem, stream>>>(b, rp, sc, ps); });
         }
@@ -748,7 +746,6 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
         ctx->stage_times[7].items = ctx->stats.shadow_rays;
         ctx->stage_times[8].items = P;
         ctx->stage_times[9].items = surrogate ? ctx->stats.thinfilm_hits : 0;
-        ctx->stage_times[10].items = surrogate ? ctx->stats.thinfilm_fallback : 0;
     }
     if (err[0] & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
     if (err[0] & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
@@ -799,45 +796,7 @@ __global__ void k_trace_shadow(DeviceScene sc, const float *rays, const int *li,
 
 }  // namespace
 
-// Stages caller arrays (host or device) in and out of device memory.
-struct Staging {
-    lambda_ctx *ctx;
-    std::vector<void *> owned;
-    ~Staging() {
-        for (void *p : owned) cudaFree(p);
-    }
-    template <typename T>
-    cudaError_t in(const T *src, size_t n, const T **dst) {
-        if (is_device_pointer(src)) {
-            *dst = src;
-            return cudaSuccess;
-        }
-        void *p = nullptr;
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n * sizeof(T), 16));
-        if (e != cudaSuccess) return e;
-        owned.push_back(p);
-        *dst = static_cast<const T *>(p);
-        return cudaMemcpyAsync(p, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
-    }
-    template <typename T>
-    cudaError_t out(T *user, size_t n, T **dst, std::vector<std::pair<void *, std::pair<void *, size_t>>> &back) {
-        if (is_device_pointer(user)) {
-            *dst = user;
-            return cudaSuccess;
-        }
-        void *p = nullptr;
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n * sizeof(T), 16));
-        if (e != cudaSuccess) return e;
-        owned.push_back(p);
-        *dst = static_cast<T *>(p);
-        back.push_back({user, {p, n * sizeof(T)}});
-        return cudaSuccess;
-    }
-};
-
-using CopyBack = std::vector<std::pair<void *, std::pair<void *, size_t>>>;
-
-static lambda_status finish_staging(lambda_ctx *ctx, CopyBack &back) {
+lambda_status finish_staging(lambda_ctx *ctx, CopyBack &back) {
     for (auto &b : back)
         CK(cudaMemcpyAsync(b.first, b.second.first, b.second.second, cudaMemcpyDeviceToHost, ctx->stream), "copy results");
     CK(cudaStreamSynchronize(ctx->stream), "query");

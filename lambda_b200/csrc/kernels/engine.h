@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -44,15 +45,12 @@ struct SceneBuffers {
 
 struct RenderBuffers {
     DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
-        q0, q1, qs, qm0, qm1, qm2, qm3, counts, wave, stats, error, out;
-    // thin-film surrogate batch
-    DeviceBuffer tf_queue, tf_in, tf_out;
+        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out;
 };
 
 struct SurrogateBuffers {
     DeviceBuffer weights_bf16;  // packed tensor-core operand tiles
     DeviceBuffer weights_f32;   // master copy, LAMBDA_MLP_PARAMS floats
-    DeviceBuffer scratch;
 };
 
 struct lambda_ctx {
@@ -85,9 +83,9 @@ struct lambda_ctx {
     lambda_status cuda_fail(cudaError_t e, const char *what);
     lambda_status ensure_state(int pixels, int depth);
     lambda_status surrogate_ready();
-    lambda_status ensure_surrogate_state(int pixels);
+    lambda_status ensure_surrogate_state();
     int launch_shade_surrogate(int bounce, const lambda_dev::RenderParams &rp, const lambda_dev::DeviceScene &sc,
-                               const lambda_dev::PathState &ps, int grid, StageProfiler *prof);
+                               const lambda_dev::PathState &ps, StageProfiler *prof);
 
     std::vector<DeviceBuffer *> all_buffers() {
         SceneBuffers &s = scene;
@@ -96,8 +94,49 @@ struct lambda_ctx {
                 &s.cspectrum_flat, &s.materials, &s.material_props, &s.scalar_tex, &s.spectrum_tex, &s.light_inst,
                 &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
-                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.qm3, &r.counts, &r.wave,
-                &r.stats, &r.error, &r.out, &r.tf_queue, &r.tf_in, &r.tf_out, &sbuf.weights_bf16,
-                &sbuf.weights_f32, &sbuf.scratch};
+                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
+                &r.stats, &r.error, &r.out, &sbuf.weights_bf16, &sbuf.weights_f32};
     }
 };
+
+// Stages caller arrays (host or device) in and out of device memory.
+struct Staging {
+    lambda_ctx *ctx;
+    std::vector<void *> owned;
+    ~Staging() {
+        for (void *p : owned) cudaFree(p);
+    }
+    template <typename T>
+    cudaError_t in(const T *src, size_t n, const T **dst) {
+        if (is_device_pointer(src)) {
+            *dst = src;
+            return cudaSuccess;
+        }
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n * sizeof(T), 16));
+        if (e != cudaSuccess) return e;
+        owned.push_back(p);
+        *dst = static_cast<const T *>(p);
+        return cudaMemcpyAsync(p, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    }
+    template <typename T>
+    cudaError_t out(T *user, size_t n, T **dst, std::vector<std::pair<void *, std::pair<void *, size_t>>> &back) {
+        if (is_device_pointer(user)) {
+            *dst = user;
+            return cudaSuccess;
+        }
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n * sizeof(T), 16));
+        if (e != cudaSuccess) return e;
+        owned.push_back(p);
+        *dst = static_cast<T *>(p);
+        back.push_back({user, {p, n * sizeof(T)}});
+        return cudaSuccess;
+    }
+};
+
+using CopyBack = std::vector<std::pair<void *, std::pair<void *, size_t>>>;
+
+// Copies staged results back to the caller's host arrays and waits for the stream.
+lambda_status finish_staging(lambda_ctx *ctx, CopyBack &back);
+

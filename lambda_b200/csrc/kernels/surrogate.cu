@@ -57,18 +57,25 @@ __host__ __device__ constexpr int core_offset(int r, int k, int K) {
     return ((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2;
 }
 
-// Shared-memory layout of k_mlp_tc (bytes).
-constexpr int sW1 = 0;                         // [64][16]
-constexpr int sW2 = sW1 + kH * kInPad * 2;     // [64][64]
-constexpr int sW3 = sW2 + kH * kH * 2;         // [64][64]
-constexpr int sW4 = sW3 + kH * kH * 2;         // [16][64]
-constexpr int sX = sW4 + kOutPad * kH * 2;     // [128][16]
-constexpr int sHid = sX + kTileM * kInPad * 2;  // [128][64]
-constexpr int sBias = sHid + kTileM * kH * 2;   // f32: b1[64] b2[64] b3[64] b4[16]
-constexpr int sBar = sBias + (3 * kH + kOutPad) * 4;
+// Shared-memory layout of the tensor-core MLP kernels (bytes). The biases ride in
+// the MMAs: every operand row carries two constant-1 columns that meet (b_hi, b_lo),
+// the bias split into two BF16 parts (b_lo = bf16(b - b_hi), so b_hi + b_lo is b to
+// about 2^-17 relative), and the epilogues add nothing. For layers 2-4 that product
+// is one extra K step whose second core matrix (k 8..15) is the zero block.
+constexpr int sW1 = 0;                           // [64][16]: W1 in k 0..4, (b1 hi, b1 lo) in k 5, 6
+constexpr int sW2 = sW1 + kH * kInPad * 2;       // [64][64]
+constexpr int sW3 = sW2 + kH * kH * 2;           // [64][64]
+constexpr int sW4 = sW3 + kH * kH * 2;           // [16][64]
+constexpr int sB2 = sW4 + kOutPad * kH * 2;      // [64][8]: (b2 hi, b2 lo, 0, ...)
+constexpr int sB3 = sB2 + kH * 16;               // [64][8]
+constexpr int sB4 = sB3 + kH * 16;               // [16][8]
+constexpr int kPackedWeightBytes = sB4 + kOutPad * 16;  // the weight image, copied as is
+constexpr int sHid = kPackedWeightBytes;         // [128][64]; the layer-1 operand [128][16] overlays its start
+constexpr int sOnes = sHid + kTileM * kH * 2;    // [128][8]: (1, 1, 0, ...)
+constexpr int sZero = sOnes + kTileM * 16;       // [128][8] zeros
+constexpr int sBar = sZero + kTileM * 16;
 constexpr int sTmem = sBar + 8;
 constexpr int kSmemBytes = sTmem + 8;
-constexpr int kPackedWeightBytes = sX;  // W1..W4 in their shared-memory layout
 constexpr int kTmemCols = 64;
 
 // Input normalisation to [-1, 1] over the trained box.
@@ -152,16 +159,60 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_
     return false;
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float *v) {
-    uint32_t r[16];
+// 32 consecutive FP32 columns of this warp's 32 TMEM lanes (one per thread). The
+// values are valid only after tmem_wait(), which names them as operands so that no
+// use is scheduled before the wait.
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld4(uint32_t addr, uint32_t (&r)[4]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+
+// Waits for this thread's outstanding tcgen05.ld; the registers passed are tied to
+// the wait.
+__device__ __forceinline__ void tmem_wait(uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.wait::ld.sync.aligned;"
+        : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]),
+          "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]),
+          "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]),
+          "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+        :
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait(uint32_t (&r)[4]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]) : : "memory");
+}
+
+// Ties registers loaded before an earlier tmem_wait to that wait (an empty volatile
+// statement after it in program order).
+__device__ __forceinline__ void tmem_after_wait(uint32_t (&r)[32]) {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31]));
+}
+
+// ReLU and round-to-nearest BF16 of two FP32 values in one instruction; lo goes
+// to the low half (the lower address, element k), hi to the high half (k + 1).
+__device__ __forceinline__ uint32_t relu_bf16x2(uint32_t lo, uint32_t hi) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(__uint_as_float(hi)), "f"(__uint_as_float(lo)));
+    return d;
 }
 
 // ---------------------------------------------------------------------------
@@ -176,28 +227,29 @@ __device__ __forceinline__ void put8(uint8_t *smem, int base, int r, int c, int 
     *reinterpret_cast<uint4 *>(smem + base + core_offset(r, c * 8, K)) = *reinterpret_cast<uint4 *>(p);
 }
 
-// Sets up one CTA of a tensor-core MLP kernel: weights and biases into shared
-// memory, the completion mbarrier, and kTmemCols TMEM columns (warp 0 allocates).
+// Sets up one CTA of a tensor-core MLP kernel: the weight image and the constant
+// (1, 1) and zero blocks into shared memory, the completion mbarrier, and
+// kTmemCols TMEM columns (warp 0 allocates).
 struct TileCtx {
     uint32_t base;       // shared-memory address of smem[0]
     uint32_t bar;        // MMA completion mbarrier
     uint32_t tmem;       // TMEM accumulator base (lane 0, column 0)
     uint32_t lane_base;  // this warp's 32 TMEM lanes
     uint32_t phase;
-    const float *bias;   // b1 b2 b3 (64 each) b4 (16) in shared memory
 };
 
-__device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__restrict__ packed,
-                                              const float *__restrict__ bias) {
+__device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__restrict__ packed) {
     const int tid = threadIdx.x, warp = tid >> 5;
     for (int i = tid; i < kPackedWeightBytes / 16; i += blockDim.x) reinterpret_cast<uint4 *>(smem)[i] = packed[i];
-    float *sb = reinterpret_cast<float *>(smem + sBias);
-    for (int i = tid; i < 3 * kH + kOutPad; i += blockDim.x) sb[i] = bias[i];
+    constexpr uint32_t kOneOne = 0x3F803F80u;  // bf16 (1, 1)
+    for (int r = tid; r < kTileM; r += blockDim.x) {
+        *reinterpret_cast<uint4 *>(smem + sOnes + r * 16) = make_uint4(kOneOne, 0, 0, 0);
+        *reinterpret_cast<uint4 *>(smem + sZero + r * 16) = make_uint4(0, 0, 0, 0);
+    }
     TileCtx t;
     t.base = smem_u32(smem);
     t.bar = smem_u32(smem + sBar);
     t.phase = 0;
-    t.bias = sb;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + sTmem);
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(t.bar) : "memory");
@@ -227,13 +279,18 @@ __device__ __forceinline__ void tile_teardown(const TileCtx &t) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem), "r"(kTmemCols) : "memory");
 }
 
-// Four layers over the 128-row operand already stored in sX (row r = thread r).
-// On return y holds this thread's four outputs (bias included). Returns false,
-// uniformly across the CTA, if an MMA completion wait timed out.
+// Four layers over the 128-row operand already stored by put_row (row r = thread r).
+// One CTA barrier per layer: the operand rows are in shared memory, then thread 0
+// issues the layer's MMAs and commits them to the mbarrier every thread waits on.
+// The hidden epilogue is two 32-column TMEM loads, 32 ReLU+BF16 conversions and
+// eight 16-byte stores of the next operand row. On return y holds this thread's four
+// outputs. Returns false, uniformly across the CTA, if an MMA completion wait timed
+// out (the accumulator is then not read as valid).
 __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
     const int tid = threadIdx.x;
     const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
     const uint32_t kPoll = 1u << 22;
+    bool done = true;
 #pragma unroll 1
     for (int layer = 0; layer < 4; layer++) {
         fence_proxy_async();
@@ -242,74 +299,94 @@ __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
         if (tid == 0) {
             fence_after();
             if (layer == 0) {
-                mma_bf16(t.tmem, smem_desc(t.base + sX, 128, 256), smem_desc(t.base + sW1, 128, 256), id64, 0);
+                mma_bf16(t.tmem, smem_desc(t.base + sHid, 128, 256), smem_desc(t.base + sW1, 128, 256), id64, 0);
             } else {
                 const int wofs = layer == 1 ? sW2 : (layer == 2 ? sW3 : sW4);
+                const int bofs = layer == 1 ? sB2 : (layer == 2 ? sB3 : sB4);
                 const uint32_t idesc = layer == 3 ? id16 : id64;
+                // bias: (1, 1, 0 ...) rows against (b_hi, b_lo, 0 ...) rows; second K core from the zero block
+                mma_bf16(t.tmem, smem_desc(t.base + sOnes, sZero - sOnes, 128),
+                         smem_desc(t.base + bofs, sZero - bofs, 128), idesc, 0);
 #pragma unroll
                 for (int kk = 0; kk < kH / 16; kk++)
                     mma_bf16(t.tmem, smem_desc(t.base + sHid + kk * 256, 128, 1024),
-                             smem_desc(t.base + wofs + kk * 256, 128, 1024), idesc, kk > 0);
+                             smem_desc(t.base + wofs + kk * 256, 128, 1024), idesc, 1);
             }
             mma_commit(t.bar);
         }
-        const bool done = mbar_wait(t.bar, t.phase, kPoll);
+        done = mbar_wait(t.bar, t.phase, kPoll) && done;
         t.phase ^= 1u;
         fence_after();
-        if (!__syncthreads_and(done)) return false;
         if (layer < 3) {
-            const float *bl = t.bias + layer * kH;
+            uint32_t a[32], b[32];
+            tmem_ld32(t.lane_base, a);
+            tmem_ld32(t.lane_base + 32, b);
+            tmem_wait(a);
+            tmem_after_wait(b);
 #pragma unroll
-            for (int c = 0; c < kH / 16; c++) {
-                float v[16];
-                tmem_ld16(t.lane_base + c * 16, v);
+            for (int c = 0; c < 4; c++) {
+                const uint4 v = make_uint4(relu_bf16x2(a[8 * c], a[8 * c + 1]), relu_bf16x2(a[8 * c + 2], a[8 * c + 3]),
+                                           relu_bf16x2(a[8 * c + 4], a[8 * c + 5]),
+                                           relu_bf16x2(a[8 * c + 6], a[8 * c + 7]));
+                *reinterpret_cast<uint4 *>(smem + sHid + core_offset(tid, 8 * c, kH)) = v;
+            }
 #pragma unroll
-                for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + bl[c * 16 + i], 0.0f);
-                put8(smem, sHid, tid, 2 * c, kH, v);
-                put8(smem, sHid, tid, 2 * c + 1, kH, v + 8);
+            for (int c = 0; c < 4; c++) {
+                const uint4 v = make_uint4(relu_bf16x2(b[8 * c], b[8 * c + 1]), relu_bf16x2(b[8 * c + 2], b[8 * c + 3]),
+                                           relu_bf16x2(b[8 * c + 4], b[8 * c + 5]),
+                                           relu_bf16x2(b[8 * c + 6], b[8 * c + 7]));
+                *reinterpret_cast<uint4 *>(smem + sHid + core_offset(tid, 32 + 8 * c, kH)) = v;
             }
         } else {
-            float v[16];
-            tmem_ld16(t.lane_base, v);
-            const float *b4 = t.bias + 3 * kH;
-            for (int i = 0; i < kOut; i++) y[i] = v[i] + b4[i];
+            uint32_t o[4];
+            tmem_ld4(t.lane_base, o);
+            tmem_wait(o);
+            for (int i = 0; i < kOut; i++) y[i] = __uint_as_float(o[i]);
         }
     }
-    return true;
+    return __syncthreads_and(done) != 0;
 }
 
-// Stores one encoded row (5 features, zero-padded to K = 16) as row r of sX.
+// Stores one encoded row (5 features, then the two constant-1 bias columns, zero
+// padded to K = 16) as row r of the layer-1 operand.
 __device__ __forceinline__ void put_row(uint8_t *smem, int r, const float *e) {
     float x[16];
 #pragma unroll
-    for (int i = 0; i < 16; i++) x[i] = i < kIn ? e[i] : 0.0f;
-    put8(smem, sX, r, 0, kInPad, x);
-    put8(smem, sX, r, 1, kInPad, x + 8);
+    for (int i = 0; i < 16; i++) x[i] = i < kIn ? e[i] : (i < kIn + 2 ? 1.0f : 0.0f);
+    put8(smem, sHid, r, 0, kInPad, x);
+    put8(smem, sHid, r, 1, kInPad, x + 8);
 }
 
-// in: rows x kRowStride floats (encoded inputs); out: rows x 4 floats.
-// error bit 1 is set if an MMA completion wait timed out.
-__global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed, const float *__restrict__ bias,
-                                                const float *__restrict__ in, const int *__restrict__ row_count,
-                                                int row_multiplier, int rows_fixed, float4 *__restrict__ out,
-                                                int *error) {
+// Inference over `rows` rows: row i's input is kRowStride floats already encoded
+// (kQueries = false) or the i-th lambda_film_query, encoded here (kQueries = true).
+// out: rows x (R_s, R_p, T_s, T_p). Error bit 1 is set if an MMA completion wait
+// timed out.
+template <bool kQueries>
+__global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed, const void *__restrict__ in, int rows,
+                                                Range rg, float4 *__restrict__ out, int *error) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x;
-    const int rows = row_count ? (*row_count) * row_multiplier : rows_fixed;
     const int tiles = (rows + kTileM - 1) / kTileM;
     if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
-    TileCtx t = tile_setup(smem, packed, bias);
+    TileCtx t = tile_setup(smem, packed);
     bool ok = true;
     for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const int row = tile * kTileM + tid;
         float e[kIn] = {0, 0, 0, 0, 0};
         if (row < rows) {
-            const float4 a = *reinterpret_cast<const float4 *>(in + size_t(row) * kRowStride);
-            e[0] = a.x;
-            e[1] = a.y;
-            e[2] = a.z;
-            e[3] = a.w;
-            e[4] = in[size_t(row) * kRowStride + 4];
+            if constexpr (kQueries) {
+                const lambda_film_query q = static_cast<const lambda_film_query *>(in)[row];
+                const float v[kIn] = {q.lambda_nm, q.cos_theta, q.thickness_nm, q.n_film, q.n_sub};
+                encode(v, rg, e);
+            } else {
+                const float *x = static_cast<const float *>(in) + size_t(row) * kRowStride;
+                const float4 a = *reinterpret_cast<const float4 *>(x);
+                e[0] = a.x;
+                e[1] = a.y;
+                e[2] = a.z;
+                e[3] = a.w;
+                e[4] = x[4];
+            }
         }
         put_row(smem, tid, e);
         float y[kOut];
@@ -494,10 +571,11 @@ struct FilmSurrogate {
 // air (index exactly 1) and a substrate inside the trained box. A back-face hit
 // (light inside the substrate) is mapped to the equivalent incidence from air by
 // Snell's law, since a lossless stack reflects the same from both sides. Hits
-// outside the domain or with total internal reflection go to the exact path's queue.
-__global__ void __launch_bounds__(128) k_film_fused(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
-                                                    FilmSurrogate fs, const uint4 *__restrict__ packed,
-                                                    const float *__restrict__ bias) {
+// outside the domain, and back-face hits past the critical angle (where the
+// transfer matrix of material.h:263-309 does not return the physical R = 1), take
+// the exact FP32 transfer matrix in the same thread.
+__global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
+                                                       FilmSurrogate fs, const uint4 *__restrict__ packed) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x;
     const int n = ps.counts[queue_slot(bounce, kQFilm)];
@@ -505,25 +583,20 @@ __global__ void __launch_bounds__(128) k_film_fused(int bounce, RenderParams rp,
     if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
     const int *q = ps.mat_queue[2];
     int *q_next = ps.queue[(bounce + 1) & 1];
-    int *q_exact = ps.mat_queue[3];
-    TileCtx t = tile_setup(smem, packed, bias);
+    TileCtx t = tile_setup(smem, packed);
     bool ok_tc = true;
     for (int tile = blockIdx.x; tile < tiles && ok_tc; tile += gridDim.x) {
         const int idx = tile * kTileM + tid;
         const bool valid = idx < n;
-        int p = 0;
-        ShadeIn s;
+        const int p = valid ? q[idx] : 0;
         bool ok = false;
         float e[kHero][kIn];
         if (valid) {
-            p = q[idx];
-            s = load_shade(ps, sc, p);
+            const ShadeIn s = load_shade(ps, sc, p);
             ok = s.m.y == 1;
-        }
-        if (ok) {
-            const float d = scalar_texture(sc, sc.material_props[s.m.w], s.sp.point);
+            const float d = ok ? scalar_texture(sc, sc.material_props[s.m.w], s.sp.point) : 0.0f;
             const float cos_in = dot(s.nrm, -s.d);
-            ok = d >= fs.d_lo && d <= fs.d_hi;
+            ok = ok && d >= fs.d_lo && d <= fs.d_hi;
 #pragma unroll
             for (int w = 0; w < kHero; w++) {
                 const float lam = s.lam.v[w];
@@ -545,60 +618,69 @@ __global__ void __launch_bounds__(128) k_film_fused(int bounce, RenderParams rp,
             }
         }
         s4 R = s4_fill(0.0f);
-#pragma unroll 1
-        for (int w = 0; w < kHero && ok_tc; w++) {
-            float row[kIn];
 #pragma unroll
-            for (int k = 0; k < kIn; k++) row[k] = ok ? e[w][k] : 0.0f;
-            put_row(smem, tid, row);
-            float y[kOut];
-            ok_tc = mlp_tile(smem, t, y);
-            R.v[w] = clampf((y[0] + y[1]) * 0.5f, 0.0f, 1.0f);
-        }
-        bool alive = false, to_exact = false;
-        if (valid && ok_tc) {
-            if (ok) {
-                Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
-                s4 att;
-                f3 nd;
-                thin_film_scatter(sc, s, R, rng, att, nd);
-                alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
-            } else {
-                to_exact = true;
+        for (int w = 0; w < kHero; w++) {
+            if (ok_tc) {
+                float row[kIn];
+#pragma unroll
+                for (int k = 0; k < kIn; k++) row[k] = ok ? e[w][k] : 0.0f;
+                put_row(smem, tid, row);
+                float y[kOut];
+                ok_tc = mlp_tile(smem, t, y);
+                R.v[w] = clampf((y[0] + y[1]) * 0.5f, 0.0f, 1.0f);
             }
+        }
+        bool alive = false;
+        if (valid && ok_tc) {
+            const ShadeIn s = load_shade(ps, sc, p);
+            if (!ok) {
+                float thick[kMaxFilmLayers];
+                thin_film_thickness(sc, s, thick);
+                R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+            }
+            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            s4 att;
+            f3 nd;
+            thin_film_scatter(sc, s, R, rng, att, nd);
+            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
-        const int xslot = warp_push(&ps.counts[queue_slot(bounce, kQFilmExact)], to_exact);
-        if (to_exact) q_exact[xslot] = p;
+        warp_push(&ps.counts[queue_slot(bounce, kQFilmFallback)], valid && ok_tc && !ok);
     }
     if (!ok_tc && tid == 0) atomicOr(ps.error, 2);
     tile_teardown(t);
 }
 
-// Host: pack FP32 parameters into the bf16 shared-memory image and the bias vector.
-void pack_weights(const float *p, std::vector<uint8_t> &packed, std::vector<float> &bias) {
+// Host: the FP32 parameters as the BF16 shared-memory image of the MLP kernels
+// (weights in their operand layouts, each bias as a (hi, lo) pair of BF16 columns).
+void pack_weights(const float *p, std::vector<uint8_t> &packed) {
     packed.assign(kPackedWeightBytes, 0);
     auto put = [&](int region, int K, int r, int k, float v) {
         const __nv_bfloat16 b = __float2bfloat16_rn(v);
         std::memcpy(&packed[region + core_offset(r, k, K)], &b, 2);
     };
-    for (int o = 0; o < kH; o++)
-        for (int i = 0; i < kInPad; i++) put(sW1, kInPad, o, i, i < kIn ? p[oW1 + o * kIn + i] : 0.0f);
-    for (int o = 0; o < kH; o++)
+    auto put_bias = [&](int region, int K, int r, int k, float v) {
+        const float hi = __bfloat162float(__float2bfloat16_rn(v));
+        put(region, K, r, k, hi);
+        put(region, K, r, k + 1, v - hi);
+    };
+    for (int o = 0; o < kH; o++) {
+        for (int i = 0; i < kIn; i++) put(sW1, kInPad, o, i, p[oW1 + o * kIn + i]);
+        put_bias(sW1, kInPad, o, kIn, p[oB1 + o]);
+    }
+    for (int o = 0; o < kH; o++) {
         for (int i = 0; i < kH; i++) {
             put(sW2, kH, o, i, p[oW2 + o * kH + i]);
             put(sW3, kH, o, i, p[oW3 + o * kH + i]);
         }
-    for (int o = 0; o < kOutPad; o++)
-        for (int i = 0; i < kH; i++) put(sW4, kH, o, i, o < kOut ? p[oW4 + o * kH + i] : 0.0f);
-    bias.assign(3 * kH + kOutPad, 0.0f);
-    for (int o = 0; o < kH; o++) {
-        bias[o] = p[oB1 + o];
-        bias[kH + o] = p[oB2 + o];
-        bias[2 * kH + o] = p[oB3 + o];
+        put_bias(sB2, 8, o, 0, p[oB2 + o]);
+        put_bias(sB3, 8, o, 0, p[oB3 + o]);
     }
-    for (int o = 0; o < kOut; o++) bias[3 * kH + o] = p[oB4 + o];
+    for (int o = 0; o < kOut; o++) {
+        for (int i = 0; i < kH; i++) put(sW4, kH, o, i, p[oW4 + o * kH + i]);
+        put_bias(sB4, 8, o, 0, p[oB4 + o]);
+    }
 }
 
 Range to_range(const lambda_film_range &r) {
@@ -619,6 +701,17 @@ bool range_ok(const lambda_film_range &r) {
            r.thickness_nm[0] >= 0;
 }
 
+// Dynamic shared memory of the MLP kernels (below the 48 KB default today; set so
+// that a larger layout needs no other change).
+cudaError_t configure_mlp_kernels() {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_film_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    return e;
+}
+
 }  // namespace mlp
 
 using namespace mlp;
@@ -633,24 +726,20 @@ lambda_status lambda_ctx::surrogate_ready() {
     if (!has_surrogate)
         return fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed (lambda_surrogate_train or lambda_surrogate_set)");
     lambda_ctx *ctx = this;
-    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+    CK(configure_mlp_kernels(), "configure MLP kernels");
     return LAMBDA_OK;
 }
 
 namespace {
 
-// Installs FP32 parameters: master copy, packed bf16 tiles and biases.
+// Installs FP32 parameters: the master copy and the packed BF16 image.
 lambda_status install(lambda_ctx *ctx, const float *params_host, const lambda_film_range &r) {
     std::vector<uint8_t> packed;
-    std::vector<float> bias;
-    pack_weights(params_host, packed, bias);
+    pack_weights(params_host, packed);
     SurrogateBuffers &b = ctx->sbuf;
     CK(b.weights_f32.upload(params_host, kParams * sizeof(float), ctx->stream), "upload surrogate");
-    CK(b.weights_bf16.reserve(packed.size() + bias.size() * 4), "upload surrogate");
+    CK(b.weights_bf16.reserve(packed.size()), "upload surrogate");
     CK(cudaMemcpyAsync(b.weights_bf16.ptr, packed.data(), packed.size(), cudaMemcpyHostToDevice, ctx->stream), "upload surrogate");
-    CK(cudaMemcpyAsync(static_cast<uint8_t *>(b.weights_bf16.ptr) + packed.size(), bias.data(), bias.size() * 4,
-                       cudaMemcpyHostToDevice, ctx->stream),
-       "upload surrogate");
     CK(cudaStreamSynchronize(ctx->stream), "upload surrogate");
     ctx->surrogate_range = r;
     ctx->has_surrogate = true;
@@ -684,24 +773,27 @@ int resident_ctas(const void *fn, int device) {
 // capture and cached on the context.
 int mlp_grid(lambda_ctx *ctx) {
     if (ctx->mlp_ctas_per_sm <= 0) {
-        const int per_sm = std::min(resident_ctas((const void *)k_mlp_tc, ctx->device),
-                                    resident_ctas((const void *)k_film_fused, ctx->device));
+        const int per_sm = std::min({resident_ctas((const void *)k_mlp_tc<false>, ctx->device),
+                                     resident_ctas((const void *)k_mlp_tc<true>, ctx->device),
+                                     resident_ctas((const void *)k_film_fused, ctx->device)});
         ctx->mlp_ctas_per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
     }
     return ctx->mlp_ctas_per_sm * ctx->sm_count;
 }
 
-lambda_status run_mlp(lambda_ctx *ctx, const float *rows_dev, int n_rows, float4 *out_dev) {
-    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+// Runs the MLP over n_rows encoded rows (kQueries = false) or film queries
+// (kQueries = true) on the context's stream and waits for it.
+template <bool kQueries>
+lambda_status run_mlp(lambda_ctx *ctx, const void *in, int n_rows, float4 *out_dev) {
+    CK(configure_mlp_kernels(), "configure MLP kernels");
     CK(ctx->rbuf.error.reserve(16), "allocate flags");
     int *err = ctx->rbuf.error.as<int>();
     CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
     const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
     const int tiles = (n_rows + kTileM - 1) / kTileM;
     const int grid = std::max(1, std::min(tiles, mlp_grid(ctx)));
-    k_mlp_tc<<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w),
-                                                     reinterpret_cast<const float *>(w + kPackedWeightBytes), rows_dev,
-                                                     nullptr, 0, n_rows, out_dev, err);
+    k_mlp_tc<kQueries><<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w), in, n_rows,
+                                                               to_range(ctx->surrogate_range), out_dev, err);
     CK(cudaGetLastError(), "launch MLP kernel");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");
@@ -713,7 +805,7 @@ lambda_status run_mlp(lambda_ctx *ctx, const float *rows_dev, int n_rows, float4
 }  // namespace
 
 int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const DeviceScene &sc, const PathState &ps,
-                                       int grid, StageProfiler *prof) {
+                                       StageProfiler *prof) {
     FilmSurrogate fs;
     fs.rg = to_range(surrogate_range);
     fs.lam_lo = surrogate_range.lambda_nm[0];
@@ -728,22 +820,16 @@ int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const
     fs.ns_hi = surrogate_range.n_sub[1];
     const uint8_t *w = static_cast<const uint8_t *>(sbuf.weights_bf16.ptr);
     if (prof) prof->begin(9);
-    k_film_fused<<<mlp_grid(this), 128, kSmemBytes, stream>>>(bounce, rp, sc, ps, fs, reinterpret_cast<const uint4 *>(w),
-                                                              reinterpret_cast<const float *>(w + kPackedWeightBytes));
+    k_film_fused<<<mlp_grid(this), 128, kSmemBytes, stream>>>(bounce, rp, sc, ps, fs, reinterpret_cast<const uint4 *>(w));
     if (prof) prof->end();
-    if (prof) prof->begin(10);
-    k_shade_film_exact<<<grid, 256, 0, stream>>>(bounce, rp, sc, ps, true);
-    if (prof) prof->end();
-    return 2;
+    return 1;
 }
 
-lambda_status lambda_ctx::ensure_surrogate_state(int pixels) {
+// Kernel attributes and the MLP grid, set up before any stream capture.
+lambda_status lambda_ctx::ensure_surrogate_state() {
     lambda_ctx *ctx = this;
-    const size_t P = size_t(pixels);
-    (void)P;
-    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
-    CK(cudaFuncSetAttribute(k_film_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
-    mlp_grid(this);  // before any stream capture
+    CK(configure_mlp_kernels(), "configure MLP kernels");
+    mlp_grid(this);
     return LAMBDA_OK;
 }
 
@@ -778,26 +864,15 @@ extern "C" lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_fil
     if (!ctx->has_surrogate) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed");
     if (n == 0) return LAMBDA_OK;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-    std::vector<lambda_film_query> hq(n);
-    if (is_device_pointer(q)) CK(cudaMemcpy(hq.data(), q, sizeof(lambda_film_query) * n, cudaMemcpyDeviceToHost), "read queries");
-    else std::memcpy(hq.data(), q, sizeof(lambda_film_query) * n);
-    const Range rg = to_range(ctx->surrogate_range);
-    std::vector<float> rows(size_t(n) * kRowStride, 0.0f);
-    for (int i = 0; i < n; i++) {
-        const float v[kIn] = {hq[i].lambda_nm, hq[i].cos_theta, hq[i].thickness_nm, hq[i].n_film, hq[i].n_sub};
-        encode(v, rg, &rows[size_t(i) * kRowStride]);
-    }
-    DeviceBuffer din, dout;
-    CK(din.upload(rows.data(), rows.size() * 4, ctx->stream), "stage queries");
-    CK(dout.reserve(size_t(n) * 16), "stage results");
-    lambda_status st = run_mlp(ctx, din.as<float>(), n, dout.as<float4>());
-    if (st == LAMBDA_OK) {
-        if (is_device_pointer(out)) CK(cudaMemcpy(out, dout.ptr, size_t(n) * 16, cudaMemcpyDeviceToDevice), "copy results");
-        else CK(cudaMemcpy(out, dout.ptr, size_t(n) * 16, cudaMemcpyDeviceToHost), "copy results");
-    }
-    din.release();
-    dout.release();
-    return st;
+    Staging sg{ctx, {}};
+    CopyBack back;
+    const lambda_film_query *dq;
+    float *dout;
+    CK(sg.in(q, size_t(n), &dq), "stage queries");
+    CK(sg.out(out, size_t(n) * 4, &dout, back), "stage results");
+    lambda_status st = run_mlp<true>(ctx, dq, n, reinterpret_cast<float4 *>(dout));
+    if (st != LAMBDA_OK) return st;
+    return finish_staging(ctx, back);
 }
 
 namespace {
@@ -898,7 +973,7 @@ extern "C" lambda_status lambda_surrogate_train(lambda_ctx *ctx, const lambda_tr
     lambda_status s = install(ctx, p.data(), d.range);
     if (s != LAMBDA_OK) return s;
     // audit: tensor-core inference against the FP64 labels
-    s = run_mlp(ctx, ax.as<float>(), audit_n, aout.as<float4>());
+    s = run_mlp<false>(ctx, ax.as<float>(), audit_n, aout.as<float4>());
     if (s != LAMBDA_OK) return s;
     std::vector<float> got(size_t(audit_n) * 4), want(size_t(audit_n) * 4);
     CK(cudaMemcpy(got.data(), aout.ptr, got.size() * 4, cudaMemcpyDeviceToHost), "read audit");
@@ -1040,15 +1115,14 @@ extern "C" lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lam
     lambda_status st = static_scratch(ctx, sc);
     if (st != LAMBDA_OK) return st;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-    CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes), "configure MLP kernel");
+    CK(configure_mlp_kernels(), "configure MLP kernels");
     CK(cudaMemsetAsync(sc.error, 0, sizeof(int) * 4, ctx->stream), "clear the static error word");
     k_encode_queries<<<(n + 255) / 256, 256, 0, ctx->stream>>>(queries, n, to_range(ctx->surrogate_range), sc.rows);
     const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
     const int tiles = (n + kTileM - 1) / kTileM;
     const int grid = std::max(1, std::min(tiles, mlp_grid(ctx)));
-    k_mlp_tc<<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w),
-                                                     reinterpret_cast<const float *>(w + kPackedWeightBytes), sc.rows,
-                                                     nullptr, 0, n, reinterpret_cast<float4 *>(out), sc.error);
+    k_mlp_tc<false><<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w), sc.rows, n, Range{},
+                                                            reinterpret_cast<float4 *>(out), sc.error);
     CK(cudaGetLastError(), "launch MLP kernel");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, sc.error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "read the static error word");

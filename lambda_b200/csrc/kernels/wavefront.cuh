@@ -79,7 +79,7 @@ LAMBDA_KERNEL void k_wave_prologue(int depth, PathState ps) {
         ps.stats[0] += tot[kQActive];
         ps.stats[1] += tot[kQShadow];
         ps.stats[2] += tot[kQFilm];
-        ps.stats[3] += tot[kQFilmExact];
+        ps.stats[3] += tot[kQFilmFallback];
         ps.stats[4] += tot[kQLambert];
         ps.stats[5] += tot[kQSpecular];
         ps.wave[1] = ps.wave[0];
@@ -441,13 +441,10 @@ __device__ __forceinline__ void thin_film_thickness(const DeviceScene &sc, const
     for (int k = 0; k < L; k++) thick[k] = scalar_texture(sc, sc.material_props[s.m.w + k], s.sp.point);
 }
 
-// Thin film with the exact FP32 transfer matrix.
-// Thin film with the exact FP32 transfer matrix, over the bounce's thin-film queue
-// (fallback = false) or over the hits the surrogate handed over (fallback = true).
-LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
-                                                                bool fallback) {
-    const int n = ps.counts[queue_slot(bounce, fallback ? kQFilmExact : kQFilm)];
-    const int *q = ps.mat_queue[fallback ? 3 : 2];
+// Thin film with the exact FP32 transfer matrix over the bounce's thin-film queue.
+LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    const int n = ps.counts[queue_slot(bounce, kQFilm)];
+    const int *q = ps.mat_queue[2];
     int *q_next = ps.queue[(bounce + 1) & 1];
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
