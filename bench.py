@@ -301,6 +301,73 @@ def film_queries(ctx, local: int, n: int = 1 << 24, reps: int = 5) -> dict:
     return res
 
 
+BATCH_WORKLOAD = ("batch32: 32 views of the thin-film sphere scene, random camera poses (seed 4), resolutions "
+                  "uniform in {128^2, 256^2, 512^2, 1024^2}, spp in {1, 4, 16, 64, 256}, depth uniform 4-24, "
+                  "380-780 nm, surrogate thin film, launch shapes from the autotuner")
+
+
+def run_batch(args, ctx, scene, lb, torch, rank, world, local):
+    """Config-3 workload: one lambda_render_batch of 32 jobs (device outputs), timed
+    on the device, against the same 32 jobs rendered one lambda_render at a time."""
+    from lambda_b200 import scenes
+
+    flags = lb.RENDER_THINFILM_SURROGATE | lb.RENDER_OUTPUT_DEVICE
+    descs = scenes.random_pose_jobs(scene, 32, seed=4, flags=flags)
+    outs = [torch.empty((d.settings.height, d.settings.width, 3), dtype=torch.float32, device=f"cuda:{local}")
+            for d in descs]
+    paths = sum(d.settings.width * d.settings.height * d.settings.samples for d in descs)
+    tuning = ctx.autotune(scene.render_desc(seed=3, flags=lb.RENDER_THINFILM_SURROGATE, samples=1))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        ctx.render_batch(descs, outs)
+    torch.cuda.synchronize()
+    barrier(world)
+    total_ms, launches = 0.0, 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ctx.render_batch(descs, outs)
+            st = ctx.stats()
+            total_ms += st.render_ms
+            launches += st.kernel_launches
+    max_ms = max_over_ranks(total_ms, world)
+    value = world * paths * args.steps / (max_ms / 1000.0)
+    # the same jobs one render call at a time
+    seq_ms = 0.0
+    for d, o in zip(descs, outs):
+        ctx.render(d, out=o)
+        seq_ms += ctx.stats().render_ms
+    # end to end: host images, through the C ABI
+    host = [np.empty((d.settings.height, d.settings.width, 3), np.float32) for d in descs]
+    hdescs = scenes.random_pose_jobs(scene, 32, seed=4, flags=lb.RENDER_THINFILM_SURROGATE)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.upload(scene)
+        ctx.render_batch(hdescs, host)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "spectral paths/sec, 32-view batched render of the thin-film scene", "value": value,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+bf16", "data": "synthetic",
+            "config": {"workload": BATCH_WORKLOAD, "paths_per_step": paths, "jobs": len(descs),
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
+                                  "grid_scale": tuning.grid_scale, "max_pixels": tuning.max_pixels}},
+            "e2e": {"value": world * paths * args.steps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": lb.scene_bytes(scene),
+                    "d2h_bytes_per_step": sum(d.settings.width * d.settings.height * 12 for d in descs)},
+            "gpu_launches": launches, "clocks": clocks.summary(),
+            "one_job_at_a_time": {"value": paths / (seq_ms / 1000.0), "ms": seq_ms,
+                                  "batch_speedup": seq_ms / (max_ms / args.steps)},
+        }))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -311,6 +378,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
     ap.add_argument("--no-compare", action="store_true", help="skip the surrogate/exact comparison")
+    ap.add_argument("--workload", default="thinfilm1080p", choices=["thinfilm1080p", "batch32"],
+                    help="batch32: 32 random-pose views of the thin-film scene in one batched render")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -346,6 +415,11 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     desc = scene.render_desc(seed=sc.seed, flags=flags | lb.RENDER_OUTPUT_DEVICE)
     paths_per_step = W * H * args.spp
+    if args.workload == "batch32":
+        return run_batch(args, ctx, scene, lb, torch, rank, world, local)
+
+    # launch shapes from the autotuner, timed on a 1-spp frame of the same scene
+    tuning = ctx.autotune(scene.render_desc(seed=sc.seed, flags=flags, samples=1))
 
     for _ in range(args.warmup):
         ctx.render(desc, out=dev_out)
@@ -430,7 +504,9 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "spp": args.spp, "thinfilm": mode,
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
-                       "paths_per_step": paths_per_step},
+                       "paths_per_step": paths_per_step,
+                       "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
+                                  "grid_scale": tuning.grid_scale, "source": "lambda_autotune, 1-spp probe"}},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 12},
             "gpu_launches": launches,

@@ -256,10 +256,41 @@ typedef struct lambda_render_desc {
 lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc *desc, float *out_rgb,
                             volatile int32_t *completed);
 
-/* Per-render statistics of the last lambda_render on this context. */
+/* One image of a batch. */
+typedef struct lambda_job {
+    lambda_render_desc desc;  /* size, depth, samples, wavelength range, camera, seed, flags */
+    float *out_rgb;           /* [height][width][3]; device memory if desc.flags has LAMBDA_RENDER_OUTPUT_DEVICE */
+} lambda_job;
+
+/* Renders n images of the uploaded scene (their own cameras, sizes, sample counts,
+ * depths, wavelength ranges and seeds) as one wavefront: every job's pixels share
+ * one path state, sample waves run until the job with the most samples is done
+ * (jobs with fewer samples drop out of later waves), and the bounces of a wave run
+ * to the deepest job. Each image is, bit for bit, what lambda_render gives for that
+ * job alone. All jobs must use the same thin-film mode and profiling flag; the
+ * output flag is per job. completed (may be NULL) rises towards the jobs' total
+ * pixels. Statistics cover the whole batch. No counterpart in the reference, whose
+ * renderKernel (renderer.h:200-213) renders one image per launch. */
+lambda_status lambda_render_batch(lambda_ctx *ctx, const lambda_job *jobs, int32_t n, volatile int32_t *completed);
+
+/* Launch shapes of the wavefront kernels. lambda_autotune times a probe render
+ * under every candidate and keeps the fastest on the context; lambda_set_tuning
+ * installs given values. No counterpart in the reference. */
+typedef struct lambda_tuning {
+    int32_t trace_block; /* threads per CTA of the traversal kernels (intersect, shadow): 64, 128 or 256 */
+    int32_t shade_block; /* threads per CTA of the shading kernels: 64, 128 or 256 */
+    int32_t grid_scale;  /* persistent grids hold grid_scale x the CTAs that fit on all SMs at once: 1 or 2 */
+    int32_t max_pixels;  /* path-state capacity: a batch above it runs as several passes of whole jobs */
+} lambda_tuning;
+
+lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out);
+lambda_status lambda_set_tuning(lambda_ctx *ctx, const lambda_tuning *tuning);
+lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning *tuning);
+
+/* Statistics of the last lambda_render or lambda_render_batch on this context. */
 typedef struct lambda_render_stats {
     double render_ms;          /* device time from first raygen to film write */
-    int64_t paths;             /* width*height*samples */
+    int64_t paths;             /* width*height*samples, summed over a batch's jobs */
     int64_t segments;          /* ray segments traced (closest-hit queries) */
     int64_t shadow_rays;       /* NEE occlusion queries */
     int64_t thinfilm_hits;     /* thin-film scatter events */

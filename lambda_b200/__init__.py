@@ -237,6 +237,37 @@ class Context:
         self._check(self._lib.lambda_render(self._h, C.byref(desc), C.c_void_p(_ptr(out)), cptr))
         return out
 
+    def render_batch(self, descs, outs=None, completed=None) -> list:
+        """Renders several images of the uploaded scene in one batch
+        (lambda_render_batch). `outs[i]` is a host numpy array, or a device tensor
+        when descs[i] has RENDER_OUTPUT_DEVICE; host arrays are made for a None."""
+        n = len(descs)
+        outs = list(outs) if outs is not None else [None] * n
+        jobs = (N.Job * n)()
+        for i, d in enumerate(descs):
+            if outs[i] is None:
+                outs[i] = np.empty((d.settings.height, d.settings.width, 3), dtype=np.float32)
+            C.memmove(C.byref(jobs[i].desc), C.byref(d), C.sizeof(N.RenderDesc))
+            jobs[i].out_rgb = _ptr(outs[i])
+        cptr = C.cast(completed, C.c_void_p) if completed is not None else None
+        self._check(self._lib.lambda_render_batch(self._h, jobs, n, cptr))
+        return outs
+
+    def autotune(self, probe: N.RenderDesc) -> N.Tuning:
+        """Picks the wavefront launch shapes by timing `probe` (lambda_autotune)."""
+        t = N.Tuning()
+        self._check(self._lib.lambda_autotune(self._h, C.byref(probe), C.byref(t)))
+        return t
+
+    def set_tuning(self, trace_block: int, shade_block: int, grid_scale: int = 1, max_pixels: int = 0) -> None:
+        t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels)
+        self._check(self._lib.lambda_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self) -> N.Tuning:
+        t = N.Tuning()
+        self._check(self._lib.lambda_get_tuning(self._h, C.byref(t)))
+        return t
+
     def stats(self) -> RenderStats:
         st = N.RenderStats()
         self._check(self._lib.lambda_get_render_stats(self._h, C.byref(st)))

@@ -105,6 +105,15 @@ class RenderDesc(C.Structure):
     _fields_ = [("settings", RenderSettings), ("seed", C.c_uint64), ("flags", C.c_uint32), ("reserved", C.c_int32)]
 
 
+class Job(C.Structure):
+    _fields_ = [("desc", RenderDesc), ("out_rgb", C.c_void_p)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("trace_block", C.c_int32), ("shade_block", C.c_int32), ("grid_scale", C.c_int32),
+                ("max_pixels", C.c_int32)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("render_ms", C.c_double), ("paths", C.c_int64), ("segments", C.c_int64),
                 ("shadow_rays", C.c_int64), ("thinfilm_hits", C.c_int64), ("thinfilm_fallback", C.c_int64),
@@ -148,6 +157,10 @@ _SIGNATURES = {
     "lambda_last_error": (C.c_char_p, [_P]),
     "lambda_scene_upload": (C.c_int, [_P, C.POINTER(SceneDesc)]),
     "lambda_render": (C.c_int, [_P, C.POINTER(RenderDesc), _P, _P]),
+    "lambda_render_batch": (C.c_int, [_P, C.POINTER(Job), C.c_int32, _P]),
+    "lambda_autotune": (C.c_int, [_P, C.POINTER(RenderDesc), C.POINTER(Tuning)]),
+    "lambda_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "lambda_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "lambda_get_render_stats": (C.c_int, [_P, C.POINTER(RenderStats)]),
     "lambda_get_stage_times": (C.c_int, [_P, C.POINTER(StageTime)]),
     "lambda_trace_closest": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P]),

@@ -100,11 +100,17 @@ __device__ __forceinline__ f3 xform_t(const float *m, f3 v, float w) {
 }
 
 // Per-pixel PCG32 (random.h): the stream of pixel p has increment 2p+1.
+// PCG32 of one pixel. Streams are pixel indices below 2^30, so the increment
+// 2 * stream + 1 fits 32 bits and is widened only in the state update.
 struct Rng {
     uint64_t state;
-    uint64_t inc;
-    __device__ __forceinline__ float next() { return lambda_rng::pcg_next_float(state, inc); }
+    uint32_t inc;
+    __device__ __forceinline__ float next() { return lambda_rng::pcg_next_float(state, uint64_t(inc)); }
 };
+
+__device__ __forceinline__ Rng pixel_rng(uint64_t state, int stream) {
+    return Rng{state, uint32_t(lambda_rng::pcg_increment(uint64_t(stream)))};
+}
 
 // randomUnitVector (utils.h:20-24). The reference's three draws are constructor
 // arguments, which its compiler (GCC, x86-64) evaluates right to left: the first

@@ -43,12 +43,25 @@ struct DeviceScene {
     uint32_t families;           // bit f set when some material of family f exists (0 Lambertian, 1 specular, 2 thin film)
 };
 
-struct RenderParams {
+// One image of a render: a single render is one job, a batch is many. The jobs'
+// pixels are laid end to end in one virtual pixel range (job j owns
+// [base, base + width * height)), ordered by decreasing sample count, so the pixels
+// that still take a sample in wave s are a prefix of that range.
+struct Job {
     int width, height, depth, samples, sqrt_samples;
     float lambda_min, lambda_max, lambda_range;
     f3 cam_pos, cam_corner, cam_h, cam_v;
     uint64_t seed;
-    int num_pixels;
+    int base;    // first virtual pixel
+    float *out;  // width * height * 3 floats of linear sRGB (device)
+};
+
+struct RenderParams {
+    const Job *jobs;    // [num_jobs]
+    int num_jobs;
+    int num_pixels;     // all jobs' pixels
+    int depth_max;      // deepest job: bounces per wave are 0..depth_max
+    const int *active;  // [samples_max + 1]: pixels with a sample in wave s (a prefix)
 };
 
 struct PathState {
@@ -73,6 +86,7 @@ struct PathState {
     int *wave;            // [2]: wave to run next, wave being run
     unsigned long long *stats;  // segments, shadow rays, thin-film hits
     int *error;           // bit 0: traversal stack overflow
+    int2 *path_info;      // job-local pixel index (the PCG stream), depth limit of the job
 };
 
 // Counters per bounce: paths to trace, then the three material queues, then NEE rays,

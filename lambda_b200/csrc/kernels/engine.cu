@@ -9,11 +9,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "lambda_gpu.h"
@@ -127,6 +129,7 @@ lambda_ctx::~lambda_ctx() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (progress_host) cudaFreeHost(progress_host);
     for (DeviceBuffer *b : all_buffers()) b->release();
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
@@ -472,12 +475,6 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
 
 namespace {
 
-int grid_for(int sm_count, const void *kernel, int block) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
-    return std::max(1, per_sm) * sm_count;
-}
-
 struct Progress {
     volatile int32_t *completed;
     int32_t value;
@@ -547,6 +544,7 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     CK(r.sh_d.reserve(P * 16), "allocate path state");
     CK(r.sh_a.reserve(P * 16), "allocate path state");
     CK(r.sh_light.reserve(P * 8), "allocate path state");
+    CK(r.path_info.reserve(P * 8), "allocate path state");
     CK(r.q0.reserve(P * 4), "allocate queues");
     CK(r.q1.reserve(P * 4), "allocate queues");
     CK(r.qs.reserve(P * 4), "allocate queues");
@@ -557,7 +555,6 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     CK(r.wave.reserve(16), "allocate queues");
     CK(r.stats.reserve(8 * 8), "allocate statistics");
     CK(r.error.reserve(16), "allocate flags");
-    CK(r.out.reserve(P * 12), "allocate output");
     PathState &ps = pstate;
     ps.rng = r.rng.as<uint64_t>();
     ps.film = r.film.as<float4>();
@@ -573,6 +570,7 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     ps.sh_d = r.sh_d.as<float4>();
     ps.sh_a = r.sh_a.as<float4>();
     ps.sh_light = r.sh_light.as<int2>();
+    ps.path_info = r.path_info.as<int2>();
     ps.queue[0] = r.q0.as<int>();
     ps.queue[1] = r.q1.as<int>();
     ps.shadow_queue = r.qs.as<int>();
@@ -586,69 +584,138 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     return LAMBDA_OK;
 }
 
-extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc *desc, float *out_rgb,
-                                       volatile int32_t *completed) {
-    if (!ctx || !desc || !out_rgb) return LAMBDA_ERR_INVALID_ARGUMENT;
-    if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
-    const lambda_render_settings &st = desc->settings;
+int resident_ctas(const void *fn, int device, int block, size_t dyn_smem) {
+    cudaFuncAttributes fa{};
+    int smem_sm = 0, regs_sm = 0, threads_sm = 0, reserved = 0, blocks_sm = 0;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const int regs = (std::max(fa.numRegs, 1) + 7) / 8 * 8;
+    const int by_regs = regs_sm / (block * regs);
+    const int by_smem = smem_sm / int(dyn_smem + fa.sharedSizeBytes + reserved);
+    const int by_threads = threads_sm / block;
+    return std::max(1, std::min({by_regs, by_smem, by_threads, blocks_sm}));
+}
+
+namespace {
+
+lambda_status check_settings(lambda_ctx *ctx, const lambda_render_settings &st) {
     if (st.width <= 0 || st.height <= 0 || st.depth < 0 || st.samples < 1 || st.sqrt_samples * st.sqrt_samples != st.samples)
         return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "invalid render settings");
     if (!(st.lambda_min >= LAMBDA_CIE_LAMBDA_MIN && st.lambda_max <= LAMBDA_CIE_LAMBDA_MAX && st.lambda_min < st.lambda_max))
         return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "wavelength range outside [360, 830] nm");
     if (int64_t(st.width) * st.height > (int64_t(1) << 30)) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "image too large");
     if (st.depth > 1024) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "depth above 1024");
-    if (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) {
-        lambda_status s = ctx->surrogate_ready();
-        if (s != LAMBDA_OK) return s;
+    return LAMBDA_OK;
+}
+
+Job device_job(const lambda_job &j) {
+    const lambda_render_settings &st = j.desc.settings;
+    Job d{};
+    d.width = st.width;
+    d.height = st.height;
+    d.depth = st.depth;
+    d.samples = st.samples;
+    d.sqrt_samples = st.sqrt_samples;
+    d.lambda_min = st.lambda_min;
+    d.lambda_max = st.lambda_max;
+    d.lambda_range = st.lambda_max - st.lambda_min;
+    const lambda_camera &c = st.camera;
+    d.cam_pos = mk(c.position[0], c.position[1], c.position[2]);
+    d.cam_corner = mk(c.corner[0], c.corner[1], c.corner[2]);
+    d.cam_h = mk(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
+    d.cam_v = mk(c.vertical[0], c.vertical[1], c.vertical[2]);
+    d.seed = j.desc.seed;
+    return d;
+}
+
+// Totals over the passes of one render call.
+struct RenderTotals {
+    double ms = 0;
+    int64_t paths = 0, pixels = 0;
+    unsigned long long stats[8] = {0};
+    int launches = 0, waves = 0;
+    int err = 0;
+};
+
+// Renders jobs[order[first..last)] as one wavefront pass (see lambda_render_batch).
+lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::vector<int> &order, size_t first,
+                          size_t last, bool surrogate, StageProfiler *prof, volatile int32_t *completed,
+                          int32_t completed_base, int32_t completed_total, RenderTotals &tot) {
+    const size_t nj = last - first;
+    std::vector<Job> dj(nj);
+    int64_t P64 = 0, host_pixels = 0;
+    int s_max = 0, d_max = 0;
+    for (size_t k = 0; k < nj; k++) {
+        const lambda_job &j = jobs[order[first + k]];
+        dj[k] = device_job(j);
+        dj[k].base = int(P64);
+        P64 += int64_t(dj[k].width) * dj[k].height;
+        if (!(j.desc.flags & LAMBDA_RENDER_OUTPUT_DEVICE)) host_pixels += int64_t(dj[k].width) * dj[k].height;
+        s_max = std::max(s_max, dj[k].samples);
+        d_max = std::max(d_max, dj[k].depth);
     }
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-    const bool out_device = (desc->flags & LAMBDA_RENDER_OUTPUT_DEVICE) != 0;
-    if (out_device && !is_device_pointer(out_rgb))
-        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "LAMBDA_RENDER_OUTPUT_DEVICE given a host pointer");
+    if (P64 > (int64_t(1) << 30)) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "more than 2^30 pixels in one pass");
+    const int P = int(P64);
+    // pixels with a sample in wave s: jobs are ordered by decreasing samples
+    std::vector<int> active(size_t(s_max) + 1, 0);
+    for (int s = 0; s <= s_max; s++)
+        for (size_t k = 0; k < nj; k++)
+            if (dj[k].samples > s) active[s] += dj[k].width * dj[k].height;
+
+    lambda_status st = ctx->ensure_state(P, d_max);
+    if (st != LAMBDA_OK) return st;
+    RenderBuffers &r = ctx->rbuf;
+    CK(r.out.reserve(size_t(std::max<int64_t>(host_pixels, 1)) * 12), "allocate output");
+    int64_t host_off = 0;
+    for (size_t k = 0; k < nj; k++) {
+        const lambda_job &j = jobs[order[first + k]];
+        if (j.desc.flags & LAMBDA_RENDER_OUTPUT_DEVICE) {
+            dj[k].out = j.out_rgb;
+        } else {
+            dj[k].out = r.out.as<float>() + host_off * 3;
+            host_off += int64_t(dj[k].width) * dj[k].height;
+        }
+    }
+    CK(r.jobs.reserve(nj * sizeof(Job)), "allocate job table");
+    CK(r.active.reserve(active.size() * 4), "allocate job table");
+    cudaStream_t stream = ctx->stream;
+    CK(cudaMemcpyAsync(r.jobs.ptr, dj.data(), nj * sizeof(Job), cudaMemcpyHostToDevice, stream), "upload job table");
+    CK(cudaMemcpyAsync(r.active.ptr, active.data(), active.size() * 4, cudaMemcpyHostToDevice, stream),
+       "upload job table");
 
     RenderParams rp{};
-    rp.width = st.width;
-    rp.height = st.height;
-    rp.depth = st.depth;
-    rp.samples = st.samples;
-    rp.sqrt_samples = st.sqrt_samples;
-    rp.lambda_min = st.lambda_min;
-    rp.lambda_max = st.lambda_max;
-    rp.lambda_range = st.lambda_max - st.lambda_min;
-    const lambda_camera &c = st.camera;
-    rp.cam_pos = mk(c.position[0], c.position[1], c.position[2]);
-    rp.cam_corner = mk(c.corner[0], c.corner[1], c.corner[2]);
-    rp.cam_h = mk(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
-    rp.cam_v = mk(c.vertical[0], c.vertical[1], c.vertical[2]);
-    rp.seed = desc->seed;
-    rp.num_pixels = st.width * st.height;
+    rp.jobs = r.jobs.as<Job>();
+    rp.num_jobs = int(nj);
+    rp.num_pixels = P;
+    rp.depth_max = d_max;
+    rp.active = r.active.as<int>();
 
-    lambda_status s = ctx->ensure_state(rp.num_pixels, rp.depth);
-    if (s != LAMBDA_OK) return s;
-    if (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) {
-        s = ctx->ensure_surrogate_state();
-        if (s != LAMBDA_OK) return s;
-    }
-    cudaStream_t stream = ctx->stream;
     const PathState ps = ctx->pstate;
     const DeviceScene sc = ctx->dscene;
-    const int P = rp.num_pixels;
+    const lambda_tuning &tu = ctx->tuning;
+    const int dev = ctx->device, sms = ctx->sm_count;
+    const int tb = tu.trace_block, sb = tu.shade_block, gs = tu.grid_scale;
+    const size_t stack_smem = size_t(tb) * kStackSmemPerThread;
+    auto grid = [&](const void *fn, int block, size_t smem) {
+        return std::max(1, std::min((P + block - 1) / block, resident_ctas(fn, dev, block, smem) * sms * gs));
+    };
+    const int g_isect = grid((const void *)k_intersect, tb, stack_smem);
+    const int g_shadow = grid((const void *)k_shadow, tb, stack_smem);
+    const int g_lambert = grid((const void *)k_shade_lambert, sb, 0);
+    const int g_spec = grid((const void *)k_shade_specular, sb, 0);
+    const int g_film = grid((const void *)k_shade_film_exact, sb, 0);
     const int pix_blocks = (P + 255) / 256;
-    const int qgrid = std::min(pix_blocks, grid_for(ctx->sm_count, (const void *)k_shade_lambert, 256));
-    const bool surrogate = (desc->flags & LAMBDA_RENDER_THINFILM_SURROGATE) != 0;
-
-    CK(cudaMemsetAsync(ps.stats, 0, 8 * 8, stream), "clear statistics");
-    CK(cudaMemsetAsync(ps.error, 0, 16, stream), "clear flags");
-    CK(cudaMemsetAsync(ps.counts, 0, size_t(kQueues * (rp.depth + 2)) * 4, stream), "clear counters");
-    CK(cudaEventRecord(ctx->ev_start, stream), "event");
-    k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps);
-    CK(cudaGetLastError(), "launch init");
-    int launches = 1;
 
     // One wave's launches. With a profiler every launch is bracketed by events.
-    const bool profile = (desc->flags & LAMBDA_RENDER_PROFILE_STAGES) != 0;
-    StageProfiler prof(stream);
-    auto wave = [&](StageProfiler *pr) -> int {
+    // Inside the pass graph's loop the prologue sets the loop condition.
+    auto wave = [&](StageProfiler *pr, cudaGraphConditionalHandle loop, int waves) -> int {
         int n = 0;
         auto timed = [&](int stage, auto &&launch) {
             if (pr) pr->begin(stage);
@@ -656,99 +723,325 @@ extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc
             if (pr) pr->end();
             n++;
         };
-        timed(1, [&] { k_wave_prologue<<<1, 256, 0, stream>>>(rp.depth, ps); });
+        timed(1, [&] { k_wave_prologue<<<1, 256, 0, stream>>>(d_max, ps, loop, waves, ctx->progress_dev); });
         timed(2, [&] { k_raygen<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
-        const size_t stack_smem = size_t(256) * kStackSmemPerThread;
-        for (int b = 0; b <= rp.depth; b++) {
-            timed(3, [&] { k_intersect<<<qgrid, 256, stack_smem, stream>>>(b, rp, sc, ps); });
-            if (sc.families & 1u) timed(4, [&] { k_shade_lambert<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
-            if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+        for (int b = 0; b <= d_max; b++) {
+            timed(3, [&] { k_intersect<<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps); });
+            if (sc.families & 1u) timed(4, [&] { k_shade_lambert<<<g_lambert, sb, 0, stream>>>(b, rp, sc, ps); });
+            if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<g_spec, sb, 0, stream>>>(b, rp, sc, ps); });
             if (sc.families & 4u) {
                 if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, pr);
-                else timed(6, [&] { k_shade_film_exact<<<qgrid, 256, 0, stream>>>(b, rp, sc, ps); });
+                else timed(6, [&] { k_shade_film_exact<<<g_film, sb, 0, stream>>>(b, rp, sc, ps); });
             }
-            if (sc.families & 1u) timed(7, [&] { k_shadow<<<qgrid, 256, stack_smem, stream>>>(b, rp, sc, ps); });
+            if (sc.families & 1u) timed(7, [&] { k_shadow<<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps); });
         }
         return n;
     };
-    std::vector<Progress> progress(completed ? size_t(rp.samples) : 0);
-    auto report = [&](int w) -> cudaError_t {
-        if (!completed) return cudaSuccess;
-        progress[w] = Progress{completed, int32_t(int64_t(P) * (w + 1) / rp.samples)};
-        if (w + 1 == rp.samples) progress[w].value = P;
-        return cudaLaunchHostFunc(stream, progress_cb, &progress[w]);
+    auto clear = [&]() -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(ps.stats, 0, 8 * 8, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ps.error, 0, 16, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ps.counts, 0, size_t(kQueues * (d_max + 2)) * 4, stream);
+        return e;
     };
-    if (profile) {
-        for (int w = 0; w < rp.samples; w++) {
-            launches += wave(&prof);
+    // pixels of this pass whose samples are all done once `waves` waves have finished
+    auto pixels_done = [&](int waves) {
+        int64_t done = 0;
+        for (size_t k = 0; k < nj; k++)
+            done += int64_t(dj[k].width) * dj[k].height * std::min(waves, dj[k].samples) / dj[k].samples;
+        return int32_t(std::min<int64_t>(completed_base + done, completed_total));
+    };
+    int launches = 0;
+    std::vector<Progress> progress(completed ? size_t(s_max) : 0);
+    if (prof) {
+        CK(clear(), "clear counters");
+        CK(cudaEventRecord(ctx->ev_start, stream), "event");
+        prof->begin(0);
+        k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps);
+        prof->end();
+        launches++;
+        for (int w = 0; w < s_max; w++) {
+            launches += wave(prof, 0, 0);
             CK(cudaGetLastError(), "launch wave");
-            CK(report(w), "progress callback");
-            CK(prof.collect(), "stage timing");
+            if (completed) {
+                progress[w] = Progress{completed, pixels_done(w + 1)};
+                CK(cudaLaunchHostFunc(stream, progress_cb, &progress[w]), "progress callback");
+            }
+            CK(prof->collect(), "stage timing");
         }
+        prof->begin(1);
+        k_wave_prologue<<<1, 256, 0, stream>>>(d_max, ps, 0, 0, nullptr);  // folds the last wave's counts in
+        prof->end();
+        prof->begin(8);
+        k_finish<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps);
+        prof->end();
+        launches += 2;
+        CK(cudaGetLastError(), "launch finish");
+        CK(cudaEventRecord(ctx->ev_stop, stream), "event");
     } else {
-        cudaGraph_t graph = nullptr;
-        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        const int wave_launches = wave(nullptr);
-        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
-        if (ce != cudaSuccess) return ctx->cuda_fail(ce, "capture wave graph");
+        // The whole pass as one graph launch: clear + k_init, a while node whose
+        // body is one sample wave (run s_max times), then the last prologue and
+        // k_finish.
+        cudaGraph_t g = nullptr, pre = nullptr, post = nullptr;
+        cudaGraphConditionalHandle loop = 0;
+        auto fail = [&](cudaError_t e, const char *what) {
+            if (pre) cudaGraphDestroy(pre);
+            if (post) cudaGraphDestroy(post);
+            if (g) cudaGraphDestroy(g);
+            return ctx->cuda_fail(e, what);
+        };
+        cudaError_t e = cudaGraphCreate(&g, 0);
+        if (e != cudaSuccess) return fail(e, "create pass graph");
+        e = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return fail(e, "create wave loop");
+        e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail(e, "begin capture");
+        e = clear();
+        k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps);
+        cudaError_t ce = cudaStreamEndCapture(stream, &pre);
+        if (e != cudaSuccess || ce != cudaSuccess) return fail(e != cudaSuccess ? e : ce, "capture pass prefix");
+        cudaGraphNode_t n_pre = nullptr, n_loop = nullptr, n_post = nullptr;
+        e = cudaGraphAddChildGraphNode(&n_pre, g, nullptr, 0, pre);
+        if (e != cudaSuccess) return fail(e, "build pass graph");
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&n_loop, g, &n_pre, 1, &cp);
+        if (e != cudaSuccess) return fail(e, "build wave loop");
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail(e, "begin capture of the wave");
+        const int wave_launches = wave(nullptr, loop, s_max);
+        ce = cudaStreamEndCapture(stream, &body);
+        if (ce != cudaSuccess) return fail(ce, "capture wave");
+        e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail(e, "begin capture");
+        k_wave_prologue<<<1, 256, 0, stream>>>(d_max, ps, 0, 0, nullptr);  // folds the last wave's counts in
+        k_finish<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps);
+        ce = cudaStreamEndCapture(stream, &post);
+        if (ce != cudaSuccess) return fail(ce, "capture pass suffix");
+        e = cudaGraphAddChildGraphNode(&n_post, g, &n_loop, 1, post);
+        if (e != cudaSuccess) return fail(e, "build pass graph");
         if (ctx->graph_exec) {
             cudaGraphExecDestroy(ctx->graph_exec);
             ctx->graph_exec = nullptr;
         }
-        ce = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (ce != cudaSuccess) return ctx->cuda_fail(ce, "instantiate wave graph");
-        for (int w = 0; w < rp.samples; w++) {
-            CK(cudaGraphLaunch(ctx->graph_exec, stream), "launch wave");
-            launches += wave_launches;
-            CK(report(w), "progress callback");
-        }
+        e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+        cudaGraphDestroy(pre);
+        cudaGraphDestroy(post);
+        cudaGraphDestroy(g);
+        pre = post = g = nullptr;
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "instantiate pass graph");
+        *ctx->progress_host = 0;
+        CK(cudaEventRecord(ctx->ev_start, stream), "event");
+        CK(cudaGraphLaunch(ctx->graph_exec, stream), "launch pass graph");
+        CK(cudaEventRecord(ctx->ev_stop, stream), "event");
+        launches = 1 + s_max * wave_launches + 2;
     }
-    k_wave_prologue<<<1, 256, 0, stream>>>(rp.depth, ps);  // folds the last wave's counts into the statistics
-    float *dout = out_device ? out_rgb : ctx->rbuf.out.as<float>();
-    k_finish<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps, dout);
-    launches += 2;
-    CK(cudaGetLastError(), "launch finish");
-    CK(cudaEventRecord(ctx->ev_stop, stream), "event");
-    if (!out_device)
-        CK(cudaMemcpyAsync(out_rgb, dout, size_t(P) * 12, cudaMemcpyDeviceToHost, stream), "copy image to host");
+    for (size_t k = 0; k < nj; k++) {
+        const lambda_job &j = jobs[order[first + k]];
+        if (!(j.desc.flags & LAMBDA_RENDER_OUTPUT_DEVICE))
+            CK(cudaMemcpyAsync(j.out_rgb, dj[k].out, size_t(dj[k].width) * dj[k].height * 12, cudaMemcpyDeviceToHost,
+                               stream),
+               "copy image to host");
+    }
     unsigned long long stats[8] = {0};
     int err[4] = {0};
     CK(cudaMemcpyAsync(stats, ps.stats, sizeof(stats), cudaMemcpyDeviceToHost, stream), "read statistics");
     CK(cudaMemcpyAsync(err, ps.error, sizeof(err), cudaMemcpyDeviceToHost, stream), "read flags");
+    if (completed && !prof) {
+        // progress from the waves the graph has started (mapped host counter)
+        for (;;) {
+            const cudaError_t q = cudaStreamQuery(stream);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) return ctx->cuda_fail(q, "render");
+            *completed = pixels_done(std::max(0, *reinterpret_cast<volatile int *>(ctx->progress_host) - 1));
+            std::this_thread::sleep_for(std::chrono::milliseconds(2));
+        }
+    }
     CK(cudaStreamSynchronize(stream), "render");
+    if (prof) CK(prof->collect(), "stage timing");
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+    tot.ms += ms;
+    for (size_t k = 0; k < nj; k++) tot.paths += int64_t(dj[k].width) * dj[k].height * dj[k].samples;
+    tot.pixels += P;
+    for (int i = 0; i < 8; i++) tot.stats[i] += stats[i];
+    tot.launches += launches;
+    tot.waves += s_max;
+    tot.err |= err[0];
+    return LAMBDA_OK;
+}
+
+// Renders n jobs in passes of whole jobs (at most tuning.max_pixels pixels a pass,
+// a larger single job alone), ordered by decreasing sample count.
+lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volatile int32_t *completed) {
+    if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
+    const uint32_t mode = jobs[0].desc.flags & (LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_PROFILE_STAGES);
+    int64_t total_pixels = 0;
+    for (int i = 0; i < n; i++) {
+        if (!jobs[i].out_rgb) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "job without an output image");
+        lambda_status s = check_settings(ctx, jobs[i].desc.settings);
+        if (s != LAMBDA_OK) return s;
+        if ((jobs[i].desc.flags & (LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_PROFILE_STAGES)) != mode)
+            return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "the jobs of a batch must share the thin-film mode and profiling flag");
+        total_pixels += int64_t(jobs[i].desc.settings.width) * jobs[i].desc.settings.height;
+    }
+    if (total_pixels > INT32_MAX) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "more than 2^31 pixels in one batch");
+    const bool surrogate = (mode & LAMBDA_RENDER_THINFILM_SURROGATE) != 0;
+    const bool profile = (mode & LAMBDA_RENDER_PROFILE_STAGES) != 0;
+    if (surrogate) {
+        lambda_status s = ctx->surrogate_ready();
+        if (s != LAMBDA_OK) return s;
+    }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    for (int i = 0; i < n; i++)
+        if ((jobs[i].desc.flags & LAMBDA_RENDER_OUTPUT_DEVICE) && !is_device_pointer(jobs[i].out_rgb))
+            return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "LAMBDA_RENDER_OUTPUT_DEVICE given a host pointer");
+    if (surrogate) {
+        lambda_status s = ctx->ensure_surrogate_state();
+        if (s != LAMBDA_OK) return s;
+    }
+    if (!ctx->progress_host) {
+        CK(cudaHostAlloc(reinterpret_cast<void **>(&ctx->progress_host), sizeof(int), cudaHostAllocMapped),
+           "allocate progress counter");
+        CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&ctx->progress_dev), ctx->progress_host, 0),
+           "map progress counter");
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return jobs[a].desc.settings.samples > jobs[b].desc.settings.samples;
+    });
+    const int64_t cap = ctx->tuning.max_pixels > 0 ? ctx->tuning.max_pixels : (int64_t(1) << 30);
+    StageProfiler prof(ctx->stream);
+    RenderTotals tot;
+    size_t first = 0;
+    while (first < size_t(n)) {
+        size_t last = first + 1;
+        int64_t px = int64_t(jobs[order[first]].desc.settings.width) * jobs[order[first]].desc.settings.height;
+        while (last < size_t(n)) {
+            const int64_t add = int64_t(jobs[order[last]].desc.settings.width) * jobs[order[last]].desc.settings.height;
+            if (px + add > cap) break;
+            px += add;
+            last++;
+        }
+        lambda_status s = render_pass(ctx, jobs, order, first, last, surrogate, profile ? &prof : nullptr, completed,
+                                      int32_t(tot.pixels), int32_t(total_pixels), tot);
+        if (s != LAMBDA_OK) return s;
+        first = last;
+    }
+    if (completed) *completed = int32_t(total_pixels);
     ctx->stats = lambda_render_stats{};
-    ctx->stats.render_ms = ms;
-    ctx->stats.paths = int64_t(P) * rp.samples;
-    ctx->stats.segments = int64_t(stats[0]);
-    ctx->stats.shadow_rays = int64_t(stats[1]);
-    ctx->stats.thinfilm_hits = int64_t(stats[2]);
-    ctx->stats.thinfilm_fallback = int64_t(stats[3]);
-    ctx->stats.kernel_launches = launches;
-    ctx->stats.waves = rp.samples;
+    ctx->stats.render_ms = tot.ms;
+    ctx->stats.paths = tot.paths;
+    ctx->stats.segments = int64_t(tot.stats[0]);
+    ctx->stats.shadow_rays = int64_t(tot.stats[1]);
+    ctx->stats.thinfilm_hits = int64_t(tot.stats[2]);
+    ctx->stats.thinfilm_fallback = int64_t(tot.stats[3]);
+    ctx->stats.kernel_launches = tot.launches;
+    ctx->stats.waves = tot.waves;
     ctx->stats.surrogate_ctas_per_sm = surrogate ? ctx->mlp_ctas_per_sm : 0;
     if (profile) {
-        prof.totals[0] = 0;
         for (int i = 0; i < LAMBDA_NUM_STAGES; i++) {
             ctx->stage_times[i].ms = prof.totals[i];
             ctx->stage_times[i].launches = prof.counts[i];
         }
-        ctx->stage_times[0].launches = 1;
-        ctx->stage_times[0].items = P;
-        ctx->stage_times[1].items = rp.samples;
-        ctx->stage_times[2].items = int64_t(P) * rp.samples;
+        ctx->stage_times[0].items = tot.pixels;
+        ctx->stage_times[1].items = tot.waves;
+        ctx->stage_times[2].items = tot.paths;
         ctx->stage_times[3].items = ctx->stats.segments;
-        ctx->stage_times[4].items = int64_t(stats[4]);
-        ctx->stage_times[5].items = int64_t(stats[5]);
+        ctx->stage_times[4].items = int64_t(tot.stats[4]);
+        ctx->stage_times[5].items = int64_t(tot.stats[5]);
         ctx->stage_times[6].items = surrogate ? 0 : ctx->stats.thinfilm_hits;
         ctx->stage_times[7].items = ctx->stats.shadow_rays;
-        ctx->stage_times[8].items = P;
+        ctx->stage_times[8].items = tot.pixels;
         ctx->stage_times[9].items = surrogate ? ctx->stats.thinfilm_hits : 0;
     }
-    if (err[0] & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
-    if (err[0] & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
+    if (tot.err & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
+    if (tot.err & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
+    return LAMBDA_OK;
+}
+
+bool tuning_ok(const lambda_tuning &t) {
+    auto block_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
+    return block_ok(t.trace_block) && block_ok(t.shade_block) && (t.grid_scale == 1 || t.grid_scale == 2) &&
+           t.max_pixels >= 0;
+}
+
+}  // namespace
+
+extern "C" lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc *desc, float *out_rgb,
+                                       volatile int32_t *completed) {
+    if (!ctx || !desc || !out_rgb) return LAMBDA_ERR_INVALID_ARGUMENT;
+    const lambda_job job{*desc, out_rgb};
+    return render_jobs(ctx, &job, 1, completed);
+}
+
+extern "C" lambda_status lambda_render_batch(lambda_ctx *ctx, const lambda_job *jobs, int32_t n,
+                                             volatile int32_t *completed) {
+    if (!ctx || !jobs || n < 1) return LAMBDA_ERR_INVALID_ARGUMENT;
+    return render_jobs(ctx, jobs, n, completed);
+}
+
+extern "C" lambda_status lambda_set_tuning(lambda_ctx *ctx, const lambda_tuning *tuning) {
+    if (!ctx || !tuning) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (!tuning_ok(*tuning)) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "invalid tuning values");
+    ctx->tuning = *tuning;
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning *tuning) {
+    if (!ctx || !tuning) return LAMBDA_ERR_INVALID_ARGUMENT;
+    *tuning = ctx->tuning;
+    return LAMBDA_OK;
+}
+
+// Times the probe render (its output stays in device memory) under every candidate
+// launch shape, after one warm-up render per candidate, and keeps the fastest. The
+// path-state capacity is set from free device memory: half of it, at the bytes of
+// path state and queues a pixel needs.
+extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out) {
+    if (!ctx || !probe) return LAMBDA_ERR_INVALID_ARGUMENT;
+    lambda_status s = check_settings(ctx, probe->settings);
+    if (s != LAMBDA_OK) return s;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t P = size_t(probe->settings.width) * probe->settings.height;
+    DeviceBuffer img;
+    CK(img.reserve(P * 12), "allocate probe image");
+    lambda_job job{*probe, img.as<float>()};
+    job.desc.flags = (probe->flags & LAMBDA_RENDER_THINFILM_SURROGATE) | LAMBDA_RENDER_OUTPUT_DEVICE;
+    const lambda_tuning keep = ctx->tuning;
+    lambda_tuning best = keep;
+    double best_ms = 1e300;
+    for (int tb : {64, 128, 256})
+        for (int sb : {64, 128, 256})
+            for (int gs : {1, 2}) {
+                ctx->tuning = lambda_tuning{tb, sb, gs, keep.max_pixels};
+                double ms = 0;
+                for (int rep = 0; rep < 2 && s == LAMBDA_OK; rep++) {
+                    s = render_jobs(ctx, &job, 1, nullptr);
+                    ms = ctx->stats.render_ms;
+                }
+                if (s != LAMBDA_OK) {
+                    ctx->tuning = keep;
+                    img.release();
+                    return s;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = ctx->tuning;
+                }
+            }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        constexpr size_t kBytesPerPixel = 8 + 16 * 13 + 8 + 8 + 4 * 6 + 12;  // path state, queues, staged image
+        best.max_pixels = int32_t(std::min<size_t>((free_b / 2) / kBytesPerPixel, size_t(1) << 30));
+    }
+    img.release();
+    ctx->tuning = best;
+    if (out) *out = best;
     return LAMBDA_OK;
 }
 

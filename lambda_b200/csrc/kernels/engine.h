@@ -21,6 +21,11 @@ struct DeviceBuffer {
 
 bool is_device_pointer(const void *p);
 
+// CTAs of `block` threads with `dyn_smem` bytes of dynamic shared memory that one SM
+// holds at once, from the kernel's registers and static shared memory and the SM's
+// limits (at least 1).
+int resident_ctas(const void *fn, int device, int block, size_t dyn_smem);
+
 // Brackets kernel launches with CUDA events and totals their device time per
 // stage (LAMBDA_RENDER_PROFILE_STAGES).
 struct StageProfiler {
@@ -45,7 +50,7 @@ struct SceneBuffers {
 
 struct RenderBuffers {
     DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
-        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out;
+        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out, path_info, jobs, active;
 };
 
 struct SurrogateBuffers {
@@ -70,6 +75,9 @@ struct lambda_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     lambda_render_stats stats{};
     lambda_stage_time stage_times[LAMBDA_NUM_STAGES]{};
+    lambda_tuning tuning{256, 256, 1, 0};  // launch shapes (max_pixels 0: no limit)
+    int *progress_host = nullptr;           // waves started by the running pass graph (mapped host memory)
+    int *progress_dev = nullptr;            // its device address
 
     // surrogate
     bool has_surrogate = false;
@@ -95,7 +103,7 @@ struct lambda_ctx {
                 &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
                 &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
-                &r.stats, &r.error, &r.out, &sbuf.weights_bf16, &sbuf.weights_f32};
+                &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &sbuf.weights_bf16, &sbuf.weights_f32};
     }
 };
 

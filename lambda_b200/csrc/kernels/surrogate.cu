@@ -638,11 +638,11 @@ __global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams 
                 thin_film_thickness(sc, s, thick);
                 R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
             }
-            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            Rng rng = path_rng(ps, p);
             s4 att;
             f3 nd;
             thin_film_scatter(sc, s, R, rng, att, nd);
-            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
+            alive = finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
@@ -746,36 +746,14 @@ lambda_status install(lambda_ctx *ctx, const float *params_host, const lambda_fi
     return LAMBDA_OK;
 }
 
-// CTAs of 128 threads with kSmemBytes of dynamic shared memory that one SM holds
-// at once, from the kernel's registers and shared memory and the SM's register
-// file, shared memory and thread limits (registers are allocated per thread in
-// multiples of 8; every CTA also holds the SM's per-block reservation).
-int resident_ctas(const void *fn, int device) {
-    cudaFuncAttributes fa{};
-    int smem_sm = 0, regs_sm = 0, threads_sm = 0, reserved = 0;
-    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess ||
-        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
-        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device) != cudaSuccess ||
-        cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device) != cudaSuccess ||
-        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess) {
-        cudaGetLastError();
-        return 1;
-    }
-    const int regs = (std::max(fa.numRegs, 1) + 7) / 8 * 8;
-    const int by_regs = regs_sm / (128 * regs);
-    const int by_smem = smem_sm / int(kSmemBytes + fa.sharedSizeBytes + reserved);
-    const int by_threads = threads_sm / 128;
-    return std::max(1, std::min({by_regs, by_smem, by_threads}));
-}
-
 // Resident CTAs per SM of the tensor-core MLP kernels, capped so their TMEM
 // columns fit the SM's 512 and no allocation ever waits. Computed outside stream
 // capture and cached on the context.
 int mlp_grid(lambda_ctx *ctx) {
     if (ctx->mlp_ctas_per_sm <= 0) {
-        const int per_sm = std::min({resident_ctas((const void *)k_mlp_tc<false>, ctx->device),
-                                     resident_ctas((const void *)k_mlp_tc<true>, ctx->device),
-                                     resident_ctas((const void *)k_film_fused, ctx->device)});
+        const int per_sm = std::min({resident_ctas((const void *)k_mlp_tc<false>, ctx->device, 128, kSmemBytes),
+                                     resident_ctas((const void *)k_mlp_tc<true>, ctx->device, 128, kSmemBytes),
+                                     resident_ctas((const void *)k_film_fused, ctx->device, 128, kSmemBytes)});
         ctx->mlp_ctas_per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
     }
     return ctx->mlp_ctas_per_sm * ctx->sm_count;

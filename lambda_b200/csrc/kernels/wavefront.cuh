@@ -43,21 +43,36 @@ __device__ __forceinline__ int warp_push(int *counter, bool want) {
     return want ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
 }
 
-__device__ __forceinline__ s4 hero_wavelengths(const RenderParams &rp, float lambda0) {
+__device__ __forceinline__ s4 hero_wavelengths(const Job &job, float lambda0) {
     s4 l;
     for (int k = 0; k < kHero; k++)
-        l.v[k] = rp.lambda_min + fmodf(lambda0 - rp.lambda_min + float(k) * rp.lambda_range / kHero, rp.lambda_range);
+        l.v[k] = job.lambda_min + fmodf(lambda0 - job.lambda_min + float(k) * job.lambda_range / kHero, job.lambda_range);
     return l;
 }
 
-// Every pixel: seed its stream, zero film and radiance.
+// Index of the job that owns virtual pixel p (jobs ordered by base).
+__device__ __forceinline__ int job_of(const RenderParams &rp, int p) {
+    int lo = 0, hi = rp.num_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (rp.jobs[mid].base <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Every pixel: seed its stream (job seed, job-local pixel index, as a render of
+// that job alone), record its depth limit, zero film and radiance.
 LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= rp.num_pixels) return;
-    ps.rng[p] = lambda_rng::pcg_seed(rp.seed, uint64_t(p));
+    const Job &job = rp.jobs[job_of(rp, p)];
+    const int local = p - job.base;
+    ps.rng[p] = lambda_rng::pcg_seed(job.seed, uint64_t(local));
+    ps.path_info[p] = make_int2(local, job.depth);
     ps.film[p] = make_float4(0, 0, 0, 0);
     ps.radiance[p] = make_float4(0, 0, 0, 0);
-    ps.lam[p] = make_float4(rp.lambda_min, rp.lambda_min, rp.lambda_min, rp.lambda_min);
+    ps.lam[p] = make_float4(job.lambda_min, job.lambda_min, job.lambda_min, job.lambda_min);
     if (p == 0) {
         ps.wave[0] = 0;
         ps.wave[1] = 0;
@@ -65,8 +80,11 @@ LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
 }
 
 // Wave prologue (one block): fold the last wave's queue sizes into the
-// statistics, clear the counters, advance the wave index.
-LAMBDA_KERNEL void k_wave_prologue(int depth, PathState ps) {
+// statistics, clear the counters, advance the wave index. Inside a graph's
+// sample-wave loop (waves > 0) it also sets the loop condition, true while waves
+// remain after the one starting now, so the loop runs exactly `waves` times, and
+// publishes the number of waves started to `progress` (mapped host memory).
+LAMBDA_KERNEL void k_wave_prologue(int depth, PathState ps, cudaGraphConditionalHandle loop, int waves, int *progress) {
     const int n = kQueues * (depth + 2);
     __shared__ unsigned long long tot[kQueues];
     if (threadIdx.x < kQueues) tot[threadIdx.x] = 0;
@@ -83,41 +101,55 @@ LAMBDA_KERNEL void k_wave_prologue(int depth, PathState ps) {
         ps.stats[4] += tot[kQLambert];
         ps.stats[5] += tot[kQSpecular];
         ps.wave[1] = ps.wave[0];
-        ps.wave[0] += 1;
+        const int started = ps.wave[0] + 1;
+        ps.wave[0] = started;
+        if (waves > 0) {
+            cudaGraphSetConditional(loop, started < waves ? 1u : 0u);
+            if (progress) *reinterpret_cast<volatile int *>(progress) = started;
+        }
     }
 }
 
 // Film += linear sRGB of the finished sample (renderer.h:84), then start the
 // next sample: stratified jitter, hero wavelength, camera ray (renderer.h:69-81).
+// Pixels of jobs whose last sample was the previous wave only bank that sample.
 LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= rp.num_pixels) return;
     const int s = ps.wave[1];
-    const int i = s / rp.sqrt_samples, j = s % rp.sqrt_samples;
-    const int px = p % rp.width, py = p / rp.width;
+    const int n_now = rp.active[s];
+    const int n_prev = s > 0 ? rp.active[s - 1] : n_now;
+    if (p == 0) ps.counts[queue_slot(0, kQActive)] = n_now;
+    if (p >= n_prev) return;
+    const Job &job = rp.jobs[job_of(rp, p)];
 
-    const f3 rgb = spectrum_to_rgb(sc, from_f4(ps.radiance[p]), from_f4(ps.lam[p]), rp.lambda_range);
+    const f3 rgb = spectrum_to_rgb(sc, from_f4(ps.radiance[p]), from_f4(ps.lam[p]), job.lambda_range);
     float4 film = ps.film[p];
     film.x += rgb.x;
     film.y += rgb.y;
     film.z += rgb.z;
     ps.film[p] = film;
+    if (p >= n_now) {
+        ps.radiance[p] = make_float4(0, 0, 0, 0);
+        return;
+    }
 
-    Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
-    const float u = (float(px) + (float(i) + rng.next()) / float(rp.sqrt_samples)) / float(rp.width);
-    const float v = (float(py) + (float(j) + rng.next()) / float(rp.sqrt_samples)) / float(rp.height);
-    const float lambda0 = rp.lambda_min + rng.next() * (rp.lambda_max - rp.lambda_min);
-    const s4 lam = hero_wavelengths(rp, lambda0);
-    const f3 dir = normalize(rp.cam_corner + rp.cam_h * u + rp.cam_v * v - rp.cam_pos);
+    const int local = p - job.base;
+    const int i = s / job.sqrt_samples, j = s % job.sqrt_samples;
+    const int px = local % job.width, py = local / job.width;
+    Rng rng = pixel_rng(ps.rng[p], local);
+    const float u = (float(px) + (float(i) + rng.next()) / float(job.sqrt_samples)) / float(job.width);
+    const float v = (float(py) + (float(j) + rng.next()) / float(job.sqrt_samples)) / float(job.height);
+    const float lambda0 = job.lambda_min + rng.next() * (job.lambda_max - job.lambda_min);
+    const s4 lam = hero_wavelengths(job, lambda0);
+    const f3 dir = normalize(job.cam_corner + job.cam_h * u + job.cam_v * v - job.cam_pos);
 
     ps.rng[p] = rng.state;
     ps.lam[p] = to_f4(lam);
-    ps.ray_o[p] = make_float4(rp.cam_pos.x, rp.cam_pos.y, rp.cam_pos.z, 1.0f);
+    ps.ray_o[p] = make_float4(job.cam_pos.x, job.cam_pos.y, job.cam_pos.z, 1.0f);
     ps.ray_d[p] = make_float4(dir.x, dir.y, dir.z, 1.0f);
     ps.throughput[p] = make_float4(1, 1, 1, 1);
     ps.radiance[p] = make_float4(0, 0, 0, 0);
     ps.queue[0][p] = p;
-    if (p == 0) ps.counts[queue_slot(0, kQActive)] = rp.num_pixels;
 }
 
 // Material index of object `obj` in instance `inst` (instance.h:38).
@@ -205,6 +237,9 @@ struct ShadeIn {
     s4 T, lam;
 };
 
+// The path's PCG32: its state and its stream, the job-local pixel index.
+__device__ __forceinline__ Rng path_rng(const PathState &ps, int p) { return pixel_rng(ps.rng[p], ps.path_info[p].x); }
+
 __device__ __forceinline__ ShadeIn load_shade(const PathState &ps, const DeviceScene &sc, int p) {
     ShadeIn s;
     s.p = p;
@@ -225,8 +260,8 @@ __device__ __forceinline__ ShadeIn load_shade(const PathState &ps, const DeviceS
 
 // Throughput update, Russian roulette and the depth limit (renderer.h:177-191);
 // writes the scattered ray and returns whether the path continues.
-__device__ __forceinline__ bool finish_scatter(const RenderParams &rp, const PathState &ps, const ShadeIn &s, Rng &rng,
-                                               int bounce, s4 att, f3 nd, float pdf, bool spec) {
+__device__ __forceinline__ bool finish_scatter(const PathState &ps, const ShadeIn &s, Rng &rng, int bounce, s4 att, f3 nd,
+                                               float pdf, bool spec) {
     s4 T = s.T;
     if (spec) T = T * att;
     else T = T * ((att * dot(s.nrm, nd)) / pdf);
@@ -236,7 +271,7 @@ __device__ __forceinline__ bool finish_scatter(const RenderParams &rp, const Pat
         if (rng.next() < qq) alive = false;
         else T = T / (1 - qq);
     }
-    if (bounce >= rp.depth) alive = false;
+    if (bounce >= ps.path_info[s.p].y) alive = false;  // the depth limit of the path's job
     ps.rng[s.p] = rng.state;
     ps.throughput[s.p] = to_f4(T);
     ps.ray_o[s.p] = make_float4(s.sp.point.x, s.sp.point.y, s.sp.point.z, pdf);
@@ -258,7 +293,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_lambert(int bounce, RenderP
         if (idx < n) {
             p = q[idx];
             const ShadeIn s = load_shade(ps, sc, p);
-            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            Rng rng = path_rng(ps, p);
             const s4 albedo = spectrum_texture4(sc, s.m.y, s.sp, s.lam);
             if (sc.total_light_power > 0) {
                 const float target = sc.total_light_power * rng.next();
@@ -311,7 +346,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_lambert(int bounce, RenderP
             const float cl = dot(s.nrm, nd);
             const s4 att = cl <= 0 ? s4_fill(0) : albedo / kPi;
             const float pdf = cl > 0 ? cl / kPi : 0;
-            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, pdf, false);
+            alive = finish_scatter(ps, s, rng, bounce, att, nd, pdf, false);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
@@ -340,7 +375,7 @@ LAMBDA_KERNEL void __launch_bounds__(256) k_shade_specular(int bounce, RenderPar
         if (idx < n) {
             p = q[idx];
             const ShadeIn s = load_shade(ps, sc, p);
-            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
+            Rng rng = path_rng(ps, p);
             s4 att;
             f3 nd;
             if (s.m.x == kMirror) {
@@ -366,7 +401,7 @@ LAMBDA_KERNEL void __launch_bounds__(256) k_shade_specular(int bounce, RenderPar
                     att.v[k] = refl ? r / rh : (fabsf(a0 - n0h) < kEps && fabsf(a1 - n1h) < kEps) ? (1 - r) / (1 - rh) : 0;
                 }
             }
-            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
+            alive = finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
@@ -454,14 +489,14 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, Rend
         if (idx < n) {
             p = q[idx];
             const ShadeIn s = load_shade(ps, sc, p);
-            Rng rng{ps.rng[p], lambda_rng::pcg_increment(uint64_t(p))};
             float thick[kMaxFilmLayers];
             thin_film_thickness(sc, s, thick);
             const s4 R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+            Rng rng = path_rng(ps, p);
             s4 att;
             f3 nd;
             thin_film_scatter(sc, s, R, rng, att, nd);
-            alive = finish_scatter(rp, ps, s, rng, bounce, att, nd, 0, true);
+            alive = finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
@@ -504,19 +539,23 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams r
     }
 }
 
-// Last sample into the film, then the average (renderer.h:84-91).
-LAMBDA_KERNEL void k_finish(RenderParams rp, DeviceScene sc, PathState ps, float *out) {
+// Last sample into the film, then the average (renderer.h:84-91), into the
+// job's own image. Jobs that finished before the last wave banked their last
+// sample in k_raygen and hold zero radiance here.
+LAMBDA_KERNEL void k_finish(RenderParams rp, DeviceScene sc, PathState ps) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= rp.num_pixels) return;
-    const f3 rgb = spectrum_to_rgb(sc, from_f4(ps.radiance[p]), from_f4(ps.lam[p]), rp.lambda_range);
+    const Job &job = rp.jobs[job_of(rp, p)];
+    const f3 rgb = spectrum_to_rgb(sc, from_f4(ps.radiance[p]), from_f4(ps.lam[p]), job.lambda_range);
     float4 film = ps.film[p];
     film.x += rgb.x;
     film.y += rgb.y;
     film.z += rgb.z;
-    const float inv = float(rp.samples);
-    out[3 * size_t(p)] = film.x / inv;
-    out[3 * size_t(p) + 1] = film.y / inv;
-    out[3 * size_t(p) + 2] = film.z / inv;
+    const float inv = float(job.samples);
+    const size_t local = size_t(p - job.base);
+    job.out[3 * local] = film.x / inv;
+    job.out[3 * local + 1] = film.y / inv;
+    job.out[3 * local + 2] = film.z / inv;
 }
 
 }  // namespace lambda_dev

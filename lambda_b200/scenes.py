@@ -36,6 +36,7 @@ __all__ = [
     "thinfilm_spheres",
     "perlin_sphere",
     "look_at_camera",
+    "random_pose_jobs",
 ]
 
 
@@ -158,6 +159,40 @@ def thinfilm_spheres(directory: str, width: int = 1920, height: int = 1080, spp:
     ]
     _write(path, lines)
     return SceneFiles(path, seed, width, height, spp, depth)
+
+
+def random_pose_jobs(scene, n: int, seed: int = 4, resolutions=(128, 256, 512, 1024), spps=(1, 4, 16, 64, 256),
+                     depth=(4, 24), flags: int = 0, target=(0.0, 0.3, 0.0)) -> list:
+    """Render descriptors of `n` views of an uploaded scene for a batch: square
+    resolutions and sample counts drawn uniformly from the given sets, depth
+    uniform in [depth[0], depth[1]], and a camera at a random azimuth, distance
+    8-11 and height 2.5-6 looking at `target` (jittered by up to 0.5) with a
+    35-50 degree field of view. Render seed of job i is seed * 1000 + i."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        res = int(rng.choice(resolutions))
+        spp = int(rng.choice(spps))
+        dep = int(rng.integers(depth[0], depth[1] + 1))
+        az = rng.uniform(0, 2 * math.pi)
+        dist = rng.uniform(8.0, 11.0)
+        height = rng.uniform(2.5, 6.0)
+        tgt = np.asarray(target) + rng.uniform(-0.5, 0.5, 3)
+        pos = (dist * math.sin(az), height, dist * math.cos(az))
+        cam = look_at_camera(pos, tgt, (0.0, 1.0, 0.0), rng.uniform(35.0, 50.0), 1.0)
+        d = scene.render_desc(seed=seed * 1000 + i, flags=flags)
+        st = d.settings
+        st.width = st.height = res
+        st.depth = dep
+        root = int(round(spp ** 0.5))
+        st.samples, st.sqrt_samples = spp, root
+        for k in range(3):
+            st.camera.position[k] = cam[0][k]
+            st.camera.corner[k] = cam[1][k]
+            st.camera.horizontal[k] = cam[2][k]
+            st.camera.vertical[k] = cam[3][k]
+        out.append(d)
+    return out
 
 
 # --------------------------------------------------------------------------
