@@ -281,6 +281,7 @@ typedef struct lambda_tuning {
     int32_t shade_block; /* threads per CTA of the shading kernels: 64, 128 or 256 */
     int32_t grid_scale;  /* persistent grids hold grid_scale x the CTAs that fit on all SMs at once: 1 or 2 */
     int32_t max_pixels;  /* path-state capacity: a batch above it runs as several passes of whole jobs */
+    int32_t bvh_width;   /* children per node of the traversed BVH: 2, 4 or 8 (every width finds the same hits) */
 } lambda_tuning;
 
 lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out);

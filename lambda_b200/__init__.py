@@ -259,8 +259,9 @@ class Context:
         self._check(self._lib.lambda_autotune(self._h, C.byref(probe), C.byref(t)))
         return t
 
-    def set_tuning(self, trace_block: int, shade_block: int, grid_scale: int = 1, max_pixels: int = 0) -> None:
-        t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels)
+    def set_tuning(self, trace_block: int, shade_block: int, grid_scale: int = 1, max_pixels: int = 0,
+                   bvh_width: int = 4) -> None:
+        t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels, bvh_width)
         self._check(self._lib.lambda_set_tuning(self._h, C.byref(t)))
 
     def tuning(self) -> N.Tuning:

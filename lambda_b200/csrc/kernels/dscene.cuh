@@ -378,19 +378,19 @@ __device__ __forceinline__ void prim_attributes(const DeviceScene &s, int obj, c
     if (!h.front) h.normal = h.normal * -1.0f;
 }
 
-// Traversal stacks: 20 entries each (BVH_MAX_DEPTH, constants.h:10; the build
-// stops at depth 20, so a depth-first walk never holds more). LocalStack lives in
-// per-thread local memory; SharedStack is a slice of shared memory laid out
-// entry-major (entry i of thread t at base[i * stride + t]) so a warp's pushes
-// and pops hit 32 different banks.
-struct LocalStack {
-    int a[kStackDepth];
-    __device__ __forceinline__ int &operator[](int i) { return a[i]; }
-};
-struct SharedStack {
-    int *base;
+// Traversal stack of one thread in shared memory, entry-major (entry i of thread t
+// at base[i * stride + t], so a warp's pushes and pops hit 32 different banks). An
+// entry is a wide-BVH code and the entry distance of its box. The capacity is the
+// most entries the scene's trees can need (computed when the scene is uploaded).
+struct WideStack {
+    int *code;
+    float *te;
     int stride;
-    __device__ __forceinline__ int &operator[](int i) { return base[i * stride]; }
+    int cap;
+    __device__ __forceinline__ void put(int i, int c, float t) const {
+        code[i * stride] = c;
+        te[i * stride] = t;
+    }
 };
 
 // World -> instance space (instance.h:50-52). An identity instance's transform
@@ -416,63 +416,79 @@ __device__ __forceinline__ void to_world(const DeviceScene &s, int inst, const I
     h.point = xform(m, h.point, 1);
 }
 
-// Scene::hit in closest-hit mode (scene.h:51-124): two-level depth-first
-// traversal, right child popped first, a TLAS leaf tests only its first instance
-// (scene.h:80), candidates accepted when t < best. Returns false on a miss.
-// `overflow` is set if a stack would overflow.
-template <class Stack>
-__device__ __forceinline__ bool closest_hit_t(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow, Stack stack,
-                                              Stack sub) {
+// Expands wide node w: tests its K children (wide_bvh.h) against ray r and pushes
+// the ones whose box the ray enters no farther than `best`, last-visited first, with
+// their entry distances. Returns the new stack size; sets `overflow` (and stops)
+// if the stack is full, which the stack sizes computed for the scene rule out.
+template <int K>
+__device__ __forceinline__ int wide_expand(const DeviceScene &s, int w, const Ray3 &r, float best, const WideStack &st,
+                                           int sp, bool &overflow) {
+    const float4 *c = s.wide + size_t(w) * (2 * K);
+#pragma unroll
+    for (int i = K - 1; i >= 0; i--) {
+        const float4 lo = __ldg(c + 2 * i), hi = __ldg(c + 2 * i + 1);
+        float te;
+        if (slab(lo, hi, r, te) && !(te > best)) {
+            if (sp >= st.cap) {
+                overflow = true;
+                return sp;
+            }
+            st.put(sp++, __float_as_int(lo.w), te);
+        }
+    }
+    return sp;
+}
+
+// Scene::hit in closest-hit mode (scene.h:51-124) over the wide BVH: two-level
+// depth-first traversal that visits the nodes the reference visits in the order it
+// visits them (right child first), culls an entry when its box starts beyond the best
+// hit, lets a TLAS leaf test only its first instance (scene.h:80), and accepts
+// candidates when t < best. Returns false on a miss.
+template <int K>
+__device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow,
+                                              const WideStack &st, const WideStack &sub) {
     const Ray3 wr = make_ray(o, d);
     float best = kMax;
     int best_obj = -1, best_inst = -1;
     int sp = 0;
-    stack[sp++] = 0;
+    float te;
+    if (slab(__ldg(&s.nodes[0]), __ldg(&s.nodes[1]), wr, te)) st.put(sp++, __ldg(&s.wide_code[0]), te);
     while (sp > 0) {
-        const int cur = stack[--sp];
-        const float4 lo = __ldg(&s.nodes[2 * cur]), hi = __ldg(&s.nodes[2 * cur + 1]);
-        float te;
-        if (!slab(lo, hi, wr, te) || te > best) continue;
-        const int count = __float_as_int(hi.w);
-        if (count > 0) {
-            const int inst = __float_as_int(lo.w);
-            const InstanceRef ir = instance_ref(s, inst);
-            const int4 hd = ir.header();
-            const Ray3 lr = to_local(s, inst, ir, o, d);
-            int ssp = 0;
-            sub[ssp++] = hd.z;
-            while (ssp > 0) {
-                const int sc = sub[--ssp];
-                const float4 l2 = __ldg(&s.nodes[2 * sc]), h2 = __ldg(&s.nodes[2 * sc + 1]);
-                if (!slab(l2, h2, lr, te) || te > best) continue;
-                const int c2 = __float_as_int(h2.w);
-                if (c2 > 0) {
-                    const int first = __float_as_int(l2.w);
-                    for (int k = 0; k < c2; k++) {
-                        const float t = intersect_t(load_prim(s, first + k), lr, best);
-                        if (t >= 0) {
-                            best = t;
-                            best_obj = first + k;
-                            best_inst = inst;
-                        }
-                    }
-                } else {
-                    if (ssp + 2 > kStackDepth) {
-                        overflow = true;
-                        break;
-                    }
-                    sub[ssp++] = sc + 1;
-                    sub[ssp++] = __float_as_int(l2.w);
+        --sp;
+        const int code = st.code[sp * st.stride];
+        if (st.te[sp * st.stride] > best) continue;
+        if (code >= 0) {
+            sp = wide_expand<K>(s, code, wr, best, st, sp, overflow);
+            if (overflow) break;
+            continue;
+        }
+        const int inst = __ldg(&s.wide_leaves[-code - 1]).x;
+        const InstanceRef ir = instance_ref(s, inst);
+        const int root = ir.header().z;
+        const Ray3 lr = to_local(s, inst, ir, o, d);
+        if (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best) continue;
+        int ssp = 0;
+        sub.put(ssp++, __ldg(&s.wide_code[root]), te);
+        while (ssp > 0) {
+            --ssp;
+            const int c2 = sub.code[ssp * sub.stride];
+            if (sub.te[ssp * sub.stride] > best) continue;
+            if (c2 >= 0) {
+                ssp = wide_expand<K>(s, c2, lr, best, sub, ssp, overflow);
+                if (overflow) break;
+                continue;
+            }
+            const int2 lf = __ldg(&s.wide_leaves[-c2 - 1]);
+            for (int k = 0; k < lf.y; k++) {
+                const float t = intersect_t(load_prim(s, lf.x + k), lr, best);
+                if (t >= 0) {
+                    best = t;
+                    best_obj = lf.x + k;
+                    best_inst = inst;
                 }
             }
-        } else {
-            if (sp + 2 > kStackDepth) {
-                overflow = true;
-                break;
-            }
-            stack[sp++] = cur + 1;
-            stack[sp++] = __float_as_int(lo.w);
         }
+        if (overflow) break;
     }
     if (best_obj < 0) {
         h.t = kMax;
@@ -489,19 +505,14 @@ __device__ __forceinline__ bool closest_hit_t(const DeviceScene &s, f3 o, f3 d, 
     return true;
 }
 
-__device__ inline bool closest_hit(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow) {
-    LocalStack a, b;
-    return closest_hit_t<LocalStack &>(s, o, d, h, overflow, a, b);
-}
-
-// Scene::hit in shadow mode (scene.h:51-124 with occludedInstance/Object): for a
-// scene light, first intersect the light primitive itself (a miss counts as
-// occluded), then any primitive other than the light closer than it occludes.
-// For the background light (-1, -1), any hit occludes. On a visible light,
-// `light` holds the light's hit record for its emission lookup.
-template <class Stack>
-__device__ __forceinline__ bool occluded_t(const DeviceScene &s, f3 o, f3 d, int light_inst, int light_obj, Hit &light,
-                                           bool &overflow, Stack stack, Stack sub) {
+// Scene::hit in shadow mode (scene.h:51-124 with occludedInstance/Object) over the
+// wide BVH: for a scene light, first intersect the light primitive itself (a miss
+// counts as occluded), then any primitive other than the light closer than it
+// occludes. For the background light (-1, -1), any hit occludes. On a visible
+// light, `light` holds the light's hit record for its emission lookup.
+template <int K>
+__device__ __forceinline__ bool occluded_w(const DeviceScene &s, f3 o, f3 d, int light_inst, int light_obj, Hit &light,
+                                           bool &overflow, const WideStack &st, const WideStack &sub) {
     const Ray3 wr = make_ray(o, d);
     float best = kMax;
     if (light_inst != -1) {
@@ -517,63 +528,53 @@ __device__ __forceinline__ bool occluded_t(const DeviceScene &s, f3 o, f3 d, int
         best = t;
     }
     int sp = 0;
-    stack[sp++] = 0;
+    float te;
+    if (slab(__ldg(&s.nodes[0]), __ldg(&s.nodes[1]), wr, te)) st.put(sp++, __ldg(&s.wide_code[0]), te);
     while (sp > 0) {
-        const int cur = stack[--sp];
-        const float4 lo = __ldg(&s.nodes[2 * cur]), hi = __ldg(&s.nodes[2 * cur + 1]);
-        float te;
-        if (!slab(lo, hi, wr, te) || te > best) continue;
-        const int count = __float_as_int(hi.w);
-        if (count > 0) {
-            const int inst = __float_as_int(lo.w);
-            const InstanceRef ir = instance_ref(s, inst);
-            const int4 hd = ir.header();
-            const Ray3 lr = to_local(s, inst, ir, o, d);
-            int ssp = 0;
-            sub[ssp++] = hd.z;
-            while (ssp > 0) {
-                const int sc = sub[--ssp];
-                const float4 l2 = __ldg(&s.nodes[2 * sc]), h2 = __ldg(&s.nodes[2 * sc + 1]);
-                if (!slab(l2, h2, lr, te) || te > best) continue;
-                const int c2 = __float_as_int(h2.w);
-                if (c2 > 0) {
-                    const int first = __float_as_int(l2.w);
-                    for (int k = 0; k < c2; k++) {
-                        if (light_inst != -1 && inst == light_inst && first + k == light_obj) continue;
-                        if (intersect_t(load_prim(s, first + k), lr, best) >= 0) return true;
-                    }
-                } else {
-                    if (ssp + 2 > kStackDepth) {
-                        overflow = true;
-                        return true;
-                    }
-                    sub[ssp++] = sc + 1;
-                    sub[ssp++] = __float_as_int(l2.w);
-                }
+        --sp;
+        const int code = st.code[sp * st.stride];
+        if (st.te[sp * st.stride] > best) continue;
+        if (code >= 0) {
+            sp = wide_expand<K>(s, code, wr, best, st, sp, overflow);
+            if (overflow) return true;
+            continue;
+        }
+        const int inst = __ldg(&s.wide_leaves[-code - 1]).x;
+        const InstanceRef ir = instance_ref(s, inst);
+        const int root = ir.header().z;
+        const Ray3 lr = to_local(s, inst, ir, o, d);
+        if (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best) continue;
+        int ssp = 0;
+        sub.put(ssp++, __ldg(&s.wide_code[root]), te);
+        while (ssp > 0) {
+            --ssp;
+            const int c2 = sub.code[ssp * sub.stride];
+            if (sub.te[ssp * sub.stride] > best) continue;
+            if (c2 >= 0) {
+                ssp = wide_expand<K>(s, c2, lr, best, sub, ssp, overflow);
+                if (overflow) return true;
+                continue;
             }
-        } else {
-            if (sp + 2 > kStackDepth) {
-                overflow = true;
-                return true;
+            const int2 lf = __ldg(&s.wide_leaves[-c2 - 1]);
+            for (int k = 0; k < lf.y; k++) {
+                if (light_inst != -1 && inst == light_inst && lf.x + k == light_obj) continue;
+                if (intersect_t(load_prim(s, lf.x + k), lr, best) >= 0) return true;
             }
-            stack[sp++] = cur + 1;
-            stack[sp++] = __float_as_int(lo.w);
         }
     }
     return false;
 }
 
-__device__ inline bool occluded(const DeviceScene &s, f3 o, f3 d, int light_inst, int light_obj, Hit &light,
-                                bool &overflow) {
-    LocalStack a, b;
-    return occluded_t<LocalStack &>(s, o, d, light_inst, light_obj, light, overflow, a, b);
+// The two traversal stacks of this thread in dynamic shared memory: TLAS codes,
+// TLAS distances, BLAS codes, BLAS distances, each [cap][blockDim.x].
+__device__ __forceinline__ void wide_stacks(int *smem, const DeviceScene &s, WideStack &a, WideStack &b) {
+    const int B = blockDim.x, t = threadIdx.x, ca = s.stack_tlas, cb = s.stack_blas;
+    a = WideStack{smem + t, reinterpret_cast<float *>(smem + ca * B) + t, B, ca};
+    b = WideStack{smem + 2 * ca * B + t, reinterpret_cast<float *>(smem + 2 * ca * B + cb * B) + t, B, cb};
 }
 
-// Shared-memory stacks of one thread: 2 * kStackDepth ints per thread, entry-major.
-constexpr int kStackSmemPerThread = 2 * kStackDepth * 4;
-__device__ __forceinline__ void thread_stacks(int *smem, SharedStack &a, SharedStack &b) {
-    a = SharedStack{smem + threadIdx.x, int(blockDim.x)};
-    b = SharedStack{smem + kStackDepth * blockDim.x + threadIdx.x, int(blockDim.x)};
+__host__ __device__ inline size_t wide_stack_bytes(int block, int stack_tlas, int stack_blas) {
+    return size_t(block) * size_t(stack_tlas + stack_blas) * 8;
 }
 
 // ---------------------------------------------------------------------------

@@ -11,7 +11,12 @@ namespace lambda_dev {
 constexpr int kMaxFilmLayers = 8;  // thin-film layers handled by the FP32 transfer matrix
 
 struct DeviceScene {
-    const float4 *nodes;
+    const float4 *nodes;         // binary BVH (min, index) (max, count): root boxes
+    const float4 *wide;          // wide BVH child records, `width` per node (wide_bvh.h)
+    const int2 *wide_leaves;     // (index, count) of every binary leaf
+    const int *wide_code;        // per binary node: wide code of the tree roots
+    int bvh_width;               // children per wide node (2, 4 or 8)
+    int stack_tlas, stack_blas;  // traversal stack entries a ray can need
     const float4 *prims;
     const float4 *tri_attr;
     const float4 *instances;

@@ -21,6 +21,7 @@
 #include "lambda_gpu.h"
 #include "engine.h"
 #include "wavefront.cuh"
+#include "wide_bvh.h"
 
 #include "../host/tables.inc"
 
@@ -289,6 +290,18 @@ lambda_status validate_scene(lambda_ctx *ctx, const lambda_scene_desc &d) {
 
 }  // namespace
 
+DeviceScene lambda_ctx::scene_view(int width) const {
+    const int k = width == 2 ? 0 : (width == 4 ? 1 : 2);
+    DeviceScene v = dscene;
+    v.wide = scene.wide[k].as<float4>();
+    v.wide_leaves = scene.wide_leaves[k].as<int2>();
+    v.wide_code = scene.wide_code[k].as<int>();
+    v.bvh_width = 2 << k;
+    v.stack_tlas = wide_stack[k][0];
+    v.stack_blas = wide_stack[k][1];
+    return v;
+}
+
 extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene_desc *desc) {
     if (!ctx || !desc) return LAMBDA_ERR_INVALID_ARGUMENT;
     const lambda_scene_desc &d = *desc;
@@ -414,6 +427,17 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     CK(b.cie.upload(cie.data(), cie.size() * sizeof(float), s), "upload CIE table");
     CK(b.perm.upload(kPerlinPermutation, sizeof(kPerlinPermutation), s), "upload permutation");
     CK(b.worley.upload(worley.data(), worley.size() * sizeof(float4), s), "upload Worley lattice");
+    for (int k = 0; k < 3; k++) {
+        lambda_host::WideBvh w = lambda_host::build_wide_bvh(d.nodes, d.num_nodes, d.instances, d.num_instances, 2 << k);
+        w.records.resize(std::max<size_t>(w.records.size(), 8));
+        w.leaves.resize(std::max<size_t>(w.leaves.size(), 2));
+        CK(b.wide[k].upload(w.records.data(), w.records.size() * sizeof(float), s), "upload wide BVH");
+        CK(b.wide_leaves[k].upload(w.leaves.data(), w.leaves.size() * sizeof(int32_t), s), "upload wide BVH");
+        CK(b.wide_code[k].upload(w.code.data(), w.code.size() * sizeof(int32_t), s), "upload wide BVH");
+        CK(cudaStreamSynchronize(s), "upload wide BVH");  // the host vectors go out of scope
+        ctx->wide_stack[k][0] = w.stack_tlas;
+        ctx->wide_stack[k][1] = w.stack_blas;
+    }
     std::vector<uint32_t> iflags(d.num_instances, 0);
     for (int i = 0; i < d.num_instances; i++) {
         bool ident = true;
@@ -462,6 +486,7 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     ds.num_lights = d.num_lights;
     ds.total_light_power = d.total_light_power;
     ds.background_texture = d.background_texture;
+    ctx->dscene = ctx->scene_view(4);
     ctx->has_scene = true;
     ctx->film_layers_max = 0;
     for (int i = 0; i < d.num_materials; i++)
@@ -698,16 +723,36 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     rp.active = r.active.as<int>();
 
     const PathState ps = ctx->pstate;
-    const DeviceScene sc = ctx->dscene;
     const lambda_tuning &tu = ctx->tuning;
+    const DeviceScene sc = ctx->scene_view(tu.bvh_width);
     const int dev = ctx->device, sms = ctx->sm_count;
-    const int tb = tu.trace_block, sb = tu.shade_block, gs = tu.grid_scale;
-    const size_t stack_smem = size_t(tb) * kStackSmemPerThread;
+    const int tb = tu.trace_block, sb = tu.shade_block, gs = tu.grid_scale, bw = tu.bvh_width;
+    const size_t stack_smem = wide_stack_bytes(tb, sc.stack_tlas, sc.stack_blas);
+    const void *f_isect = bw == 2 ? (const void *)k_intersect<2> : bw == 4 ? (const void *)k_intersect<4>
+                                                                            : (const void *)k_intersect<8>;
+    const void *f_shadow = bw == 2 ? (const void *)k_shadow<2> : bw == 4 ? (const void *)k_shadow<4>
+                                                                         : (const void *)k_shadow<8>;
+    int smem_optin = 0;
+    CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
+    if (stack_smem > size_t(smem_optin))
+        return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "the scene's traversal stacks exceed shared memory at this block size");
+    CK(cudaFuncSetAttribute(f_isect, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)), "configure kernels");
+    CK(cudaFuncSetAttribute(f_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)), "configure kernels");
     auto grid = [&](const void *fn, int block, size_t smem) {
         return std::max(1, std::min((P + block - 1) / block, resident_ctas(fn, dev, block, smem) * sms * gs));
     };
-    const int g_isect = grid((const void *)k_intersect, tb, stack_smem);
-    const int g_shadow = grid((const void *)k_shadow, tb, stack_smem);
+    const int g_isect = grid(f_isect, tb, stack_smem);
+    const int g_shadow = grid(f_shadow, tb, stack_smem);
+    auto intersect = [&](int b) {
+        if (bw == 2) k_intersect<2><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
+        else if (bw == 4) k_intersect<4><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
+        else k_intersect<8><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
+    };
+    auto shadow = [&](int b) {
+        if (bw == 2) k_shadow<2><<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps);
+        else if (bw == 4) k_shadow<4><<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps);
+        else k_shadow<8><<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps);
+    };
     const int g_lambert = grid((const void *)k_shade_lambert, sb, 0);
     const int g_spec = grid((const void *)k_shade_specular, sb, 0);
     const int g_film = grid((const void *)k_shade_film_exact, sb, 0);
@@ -726,14 +771,14 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         timed(1, [&] { k_wave_prologue<<<1, 256, 0, stream>>>(d_max, ps, loop, waves, ctx->progress_dev); });
         timed(2, [&] { k_raygen<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
         for (int b = 0; b <= d_max; b++) {
-            timed(3, [&] { k_intersect<<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps); });
+            timed(3, [&] { intersect(b); });
             if (sc.families & 1u) timed(4, [&] { k_shade_lambert<<<g_lambert, sb, 0, stream>>>(b, rp, sc, ps); });
             if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<g_spec, sb, 0, stream>>>(b, rp, sc, ps); });
             if (sc.families & 4u) {
                 if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, pr);
                 else timed(6, [&] { k_shade_film_exact<<<g_film, sb, 0, stream>>>(b, rp, sc, ps); });
             }
-            if (sc.families & 1u) timed(7, [&] { k_shadow<<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps); });
+            if (sc.families & 1u) timed(7, [&] { shadow(b); });
         }
         return n;
     };
@@ -967,7 +1012,7 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
 bool tuning_ok(const lambda_tuning &t) {
     auto block_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
     return block_ok(t.trace_block) && block_ok(t.shade_block) && (t.grid_scale == 1 || t.grid_scale == 2) &&
-           t.max_pixels >= 0;
+           t.max_pixels >= 0 && (t.bvh_width == 2 || t.bvh_width == 4 || t.bvh_width == 8);
 }
 
 }  // namespace
@@ -998,14 +1043,16 @@ extern "C" lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning 
     return LAMBDA_OK;
 }
 
-// Times the probe render (its output stays in device memory) under every candidate
-// launch shape, after one warm-up render per candidate, and keeps the fastest. The
+// Times the probe render (its output stays in device memory): first the three BVH
+// widths, then every block-shape candidate at the fastest width, each after one
+// warm-up render, and keeps the fastest. The
 // path-state capacity is set from free device memory: half of it, at the bytes of
 // path state and queues a pixel needs.
 extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out) {
     if (!ctx || !probe) return LAMBDA_ERR_INVALID_ARGUMENT;
     lambda_status s = check_settings(ctx, probe->settings);
     if (s != LAMBDA_OK) return s;
+    if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const size_t P = size_t(probe->settings.width) * probe->settings.height;
     DeviceBuffer img;
@@ -1015,19 +1062,41 @@ extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_de
     const lambda_tuning keep = ctx->tuning;
     lambda_tuning best = keep;
     double best_ms = 1e300;
+    // the BVH width first, at the current block shapes, then the block shapes at that width
+    auto trial = [&](const lambda_tuning &t, double &ms) -> lambda_status {
+        ctx->tuning = t;
+        lambda_status r = LAMBDA_OK;
+        for (int rep = 0; rep < 2 && r == LAMBDA_OK; rep++) {
+            r = render_jobs(ctx, &job, 1, nullptr);
+            ms = ctx->stats.render_ms;
+        }
+        return r;
+    };
+    for (int bw : {2, 4, 8}) {
+        double ms = 0;
+        const lambda_status r = trial(lambda_tuning{keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, bw}, ms);
+        if (r == LAMBDA_ERR_UNSUPPORTED) continue;  // stacks too deep for shared memory at this block size
+        if (r != LAMBDA_OK) {
+            ctx->tuning = keep;
+            img.release();
+            return r;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = ctx->tuning;
+        }
+    }
+    const int width = best.bvh_width;
     for (int tb : {64, 128, 256})
         for (int sb : {64, 128, 256})
             for (int gs : {1, 2}) {
-                ctx->tuning = lambda_tuning{tb, sb, gs, keep.max_pixels};
                 double ms = 0;
-                for (int rep = 0; rep < 2 && s == LAMBDA_OK; rep++) {
-                    s = render_jobs(ctx, &job, 1, nullptr);
-                    ms = ctx->stats.render_ms;
-                }
-                if (s != LAMBDA_OK) {
+                const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, width}, ms);
+                if (r == LAMBDA_ERR_UNSUPPORTED) continue;
+                if (r != LAMBDA_OK) {
                     ctx->tuning = keep;
                     img.release();
-                    return s;
+                    return r;
                 }
                 if (ms < best_ms) {
                     best_ms = ms;
@@ -1063,28 +1132,52 @@ extern "C" lambda_status lambda_get_render_stats(const lambda_ctx *ctx, lambda_r
 
 namespace {
 
+template <int K>
 __global__ void k_trace_closest(DeviceScene sc, const float *rays, int n, int *inst, int *obj, float *t, int *error) {
+    extern __shared__ int stack_smem[];
+    WideStack st_a, st_b;
+    wide_stacks(stack_smem, sc, st_a, st_b);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float *r = rays + 6 * size_t(k);
     Hit h;
     bool overflow = false;
-    closest_hit(sc, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), h, overflow);
+    closest_hit_w<K>(sc, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), h, overflow, st_a, st_b);
     inst[k] = h.instance;
     obj[k] = h.object;
     t[k] = h.t;
     if (overflow) atomicOr(error, 1);
 }
 
+template <int K>
 __global__ void k_trace_shadow(DeviceScene sc, const float *rays, const int *li, const int *lo, int n, int *occ,
                                int *error) {
+    extern __shared__ int stack_smem[];
+    WideStack st_a, st_b;
+    wide_stacks(stack_smem, sc, st_a, st_b);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float *r = rays + 6 * size_t(k);
     Hit h;
     bool overflow = false;
-    occ[k] = occluded(sc, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), li[k], lo[k], h, overflow) ? 1 : 0;
+    occ[k] = occluded_w<K>(sc, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), li[k], lo[k], h, overflow, st_a, st_b) ? 1 : 0;
     if (overflow) atomicOr(error, 1);
+}
+
+// Launches a ray-query kernel of the tuned BVH width with its stacks in shared memory.
+template <class F2, class F4, class F8, class... A>
+cudaError_t launch_query(lambda_ctx *ctx, F2 f2, F4 f4, F8 f8, int n, A... args) {
+    const DeviceScene sc = ctx->scene_view(ctx->tuning.bvh_width);
+    const size_t smem = wide_stack_bytes(128, sc.stack_tlas, sc.stack_blas);
+    const int w = sc.bvh_width;
+    const void *fn = w == 2 ? (const void *)f2 : w == 4 ? (const void *)f4 : (const void *)f8;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    const int blocks = (n + 127) / 128;
+    if (w == 2) f2<<<blocks, 128, smem, ctx->stream>>>(sc, args...);
+    else if (w == 4) f4<<<blocks, 128, smem, ctx->stream>>>(sc, args...);
+    else f8<<<blocks, 128, smem, ctx->stream>>>(sc, args...);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -1114,7 +1207,9 @@ extern "C" lambda_status lambda_trace_closest(lambda_ctx *ctx, const float *rays
     CK(ctx->rbuf.error.reserve(16), "allocate flags");
     int *err = ctx->rbuf.error.as<int>();
     CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
-    k_trace_closest<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->dscene, dr, n, di, dobj, dt, err);
+    CK(launch_query(ctx, k_trace_closest<2>, k_trace_closest<4>, k_trace_closest<8>, n, static_cast<const float *>(dr), n,
+                    di, dobj, dt, err),
+       "launch closest-hit queries");
     CK(cudaGetLastError(), "launch trace");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");
@@ -1154,7 +1249,9 @@ extern "C" lambda_status lambda_trace_shadow(lambda_ctx *ctx, const float *rays,
     CK(ctx->rbuf.error.reserve(16), "allocate flags");
     int *err = ctx->rbuf.error.as<int>();
     CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
-    k_trace_shadow<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->dscene, dr, dli, dlo, n, docc, err);
+    CK(launch_query(ctx, k_trace_shadow<2>, k_trace_shadow<4>, k_trace_shadow<8>, n, static_cast<const float *>(dr),
+                    static_cast<const int *>(dli), static_cast<const int *>(dlo), n, docc, err),
+       "launch shadow queries");
     CK(cudaGetLastError(), "launch trace");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");

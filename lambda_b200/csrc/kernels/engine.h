@@ -46,6 +46,7 @@ struct SceneBuffers {
     DeviceBuffer nodes, prims, tri, instances, spectra, spectrum_flat, cspectra, cspectrum_flat, materials,
         material_props, scalar_tex, spectrum_tex, light_inst, light_obj, light_power, light_cdf, material_emission,
         cie, perm, worley, instance_flags;
+    DeviceBuffer wide[3], wide_leaves[3], wide_code[3];  // wide BVH of width 2, 4, 8
 };
 
 struct RenderBuffers {
@@ -69,13 +70,14 @@ struct lambda_ctx {
     int film_layers_max = 0;
     SceneBuffers scene;
     lambda_dev::DeviceScene dscene{};
+    int wide_stack[3][2] = {};  // traversal stack entries (TLAS, BLAS) of the width 2, 4, 8 trees
 
     RenderBuffers rbuf;
     lambda_dev::PathState pstate{};
     cudaGraphExec_t graph_exec = nullptr;
     lambda_render_stats stats{};
     lambda_stage_time stage_times[LAMBDA_NUM_STAGES]{};
-    lambda_tuning tuning{256, 256, 1, 0};  // launch shapes (max_pixels 0: no limit)
+    lambda_tuning tuning{256, 256, 1, 0, 4};  // launch shapes (max_pixels 0: no limit)
     int *progress_host = nullptr;           // waves started by the running pass graph (mapped host memory)
     int *progress_dev = nullptr;            // its device address
 
@@ -87,6 +89,8 @@ struct lambda_ctx {
 
     ~lambda_ctx();
 
+    // The scene as the kernels see it with the wide BVH of the given width (2, 4 or 8).
+    lambda_dev::DeviceScene scene_view(int width) const;
     lambda_status fail(lambda_status s, const std::string &msg);
     lambda_status cuda_fail(cudaError_t e, const char *what);
     lambda_status ensure_state(int pixels, int depth);
@@ -101,6 +105,8 @@ struct lambda_ctx {
         return {&s.nodes, &s.prims, &s.tri, &s.instances, &s.spectra, &s.spectrum_flat, &s.cspectra,
                 &s.cspectrum_flat, &s.materials, &s.material_props, &s.scalar_tex, &s.spectrum_tex, &s.light_inst,
                 &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley, &s.instance_flags,
+                &s.wide[0], &s.wide[1], &s.wide[2], &s.wide_leaves[0], &s.wide_leaves[1], &s.wide_leaves[2],
+                &s.wide_code[0], &s.wide_code[1], &s.wide_code[2],
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
                 &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
                 &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &sbuf.weights_bf16, &sbuf.weights_f32};

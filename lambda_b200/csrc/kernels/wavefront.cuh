@@ -159,10 +159,11 @@ __device__ __forceinline__ int material_of(const DeviceScene &sc, int inst_mater
 
 // Closest hit; misses and emitter hits add their radiance and end the path
 // (renderer.h:105-131); other hits go to their material's queue.
+template <int K>
 LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
     extern __shared__ int stack_smem[];
-    SharedStack st_a, st_b;
-    thread_stacks(stack_smem, st_a, st_b);
+    WideStack st_a, st_b;
+    wide_stacks(stack_smem, sc, st_a, st_b);
     const int n = ps.counts[queue_slot(bounce, kQActive)];
     const int *q = ps.queue[bounce & 1];
     const int stride = gridDim.x * blockDim.x;
@@ -175,7 +176,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParam
             const f3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
             Hit h;
             bool overflow = false;
-            const bool hit = closest_hit_t(sc, o, d, h, overflow, st_a, st_b);
+            const bool hit = closest_hit_w<K>(sc, o, d, h, overflow, st_a, st_b);
             if (overflow) atomicOr(ps.error, 1);
             const bool specular = d4.w != 0.0f;
             const float prev_pdf = o4.w;
@@ -503,10 +504,11 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, Rend
     }
 }
 
+template <int K>
 LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
     extern __shared__ int stack_smem[];
-    SharedStack st_a, st_b;
-    thread_stacks(stack_smem, st_a, st_b);
+    WideStack st_a, st_b;
+    wide_stacks(stack_smem, sc, st_a, st_b);
     const int n = ps.counts[queue_slot(bounce, kQShadow)];
     const int stride = gridDim.x * blockDim.x;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
@@ -516,7 +518,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams r
         const f3 d = mk(dd.x, dd.y, dd.z);
         Hit lh;
         bool overflow = false;
-        if (!occluded_t(sc, mk(o.x, o.y, o.z), d, light.x, light.y, lh, overflow, st_a, st_b)) {
+        if (!occluded_w<K>(sc, mk(o.x, o.y, o.z), d, light.x, light.y, lh, overflow, st_a, st_b)) {
             const s4 lam = from_f4(ps.lam[p]);
             s4 e;
             if (light.x != -1) {
