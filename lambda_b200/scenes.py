@@ -37,6 +37,7 @@ __all__ = [
     "perlin_sphere",
     "look_at_camera",
     "random_pose_jobs",
+    "instanced_meshes",
 ]
 
 
@@ -306,6 +307,87 @@ def perlin_sphere(directory: str, width: int = 1024, height: int = 1024, spp: in
         "Material body lambertian tiles",
         f"Object mesh mesh body {obj}",
         "Instance mesh default (0 0 0) (0 0 0) (1 1 1)",
+        "Background equirectangular sky",
+        f"Camera {_v(pos)} {_v(corner)} {_v(hor)} {_v(ver)}",
+    ]
+    _write(path, lines)
+    return SceneFiles(path, seed, width, height, spp, depth)
+
+
+# --------------------------------------------------------------------------
+# Large instanced scene
+# --------------------------------------------------------------------------
+
+def write_latlong_sphere_obj(path: str, segments: int = 250, rings: int = 201, amplitude: float = 0.1,
+                             frequency: float = 4.0, seed: int = 5) -> int:
+    """A latitude-longitude sphere of 2 * segments * (rings - 1) triangles (fans at
+    the poles, two triangles per quad between), radially displaced by Perlin noise
+    like the mesh of perlin_sphere; 250 x 201 gives exactly 100,000 triangles.
+    Returns the triangle count."""
+    th = np.linspace(0.0, math.pi, rings + 1)[1:-1]                 # interior latitudes
+    ph = np.linspace(0.0, 2 * math.pi, segments, endpoint=False)
+    st, ct = np.sin(th)[:, None], np.cos(th)[:, None]
+    ring = np.stack([st * np.cos(ph), np.broadcast_to(ct, (len(th), segments)), st * np.sin(ph)], -1).reshape(-1, 3)
+    v = np.concatenate([[[0.0, 1.0, 0.0]], ring, [[0.0, -1.0, 0.0]]])
+    top, bottom = 0, len(v) - 1
+    idx = lambda r, k: 1 + r * segments + (k % segments)  # noqa: E731
+    tris = []
+    for k in range(segments):
+        tris.append((top, idx(0, k + 1), idx(0, k)))
+        tris.append((bottom, idx(rings - 2, k), idx(rings - 2, k + 1)))
+    for r in range(rings - 2):
+        for k in range(segments):
+            a, b, c, d = idx(r, k), idx(r, k + 1), idx(r + 1, k), idx(r + 1, k + 1)
+            tris.append((a, b, d))
+            tris.append((a, d, c))
+    tris = np.asarray(tris, dtype=np.int64)
+    offset = np.random.default_rng(seed).uniform(0, 64, size=3)
+    n = perlin_noise_np(v * frequency + offset)
+    v = v * (1.0 + amplitude * (2.0 * n - 1.0))[:, None]
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        f.write(f"# {len(tris)} triangles: lat-long sphere {segments}x{rings}, Perlin amplitude {amplitude}\n")
+        np.savetxt(f, v, fmt="v %.7g %.7g %.7g")
+        np.savetxt(f, tris + 1, fmt="f %d %d %d")
+    return len(tris)
+
+
+def instanced_meshes(directory: str, width: int = 3840, height: int = 2160, spp: int = 1024, depth: int = 32,
+                     instances: int = 10000, segments: int = 250, rings: int = 201, box: float = 100.0,
+                     seed: int = 5, name: str = "instanced.lrd") -> SceneFiles:
+    """`instances` copies of one Perlin-displaced mesh (write_latlong_sphere_obj;
+    the defaults give 100,000 triangles and 10,000 instances) with a random
+    translation in a box^3 cube, random rotation and uniform scale 0.5-2 (`seed`).
+    Materials are set per instance (the Instance material override): 40 % thin film
+    [1 1.33 1.5] with Worley thickness 200-800 nm, 30 % dielectric 1.0/1.5, 30 %
+    Lambertian checker 0.8/0.2. A Perlin equirectangular sky is the only light. The
+    camera stands outside the cube looking at its centre."""
+    obj = os.path.join(directory, f"latlong_{segments}x{rings}.obj")
+    if not os.path.exists(obj):
+        write_latlong_sphere_obj(obj, segments, rings, seed=seed)
+    rng = np.random.default_rng(seed)
+    path = os.path.join(directory, name)
+    pos, corner, hor, ver = look_at_camera((0.0, 0.35 * box, -1.6 * box), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 45.0,
+                                           width / height)
+    lines = [
+        "# instanced Perlin-displaced meshes under a Perlin sky",
+        f"Render {width} {height} {depth} {spp} 380 780",
+        "Texture sky scalar perlin 0.2 1.0 1",
+        "Texture thickness scalar worley 200 800 3",
+        "Texture tiles spectrum checker 0.8 0.2 10",
+        "Material film thinfilm [1 1.33 1.5] [thickness]",
+        "Material glass dielectric 1.0 1.5",
+        "Material tiled lambertian tiles",
+        f"Object mesh mesh tiled {obj}",
+    ]
+    u = rng.uniform(0, 1, instances)
+    mats = np.where(u < 0.4, "film", np.where(u < 0.7, "glass", "tiled"))
+    t = rng.uniform(-box / 2, box / 2, (instances, 3))
+    r = rng.uniform(0, 2 * math.pi, (instances, 3))
+    sc = rng.uniform(0.5, 2.0, instances)
+    for i in range(instances):
+        lines.append(f"Instance mesh {mats[i]} {_v(t[i])} {_v(r[i])} ({_f(sc[i])} {_f(sc[i])} {_f(sc[i])})")
+    lines += [
         "Background equirectangular sky",
         f"Camera {_v(pos)} {_v(corner)} {_v(hor)} {_v(ver)}",
     ]

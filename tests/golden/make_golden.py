@@ -84,6 +84,8 @@ def scene_files():
             "thinfilm": scenes.thinfilm_spheres(".", 32, 18, 4, name="thinfilm.lrd"),
             "thinfilm_deep": scenes.thinfilm_spheres(".", 24, 14, 9, depth=24, name="thinfilm_deep.lrd"),
             "mesh": scenes.perlin_sphere(".", 24, 24, 4, levels=4, name="mesh.lrd"),
+            "instanced": scenes.instanced_meshes(".", 24, 16, 4, depth=6, instances=40, segments=12, rings=7,
+                                                 box=10.0, name="instanced.lrd"),
         }
     finally:
         os.chdir(cwd)

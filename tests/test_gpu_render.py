@@ -19,6 +19,8 @@ CASES = {
     "thinfilm": lambda d: scenes.thinfilm_spheres(d, 96, 54, 16, name="r_thinfilm.lrd"),
     "thinfilm_deep": lambda d: scenes.thinfilm_spheres(d, 64, 36, 4, depth=24, name="r_thinfilm_deep.lrd"),
     "mesh": lambda d: scenes.perlin_sphere(d, 48, 48, 4, levels=5, name="r_mesh.lrd"),
+    "instanced": lambda d: scenes.instanced_meshes(d, 64, 40, 9, depth=8, instances=120, segments=16, rings=9,
+                                                   box=14.0, name="r_instanced.lrd"),
 }
 
 

@@ -93,6 +93,46 @@ def test_trained_weights_accuracy(ctx):
     assert e.mean() < 3e-3 and np.quantile(e, 0.99) < 2e-2
 
 
+def _bare_substrate_r(q):
+    """(R_s + R_p) / 2 of air over the bare substrate (Fresnel, no film): what a
+    renderer without a thin-film model would use."""
+    c0 = q[:, 1].astype(np.float64)
+    ns = q[:, 4].astype(np.float64)
+    ct = np.sqrt(np.maximum(1 - (1 - c0 * c0) / (ns * ns), 0))
+    rs = ((c0 - ns * ct) / (c0 + ns * ct)) ** 2
+    rp = ((ns * c0 - ct) / (ns * c0 + ct)) ** 2
+    return (rs + rp) / 2
+
+
+def test_trained_network_gain(ctx):
+    """What training buys: the shipped network's error on R against the FP64
+    transfer matrix, beside (a) the same network untrained (its initial weights)
+    and (b) dropping the film (bare-substrate Fresnel), the model a renderer
+    without the thin-film term would use."""
+    rng = np.random.default_rng(8)
+    n = 100000
+    q = np.stack([rng.uniform(380, 780, n), rng.uniform(0.05, 1, n), rng.uniform(150, 850, n),
+                  rng.uniform(1.2, 1.8, n), rng.uniform(1.0, 2.0, n)], 1).astype(np.float32)
+    fp64 = ctx.thinfilm_fp64(q)
+    want = (fp64[:, 0] + fp64[:, 1]) / 2
+
+    def err(out):
+        return float(np.abs((out[:, 0] + out[:, 1]) / 2 - want).mean())
+
+    surrogate.install(ctx)
+    trained = err(ctx.surrogate_eval(q))
+    # untrained: the initialisation the training kernels start from (one epoch at a
+    # learning rate of 1e-12 leaves it in place)
+    rep = ctx.surrogate_train(samples=1 << 16, epochs=1, batch=8192, lr=1e-12, seed=11)
+    untrained = err(ctx.surrogate_eval(q))
+    bare = float(np.abs(_bare_substrate_r(q) - want).mean())
+    surrogate.install(ctx)
+    print(f"mean |R - R_fp64|: trained {trained:.2e}, untrained {untrained:.2e}, no film {bare:.2e}; "
+          f"untrained audit {rep.mean_abs_error:.2e}")
+    assert trained < 0.1 * bare
+    assert trained < 0.05 * untrained
+
+
 def test_surrogate_render_unbiased(scene_dir, ctx):
     """A noisy render differs from the exact form's by no more than a second exact
     render (another seed) does, plus 1%; the image means agree within 2%."""

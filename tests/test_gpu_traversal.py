@@ -15,6 +15,8 @@ SCENES = {
     "cornell": lambda d: scenes.cornell(d, 32, 32, 4),
     "thinfilm": lambda d: scenes.thinfilm_spheres(d, 64, 36, 4),
     "mesh": lambda d: scenes.perlin_sphere(d, 64, 64, 4, levels=5),
+    "instanced": lambda d: scenes.instanced_meshes(d, 64, 40, 4, depth=8, instances=300, segments=24, rings=13,
+                                                   box=20.0, name="t_instanced.lrd"),
 }
 
 

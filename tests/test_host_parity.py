@@ -12,7 +12,7 @@ from oracle import ref
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 SCN = os.path.join(GOLDEN, "scenes")
-NAMES = ["cornell", "thinfilm", "thinfilm_deep", "mesh"]
+NAMES = ["cornell", "thinfilm", "thinfilm_deep", "mesh", "instanced"]
 
 
 @pytest.fixture(scope="module")
