@@ -513,6 +513,7 @@ def main():
             "clocks": clocks.summary(),
             "roofline": roof,
             "stages": stage,
+            "stage_rooflines": lb.stage_rooflines(stage, hbm, tf),
             "segments_per_path": stats[-1].segments / stats[-1].paths,
             "thinfilm": {"hits_per_step": stats[-1].thinfilm_hits,
                          "surrogate_exact_fallback_per_step": stats[-1].thinfilm_fallback},

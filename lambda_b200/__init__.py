@@ -406,6 +406,23 @@ def stage_profile(ctx: "Context", desc, out) -> dict:
     return st
 
 
+def stage_rooflines(stages: dict, hbm_gbs: float, bf16_tflops: float) -> dict:
+    """Every timed stage as a fraction of its roofline: algorithmic bytes (STAGE_BYTES
+    per item) over its device time against the measured HBM bandwidth, and for the
+    surrogate stage MLP FLOPs against the measured BF16 tensor peak."""
+    out = {}
+    for name, s in stages.items():
+        if s["ms"] <= 0 or not s["items"]:
+            continue
+        if name == "film_surrogate":
+            tf = 17536.0 * s["items"] * 4 / (s["ms"] / 1000.0) / 1e12
+            out[name] = {"bound": "tensor", "achieved_tflops": tf, "frac": tf / bf16_tflops}
+        elif name in STAGE_BYTES:
+            gbs = STAGE_BYTES[name] * s["items"] / (s["ms"] / 1000.0) / 1e9
+            out[name] = {"bound": "hbm", "achieved_gbs": gbs, "frac": gbs / hbm_gbs}
+    return out
+
+
 def roofline(stages: dict, hbm_gbs: float, bf16_tflops: float, peak_kind: str) -> dict:
     """Roofline entry for the stage with the largest device time."""
     name, s = max(((k, v) for k, v in stages.items() if v["ms"] > 0), key=lambda kv: kv[1]["ms"])

@@ -16,6 +16,7 @@
 #include <cmath>
 #include <map>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "hmath.h"
@@ -142,6 +143,23 @@ ItemBounds object_bounds(const lambda_object &o) {
 
 float half_area(const V3 &e) { return 2 * (e[0] * e[1] + e[0] * e[2] + e[1] * e[2]); }
 
+// Runs fn(i) for i in [0, n) on all host threads, in contiguous blocks. Each i is
+// computed by one thread alone, so results do not depend on the thread count.
+template <class F>
+void parallel_for(size_t n, F fn) {
+    const size_t threads = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), std::max<size_t>(n / 64, 1));
+    if (threads <= 1) {
+        for (size_t i = 0; i < n; i++) fn(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < threads; t++)
+        pool.emplace_back([&, t] {
+            for (size_t i = n * t / threads; i < n * (t + 1) / threads; i++) fn(i);
+        });
+    for (auto &th : pool) th.join();
+}
+
 // One recursive binned-SAH build over order[start, end) (bvh.h:111-246). Returns
 // the node index of the subtree root.
 int build_range(const std::vector<ItemBounds> &items, std::vector<int> &order, int start, int end,
@@ -255,8 +273,10 @@ void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
     s.nodes.reserve(2 * s.objects.size());
 
     // TLAS over instances
+    // An instance's bounds visit all its objects (O(instances x objects)); instances
+    // are independent, so they run on all host threads.
     std::vector<ItemBounds> inst_bounds(s.instances.size());
-    for (size_t i = 0; i < s.instances.size(); i++) inst_bounds[i] = instance_bounds(s, s.instances[i]);
+    parallel_for(s.instances.size(), [&](size_t i) { inst_bounds[i] = instance_bounds(s, s.instances[i]); });
     std::vector<int> order(s.instances.size());
     std::iota(order.begin(), order.end(), 0);
     build_range(inst_bounds, order, 0, int(s.instances.size()), s.nodes, 1);
@@ -289,15 +309,46 @@ void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
 void build_lights(HostScene &s) {
     V3 scene_center = v3(0, 0, 0);
     float scene_radius = 0;
+    // The merge below is sequential in instance and object order. The transformed
+    // centres and radii it consumes are not, so they are computed ahead on all host
+    // threads, a block of instances at a time (at most about 8M objects per block).
+    struct Sphere {
+        V3 c;
+        float r;
+    };
+    std::vector<Sphere> pre;
+    std::vector<size_t> offset;
+    int block_end = 0;
+    size_t block_base = 0;
     for (int i = 0; i < int(s.instances.size()); i++) {
+        if (i == block_end) {
+            size_t total = 0;
+            offset.clear();
+            block_end = i;
+            while (block_end < int(s.instances.size()) && (total == 0 || total + s.instances[block_end].count <= (size_t(1) << 23))) {
+                offset.push_back(total);
+                total += size_t(s.instances[block_end].count);
+                block_end++;
+            }
+            block_base = size_t(i);
+            pre.resize(total);
+            parallel_for(size_t(block_end - i), [&](size_t k) {
+                const lambda_instance &in = s.instances[block_base + k];
+                const float scale = length(col0(in));
+                for (int j = 0; j < in.count; j++) {
+                    ObjectGeom g{s.objects[in.object + j]};
+                    pre[offset[k] + j] = Sphere{transform(in.transform, g.center(), 1), g.bounding_radius() * scale};
+                }
+            });
+        }
         const lambda_instance &in = s.instances[i];
-        const float scale = length(col0(in));
         const float scale_sq = length_sq(col0(in));
+        const Sphere *sph = &pre[offset[size_t(i) - block_base]];
         for (int j = 0; j < in.count; j++) {
             const int object_index = in.object + j;
             ObjectGeom g{s.objects[object_index]};
-            const V3 object_center = transform(in.transform, g.center(), 1);
-            const float object_radius = g.bounding_radius() * scale;
+            const V3 object_center = sph[j].c;
+            const float object_radius = sph[j].r;
             const V3 to_object = object_center - scene_center;
             const float distance = length(to_object);
             if (distance + scene_radius <= object_radius) {
