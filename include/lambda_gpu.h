@@ -211,6 +211,14 @@ void lambda_host_scene_destroy(lambda_host_scene *scene);
 lambda_status lambda_write_ppm(const char *path, int32_t width, int32_t height, const float *rgb,
                                char *err, size_t err_len);
 
+/* Binary float output beside the reference's 8-bit text PPM (no counterpart in the
+ * reference): a little-endian PFM ("PF", scale -1.0, rows bottom to top) of the
+ * unclamped linear sRGB image, or with xyz != 0 of linear CIE XYZ (the inverse of
+ * the XYZ -> sRGB matrix of utils.h:230, in double), the space image error is
+ * measured in. The path must end in ".pfm". */
+lambda_status lambda_write_pfm(const char *path, int32_t width, int32_t height, const float *rgb, int32_t xyz,
+                               char *err, size_t err_len);
+
 /* ---------------------------------------------------------------------------
  * GPU context.
  * ------------------------------------------------------------------------- */

@@ -30,6 +30,7 @@ __all__ = [
     "Context",
     "LambdaError",
     "write_ppm",
+    "write_pfm",
     "RENDER_THINFILM_EXACT",
     "RENDER_THINFILM_SURROGATE",
     "RENDER_OUTPUT_DEVICE",
@@ -165,6 +166,17 @@ def write_ppm(path: str, rgb: np.ndarray) -> None:
     h, w = rgb.shape[:2]
     err = C.create_string_buffer(1024)
     st = lib.lambda_write_ppm(path.encode(), w, h, rgb.ctypes.data, err, len(err))
+    if st != 0:
+        raise LambdaError(st, err.value.decode())
+
+
+def write_pfm(path: str, rgb: np.ndarray, xyz: bool = False) -> None:
+    """Float image to a little-endian PFM: linear sRGB, or linear CIE XYZ."""
+    lib = N.load()
+    rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+    h, w = rgb.shape[:2]
+    err = C.create_string_buffer(1024)
+    st = lib.lambda_write_pfm(path.encode(), w, h, rgb.ctypes.data, 1 if xyz else 0, err, len(err))
     if st != 0:
         raise LambdaError(st, err.value.decode())
 

@@ -152,6 +152,7 @@ _SIGNATURES = {
     "lambda_host_scene_get": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(RenderSettings)]),
     "lambda_host_scene_destroy": (None, [_P]),
     "lambda_write_ppm": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _P, C.c_char_p, C.c_size_t]),
+    "lambda_write_pfm": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _P, C.c_int32, C.c_char_p, C.c_size_t]),
     "lambda_ctx_create": (C.c_int, [C.c_int32, C.POINTER(_P)]),
     "lambda_ctx_destroy": (None, [_P]),
     "lambda_last_error": (C.c_char_p, [_P]),

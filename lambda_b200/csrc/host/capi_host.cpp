@@ -78,3 +78,22 @@ extern "C" lambda_status lambda_write_ppm(const char *path, int32_t width, int32
     put_error(err, err_len, "");
     return LAMBDA_OK;
 }
+
+extern "C" lambda_status lambda_write_pfm(const char *path, int32_t width, int32_t height, const float *rgb,
+                                          int32_t xyz, char *err, size_t err_len) {
+    if (!path || !rgb || width <= 0 || height <= 0) {
+        put_error(err, err_len, "lambda_write_pfm: invalid argument");
+        return LAMBDA_ERR_INVALID_ARGUMENT;
+    }
+    try {
+        lambda_host::write_pfm(path, width, height, rgb, xyz != 0);
+    } catch (const lambda_host::SceneError &e) {
+        put_error(err, err_len, e.what());
+        return e.status;
+    } catch (const std::exception &e) {
+        put_error(err, err_len, e.what());
+        return LAMBDA_ERR_INTERNAL;
+    }
+    put_error(err, err_len, "");
+    return LAMBDA_OK;
+}

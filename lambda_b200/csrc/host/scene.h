@@ -54,6 +54,7 @@ void build_lights(HostScene &scene);
 
 // Writer::write (writer.h:11-41): throws SceneError with the reference's text.
 void write_ppm(const std::string &path, int width, int height, const float *rgb);
+void write_pfm(const std::string &path, int width, int height, const float *rgb, bool xyz);
 
 // Scalar/spectrum texture and spectrum statistics used while parsing.
 float spectrum_average(const HostScene &s, int spectrum);

@@ -77,3 +77,31 @@ def test_cli_argument_errors(tmp_path):
     bad.write_text("Camera (0 0 0) (0 0 0) (1 0 0) (0 1 0)\n")
     r = subprocess.run([exe, str(bad)], capture_output=True, text=True)
     assert r.returncode == 1 and r.stderr.strip() == f'{bad}:1: expected "Render", got "Camera"'
+
+
+def test_write_pfm_round_trip(tmp_path):
+    """Binary float output: rows bottom-up, values bit-exact; the XYZ variant equals
+    the linear-sRGB -> XYZ conversion the image metric uses."""
+    import numpy as np
+
+    import lambda_b200 as lb
+    from tests.helpers import to_xyz
+
+    rng = np.random.default_rng(3)
+    img = rng.uniform(-0.5, 3.0, (7, 11, 3)).astype(np.float32)
+
+    def read(p):
+        with open(p, "rb") as f:
+            assert f.readline() == b"PF\n"
+            w, h = map(int, f.readline().split())
+            assert float(f.readline()) == -1.0
+            data = np.frombuffer(f.read(), dtype="<f4").reshape(h, w, 3)
+        return data[::-1]
+
+    lb.write_pfm(str(tmp_path / "a.pfm"), img)
+    assert np.array_equal(read(tmp_path / "a.pfm").view(np.uint32), img.view(np.uint32))
+    lb.write_pfm(str(tmp_path / "b.pfm"), img, xyz=True)
+    want = to_xyz(img).reshape(img.shape).astype(np.float32)
+    assert np.allclose(read(tmp_path / "b.pfm"), want, rtol=1e-6, atol=1e-6)
+    with pytest.raises(lb.LambdaError):
+        lb.write_pfm(str(tmp_path / "c.ppm"), img)
