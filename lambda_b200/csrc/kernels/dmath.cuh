@@ -38,6 +38,10 @@ __device__ __forceinline__ f3 cross(f3 a, f3 b) {
 }
 __device__ __forceinline__ float length_sq(f3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
 __device__ __forceinline__ float length(f3 a) { return sqrtf(length_sq(a)); }
+// 1 / x rounded to nearest: the same correctly rounded value as the IEEE division
+// 1.0f / x, without the division routine.
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+
 __device__ __forceinline__ f3 normalize(f3 a) {
     const float l = length(a);
     return mk(a.x / l, a.y / l, a.z / l);

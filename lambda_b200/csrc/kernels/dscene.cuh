@@ -121,20 +121,30 @@ __device__ __forceinline__ f3 worley_feature(const DeviceScene &s, int cx, int c
               fract(float(sin(double(d))) * 43758.5453f));
 }
 
-// F1 Worley distance over the 27 neighbouring cells (utils.h:154-171). The
-// minimum does not depend on visit order, so cells are visited nearest first and
-// a cell is skipped when every point of its box [c, c+1]^3 (where its feature
-// lies) is farther than the best distance so far, with a relative margin that
-// covers float rounding: the result equals the full 27-cell minimum.
+// F1 Worley distance over the 27 neighbouring cells (utils.h:154-171). Results
+// equal the reference's:
+// - The minimum does not depend on visit order, so cells are visited nearest
+//   first. A cell is skipped when every point of its box [c, c+1]^3 (where its
+//   feature lies) is farther than the best so far, with a relative margin that
+//   covers float rounding.
+// - sqrtf is correctly rounded and monotone, so the minimum of the distances is
+//   the square root of the minimum squared distance: one sqrtf at the end.
+// - When the whole 3x3x3 neighbourhood lies inside the host-built feature table,
+//   cells are read from it at offsets from one base, without per-cell range checks.
 // Neighbour offsets ordered by |xo| + |yo| + |zo|, packed as (xo+1) | (yo+1) << 2 | (zo+1) << 4.
-__constant__ unsigned char kWorleyOrder[27] = {
-    0x15, 0x14, 0x16, 0x11, 0x19, 0x05, 0x25, 0x10, 0x18, 0x12, 0x1a, 0x04, 0x24, 0x06,
-    0x26, 0x01, 0x21, 0x09, 0x29, 0x00, 0x20, 0x08, 0x28, 0x02, 0x22, 0x0a, 0x2a};
+__constant__ unsigned char kWorleyOrder[27] = {0x15, 0x14, 0x16, 0x11, 0x19, 0x05, 0x25, 0x10, 0x18,
+                                               0x12, 0x1a, 0x04, 0x24, 0x06, 0x26, 0x01, 0x21, 0x09,
+                                               0x29, 0x00, 0x20, 0x08, 0x28, 0x02, 0x22, 0x0a, 0x2a};
 
 __device__ inline float worley_noise(const DeviceScene &s, f3 p) {
     const int xi = int(floorf(p.x)), yi = int(floorf(p.y)), zi = int(floorf(p.z));
-    float distance = 9999;
     const float fx = p.x - float(xi), fy = p.y - float(yi), fz = p.z - float(zi);
+    const int dx = s.worley_dim.x, dxy = s.worley_dim.x * s.worley_dim.y;
+    const int ix = xi - 1 - s.worley_lo.x, iy = yi - 1 - s.worley_lo.y, iz = zi - 1 - s.worley_lo.z;
+    const bool inside = ix >= 0 && iy >= 0 && iz >= 0 && ix + 2 < s.worley_dim.x && iy + 2 < s.worley_dim.y &&
+                        iz + 2 < s.worley_dim.z;
+    const float4 *block = inside ? s.worley_cells + (size_t(iz) * dxy + size_t(iy) * dx + ix) : nullptr;
+    float d2 = 0;
 #pragma unroll 1
     for (int c = 0; c < 27; c++) {
         const int code = kWorleyOrder[c];
@@ -144,13 +154,20 @@ __device__ inline float worley_noise(const DeviceScene &s, f3 p) {
             const float gy = yo < 0 ? fy : (yo > 0 ? 1 - fy : 0);
             const float gz = zo < 0 ? fz : (zo > 0 ? 1 - fz : 0);
             const float lb2 = gx * gx + gy * gy + gz * gz;
-            if (lb2 > distance * distance * 1.0001f + 1e-6f) continue;
+            if (lb2 > d2 * 1.0001f + 1e-6f) continue;
         }
-        const f3 cell = mk(float(xi + xo), float(yi + yo), float(zi + zo));
-        const f3 feature = worley_feature(s, xi + xo, yi + yo, zi + zo) + cell;
-        distance = fminf(distance, length(p - feature));
+        f3 off;
+        if (inside) {
+            const float4 h = __ldg(block + ((zo + 1) * dxy + (yo + 1) * dx + (xo + 1)));
+            off = mk(h.x, h.y, h.z);
+        } else {
+            off = worley_feature(s, xi + xo, yi + yo, zi + zo);
+        }
+        const f3 feature = off + mk(float(xi + xo), float(yi + yo), float(zi + zo));
+        const float e2 = length_sq(p - feature);
+        d2 = c == 0 ? e2 : fminf(d2, e2);
     }
-    return distance;
+    return fminf(9999.0f, sqrtf(d2));
 }
 
 // ---------------------------------------------------------------------------
@@ -211,7 +228,7 @@ struct Ray3 {
     f3 o, d, inv;
 };
 
-__device__ __forceinline__ Ray3 make_ray(f3 o, f3 d) { return Ray3{o, d, mk(1 / d.x, 1 / d.y, 1 / d.z)}; }
+__device__ __forceinline__ Ray3 make_ray(f3 o, f3 d) { return Ray3{o, d, mk(rcp(d.x), rcp(d.y), rcp(d.z))}; }
 
 __device__ __forceinline__ bool slab(float4 lo, float4 hi, const Ray3 &r, float &t_entry) {
     float t1 = 0, t2 = kMax;
@@ -290,7 +307,7 @@ __device__ __forceinline__ float intersect_t(const Prim &p, const Ray3 &r, float
     const f3 rcv = cross(r.d, v);
     const float det = dot(h, rcv);
     if (fabsf(det) < kEpsSq) return -1;
-    const float inv = 1 / det;
+    const float inv = rcp(det);
     const f3 oc = r.o - corner;
     const float alpha = inv * dot(oc, rcv);
     if (alpha < 0 || alpha > 1) return -1;
@@ -362,7 +379,7 @@ __device__ __forceinline__ void prim_attributes(const DeviceScene &s, int obj, c
     }
     const f3 rcv = cross(d, v);
     const float det = dot(hz, rcv);
-    const float inv = 1 / det;
+    const float inv = rcp(det);
     const f3 oc = o - corner;
     const float alpha = inv * dot(oc, rcv);
     const f3 och = cross(oc, hz);
@@ -613,7 +630,7 @@ __device__ __forceinline__ float prim_pdf(const Prim &p, f3 point, f3 dir) {
     const f3 rcv = cross(dir, v);
     const float det = dot(h, rcv);
     if (fabsf(det) < kEpsSq) return 0;
-    const float inv = 1 / det;
+    const float inv = rcp(det);
     const f3 oc = point - corner;
     const float alpha = inv * dot(oc, rcv);
     if (alpha < 0 || alpha > 1) return 0;

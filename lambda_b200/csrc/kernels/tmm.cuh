@@ -125,6 +125,11 @@ struct FilmPrep {
     cx<R> cos_layer[MAXL > 0 ? MAXL : 1];
     cx<R> n_in, n_out, cos_out;
     R cos0;
+    // One real-index film with real cosines everywhere (no total internal
+    // reflection): the Fresnel coefficients of its two interfaces (s, p) for the
+    // Airy form in film_apply.
+    bool airy;
+    R rs01, rs12, rp01, rp12;
 };
 
 template <typename R, int MAXL>
@@ -155,11 +160,43 @@ __device__ __forceinline__ void film_prepare(int L, const cx<R> *n, R cos0, Film
     f.n_in = n[0];
     f.n_out = n[f.L + 1];
     f.cos_out = cos_next;
+    f.airy = false;
+    if constexpr (sizeof(R) == 4 && MAXL >= 1) {
+        if (f.L == 1 && n[0].im == R(0) && n[1].im == R(0) && n[2].im == R(0) && f.cos_layer[0].im == R(0) &&
+            cos_next.im == R(0)) {
+            const R n0 = n[0].re, n1 = n[1].re, n2 = n[2].re, c0 = cos0, c1 = f.cos_layer[0].re, c2 = cos_next.re;
+            f.airy = true;
+            f.rs01 = (n0 * c0 - n1 * c1) / (n0 * c0 + n1 * c1);
+            f.rs12 = (n1 * c1 - n2 * c2) / (n1 * c1 + n2 * c2);
+            f.rp01 = (n1 * c0 - n0 * c1) / (n1 * c0 + n0 * c1);
+            f.rp12 = (n2 * c1 - n1 * c2) / (n2 * c1 + n1 * c2);
+        }
+    }
+}
+
+// Reflectance of one film from its two interface coefficients and the cosine of the
+// round-trip phase (Airy summation, the closed form of the 2x2 product), ratio in double.
+__device__ __forceinline__ float airy_r(float r01, float r12, float cos2phi) {
+    const double a = r01, b = r12, ab = a * b, c = cos2phi;
+    return float((a * a + b * b + 2 * ab * c) / (1 + ab * ab + 2 * ab * c));
 }
 
 // Layer phases at one wavelength; k = 2 pi / lambda, d[j] in nm.
 template <typename R, int MAXL>
 __device__ __forceinline__ FilmResult<R> film_apply(const FilmPrep<R, MAXL> &f, const R *d, R k, bool want_t) {
+    if constexpr (sizeof(R) == 4 && MAXL >= 1) {
+        if (f.airy) {
+            // the same phase as below: ((n k) d) cos, real here; round trip 2 phi
+            const R phi = ((f.n_layer[0].re * k) * d[0]) * f.cos_layer[0].re;
+            const R c2 = cosf(2 * phi);
+            FilmResult<R> out;
+            out.rs = airy_r(f.rs01, f.rs12, c2);
+            out.rp = airy_r(f.rp01, f.rp12, c2);
+            out.ts = want_t ? 1 - out.rs : R(0);  // lossless, no total internal reflection
+            out.tp = want_t ? 1 - out.rp : R(0);
+            return out;
+        }
+    }
     m2<R> ms = f.is[0], mp = f.ip[0];
 #pragma unroll
     for (int j = 0; j < MAXL; j++) {
