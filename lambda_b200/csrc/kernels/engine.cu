@@ -1044,8 +1044,8 @@ extern "C" lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning 
 }
 
 // Times the probe render (its output stays in device memory): first the three BVH
-// widths, then every block-shape candidate at the fastest width, each after one
-// warm-up render, and keeps the fastest. The
+// widths, then every block-shape candidate at the fastest width, each as the best
+// of three renders after one warm-up, and keeps the fastest. The
 // path-state capacity is set from free device memory: half of it, at the bytes of
 // path state and queues a pixel needs.
 extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out) {
@@ -1063,12 +1063,14 @@ extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_de
     lambda_tuning best = keep;
     double best_ms = 1e300;
     // the BVH width first, at the current block shapes, then the block shapes at that width
+    // one warm-up render, then the best of three timed ones
     auto trial = [&](const lambda_tuning &t, double &ms) -> lambda_status {
         ctx->tuning = t;
-        lambda_status r = LAMBDA_OK;
-        for (int rep = 0; rep < 2 && r == LAMBDA_OK; rep++) {
+        lambda_status r = render_jobs(ctx, &job, 1, nullptr);
+        ms = 1e300;
+        for (int rep = 0; rep < 3 && r == LAMBDA_OK; rep++) {
             r = render_jobs(ctx, &job, 1, nullptr);
-            ms = ctx->stats.render_ms;
+            ms = std::min(ms, ctx->stats.render_ms);
         }
         return r;
     };
