@@ -42,3 +42,16 @@ def camera_rays(settings, n: int, seed: int) -> np.ndarray:
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     o = np.repeat(pos[None], n, axis=0)
     return np.concatenate([o, d], axis=1).astype(np.float32)
+
+
+_REF_SCENES = {}
+
+
+def ref_scene(lrd: str):
+    """The reference harness's scene for an .lrd file, built once per test session
+    (the reference's BVH build takes seconds on a million triangles)."""
+    from oracle import ref
+
+    if lrd not in _REF_SCENES:
+        _REF_SCENES[lrd] = ref.RefScene(lrd)
+    return _REF_SCENES[lrd]

@@ -7,7 +7,7 @@ import pytest
 import lambda_b200 as lb
 from lambda_b200 import scenes
 from oracle import port, ref
-from tests.helpers import rel_rmse
+from tests.helpers import ref_scene, rel_rmse
 
 pytestmark = pytest.mark.gpu
 
@@ -19,6 +19,7 @@ CASES = {
     "thinfilm": lambda d: scenes.thinfilm_spheres(d, 96, 54, 16, name="r_thinfilm.lrd"),
     "thinfilm_deep": lambda d: scenes.thinfilm_spheres(d, 64, 36, 4, depth=24, name="r_thinfilm_deep.lrd"),
     "mesh": lambda d: scenes.perlin_sphere(d, 48, 48, 4, levels=5, name="r_mesh.lrd"),
+    "mesh_1m": lambda d: scenes.perlin_sphere(d, 48, 48, 4, levels=9, name="r_mesh_1m.lrd"),
     "instanced": lambda d: scenes.instanced_meshes(d, 64, 40, 9, depth=8, instances=120, segments=16, rings=9,
                                                    box=14.0, name="r_instanced.lrd"),
 }
@@ -31,7 +32,7 @@ def test_matched_stream_render(case, scene_dir, ctx):
     ctx.upload(scene)
     img = ctx.render(scene.render_desc(seed=sc.seed))
     # the reference's own CPU renderer when built, else the oracle pinned to it bit for bit
-    want = ref.RefScene(sc.lrd).render(sc.seed)[0] if ref.available() else port.render(scene, sc.seed)
+    want = ref_scene(sc.lrd).render(sc.seed)[0] if ref.available() else port.render(scene, sc.seed)
     assert np.isfinite(img).all()
     err = rel_rmse(img, want)
     same = float((img == want).all(axis=2).mean())

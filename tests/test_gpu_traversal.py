@@ -7,7 +7,7 @@ import pytest
 import lambda_b200 as lb
 from lambda_b200 import scenes
 from oracle import port, ref
-from tests.helpers import camera_rays, random_rays
+from tests.helpers import camera_rays, random_rays, ref_scene
 
 pytestmark = pytest.mark.gpu
 
@@ -17,6 +17,8 @@ SCENES = {
     "mesh": lambda d: scenes.perlin_sphere(d, 64, 64, 4, levels=5),
     "instanced": lambda d: scenes.instanced_meshes(d, 64, 40, 4, depth=8, instances=300, segments=24, rings=13,
                                                    box=20.0, name="t_instanced.lrd"),
+    # the BVH stress configuration at full size: 1,048,576 triangles, tree depth capped at 20
+    "mesh_1m": lambda d: scenes.perlin_sphere(d, 64, 64, 4, levels=9, name="t_mesh_1m.lrd"),
 }
 
 
@@ -59,7 +61,7 @@ def _plane_rays(scene, n=6000, seed=17):
 
 def _oracle_hit(sc, scene, rays):
     if ref.available():
-        r_inst, r_obj, r_t, _, _ = ref.RefScene(sc.lrd).hit(rays)
+        r_inst, r_obj, r_t, _, _ = ref_scene(sc.lrd).hit(rays)
         return r_inst, r_obj, r_t
     return port.hit(scene, rays)
 
@@ -92,7 +94,7 @@ def test_shadow_bit_exact(loaded, width, ctx):
     pick = np.random.default_rng(5).integers(0, len(li_all), size=rays.shape[0])
     li, lo = li_all[pick], lo_all[pick]
     occ = ctx.trace_shadow(rays, li, lo)
-    r_occ = ref.RefScene(sc.lrd).shadow(rays, li, lo) if ref.available() else port.shadow(scene, rays, li, lo)
+    r_occ = ref_scene(sc.lrd).shadow(rays, li, lo) if ref.available() else port.shadow(scene, rays, li, lo)
     assert (occ == r_occ).all(), f"{name}/{width}: occlusion differs at {np.flatnonzero(occ != r_occ)[:10]}"
 
 
