@@ -143,6 +143,17 @@ ItemBounds object_bounds(const lambda_object &o) {
 
 float half_area(const V3 &e) { return 2 * (e[0] * e[1] + e[0] * e[2] + e[1] * e[2]); }
 
+// Subtrees of at least this many items are split across threads (see build_range).
+constexpr int kParallelItems = 1024;
+
+// Levels of the build that hand their right subtree to another thread: enough for
+// every host thread.
+int spawn_levels() {
+    int levels = 0;
+    for (unsigned t = std::max(1u, std::thread::hardware_concurrency()); t > 1; t >>= 1) levels++;
+    return levels;
+}
+
 // Runs fn(i) for i in [0, n) on all host threads, in contiguous blocks. Each i is
 // computed by one thread alone, so results do not depend on the thread count.
 template <class F>
@@ -163,7 +174,7 @@ void parallel_for(size_t n, F fn) {
 // One recursive binned-SAH build over order[start, end) (bvh.h:111-246). Returns
 // the node index of the subtree root.
 int build_range(const std::vector<ItemBounds> &items, std::vector<int> &order, int start, int end,
-                std::vector<lambda_bvh_node> &nodes, int depth) {
+                std::vector<lambda_bvh_node> &nodes, int depth, int spawn = 0) {
     V3 lo = v3(kMax, kMax, kMax), hi = v3(-kMax, -kMax, -kMax);
     V3 clo = lo, chi = hi;
     for (int i = start; i < end; i++) {
@@ -259,8 +270,26 @@ int build_range(const std::vector<ItemBounds> &items, std::vector<int> &order, i
     inner.index = -1;
     inner.count = 0;
     nodes.push_back(inner);
-    build_range(items, order, start, mid, nodes, depth + 1);
-    const int right = build_range(items, order, mid, end, nodes, depth + 1);
+    if (spawn > 0 && end - start >= kParallelItems) {
+        // The right subtree reorders only order[mid, end), so it is built on another
+        // thread into its own array (node links relative to that array) while the left
+        // one is built here; it is then appended after the left subtree with its links
+        // shifted, which is the array the sequential build writes.
+        std::vector<lambda_bvh_node> right_nodes;
+        right_nodes.reserve(size_t(2 * (end - mid)));
+        std::thread t([&] { build_range(items, order, mid, end, right_nodes, depth + 1, spawn - 1); });
+        build_range(items, order, start, mid, nodes, depth + 1, spawn - 1);
+        t.join();
+        const int offset = int(nodes.size());
+        for (lambda_bvh_node &n : right_nodes) {
+            if (n.count == 0) n.index += offset;  // interior: link to its right child
+            nodes.push_back(n);
+        }
+        nodes[self].index = offset;
+        return self;
+    }
+    build_range(items, order, start, mid, nodes, depth + 1, spawn);
+    const int right = build_range(items, order, mid, end, nodes, depth + 1, spawn);
     nodes[self].index = right;
     return self;
 }
@@ -279,7 +308,7 @@ void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
     parallel_for(s.instances.size(), [&](size_t i) { inst_bounds[i] = instance_bounds(s, s.instances[i]); });
     std::vector<int> order(s.instances.size());
     std::iota(order.begin(), order.end(), 0);
-    build_range(inst_bounds, order, 0, int(s.instances.size()), s.nodes, 1);
+    build_range(inst_bounds, order, 0, int(s.instances.size()), s.nodes, 1, spawn_levels());
     {
         std::vector<lambda_instance> reordered;
         reordered.reserve(s.instances.size());
@@ -289,13 +318,13 @@ void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
 
     // one BLAS per object group, over a shared object order
     std::vector<ItemBounds> obj_bounds(s.objects.size());
-    for (size_t i = 0; i < s.objects.size(); i++) obj_bounds[i] = object_bounds(s.objects[i]);
+    parallel_for(s.objects.size(), [&](size_t i) { obj_bounds[i] = object_bounds(s.objects[i]); });
     std::vector<int> obj_order(s.objects.size());
     std::iota(obj_order.begin(), obj_order.end(), 0);
     std::map<int, int> root_of_group;
     for (size_t g = 0; g + 1 < group_offsets.size(); g++) {
         root_of_group[group_offsets[g]] = int(s.nodes.size());
-        build_range(obj_bounds, obj_order, group_offsets[g], group_offsets[g + 1], s.nodes, 1);
+        build_range(obj_bounds, obj_order, group_offsets[g], group_offsets[g + 1], s.nodes, 1, spawn_levels());
     }
     for (auto &in : s.instances) in.node = root_of_group.at(in.object);
     {
