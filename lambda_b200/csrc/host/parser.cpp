@@ -14,6 +14,10 @@
 #include <complex>
 #include <cstring>
 #include <fstream>
+#include <iterator>
+#include <limits>
+#include <string_view>
+#include <charconv>
 #include <map>
 #include <sstream>
 #include <string>
@@ -637,9 +641,60 @@ void LrdReader::run() {
 
 // parser.h:639-786. Faces are fan-triangulated; missing vt gives per-triangle
 // uvs (0,0), (1,0), (0,1); missing vn gives the flat normal.
+// Fast reading of the common OBJ lines ("v x y z", "vt u v", "vn x y z" with plain
+// decimal numbers, "f a b c ..." with plain positive indices). A token is taken only
+// when std::from_chars consumes it whole, its characters are [0-9.eE+-] (so no
+// inf/nan, which the stream extraction rejects), and the value is zero or normal
+// (no overflow or subnormal range, where stream extraction may fail): for those
+// both give the same correctly rounded float. Any other line returns false and is
+// read by the stream-based code, which keeps the reference's semantics and errors.
+namespace obj_fast {
+
+bool is_space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+
+bool next_token(const char *&p, const char *end, const char *&tb, const char *&te) {
+    while (p < end && is_space(*p)) p++;
+    if (p >= end) return false;
+    tb = p;
+    while (p < end && !is_space(*p)) p++;
+    te = p;
+    return true;
+}
+
+bool number(const char *tb, const char *te, float &out) {
+    bool digit_nonzero = false;
+    for (const char *c = tb; c < te; c++) {
+        if (!((*c >= '0' && *c <= '9') || *c == '.' || *c == 'e' || *c == 'E' || *c == '+' || *c == '-')) return false;
+        if (*c >= '1' && *c <= '9') digit_nonzero = true;
+    }
+    if (*tb == '+') return false;
+    float v = 0;
+    const auto r = std::from_chars(tb, te, v, std::chars_format::general);
+    if (r.ec != std::errc() || r.ptr != te) return false;
+    if (v == 0.0f ? digit_nonzero : !(std::fabs(v) >= std::numeric_limits<float>::min())) return false;
+    if (!std::isfinite(v)) return false;
+    out = v;
+    return true;
+}
+
+bool index(const char *tb, const char *te, int size, int &out) {
+    if (te - tb > 9) return false;
+    int v = 0;
+    for (const char *c = tb; c < te; c++) {
+        if (*c < '0' || *c > '9') return false;
+        v = v * 10 + (*c - '0');
+    }
+    if (v < 1 || v > size) return false;
+    out = v - 1;
+    return true;
+}
+
+}  // namespace obj_fast
+
 void read_obj(const std::string &path, std::vector<lambda_object> &objects, int material) {
-    std::ifstream in(path);
+    std::ifstream in(path, std::ios::binary);
     if (!in.is_open()) throw SceneError(LAMBDA_ERR_IO, path + ": failed to open file (" + strerror_lower() + ")");
+    const std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
     int line_no = 0;
     auto error = [&](const std::string &msg) {
         return SceneError(LAMBDA_ERR_PARSE, path + ":" + std::to_string(line_no) + ": " + msg);
@@ -647,11 +702,71 @@ void read_obj(const std::string &path, std::vector<lambda_object> &objects, int 
     bool have_face = false;
     std::vector<V3> vertices, normals;
     std::vector<float> us, vs;
-    std::string line;
     std::vector<int> vi, ti, ni;
-    while (std::getline(in, line)) {
+    auto emit_face = [&]() {
+        if (vi.size() < 3) throw error("'f' must have at least 3 vertices");
+        const V3 zero = v3(0, 0, 0);
+        const V3 p0 = vertices[vi[0]];
+        const V3 n0 = ni[0] >= 0 ? normals[ni[0]] : zero;
+        const float u0 = ti[0] >= 0 ? us[ti[0]] : 0, v0 = ti[0] >= 0 ? vs[ti[0]] : 0;
+        for (size_t k = 1; k + 1 < vi.size(); k++) {
+            const V3 p1 = vertices[vi[k]], p2 = vertices[vi[k + 1]];
+            const V3 n1 = ni[k] >= 0 ? normals[ni[k]] : zero;
+            const V3 n2 = ni[k + 1] >= 0 ? normals[ni[k + 1]] : zero;
+            const float u1 = ti[k] >= 0 ? us[ti[k]] : 1, v1 = ti[k] >= 0 ? vs[ti[k]] : 0;
+            const float u2 = ti[k + 1] >= 0 ? us[ti[k + 1]] : 0, v2 = ti[k + 1] >= 0 ? vs[ti[k + 1]] : 1;
+            objects.push_back(make_tri(material, p0, p1 - p0, p2 - p0, n0, n1, n2, u0, u1, u2, v0, v1, v2));
+        }
+    };
+    // One line by the fast rules; false leaves every container as it was.
+    auto fast_line = [&](const char *p, const char *end) -> bool {
+        const char *tb, *te;
+        if (!obj_fast::next_token(p, end, tb, te)) return true;  // blank line
+        const std::string_view tag(tb, size_t(te - tb));
+        if (tag == "v" || tag == "vn") {
+            float x[3];
+            for (float &c : x)
+                if (!obj_fast::next_token(p, end, tb, te) || !obj_fast::number(tb, te, c)) return false;
+            if (obj_fast::next_token(p, end, tb, te)) return false;
+            (tag == "v" ? vertices : normals).push_back(v3(x[0], x[1], x[2]));
+            return true;
+        }
+        if (tag == "vt") {
+            float u, v;
+            if (!obj_fast::next_token(p, end, tb, te) || !obj_fast::number(tb, te, u)) return false;
+            if (!obj_fast::next_token(p, end, tb, te) || !obj_fast::number(tb, te, v)) return false;
+            if (obj_fast::next_token(p, end, tb, te)) return false;
+            us.push_back(u);
+            vs.push_back(v);
+            return true;
+        }
+        if (tag == "f") {
+            vi.clear();
+            while (obj_fast::next_token(p, end, tb, te)) {
+                int idx;
+                if (!obj_fast::index(tb, te, int(vertices.size()), idx)) return false;
+                vi.push_back(idx);
+            }
+            if (vi.size() < 3) return false;
+            ti.assign(vi.size(), -1);
+            ni.assign(vi.size(), -1);
+            have_face = true;
+            emit_face();
+            return true;
+        }
+        return false;
+    };
+    std::string line;
+    size_t pos = 0;
+    while (pos < text.size()) {
+        size_t eol = text.find('\n', pos);
+        if (eol == std::string::npos) eol = text.size();
+        const char *lb = text.data() + pos, *le = text.data() + eol;
+        pos = eol + 1;
         line_no++;
-        if (line.empty()) continue;
+        if (lb == le) continue;
+        if (fast_line(lb, le)) continue;
+        line.assign(lb, le);
         std::istringstream ss(line);
         std::string tag;
         if (!(ss >> tag)) continue;
@@ -704,19 +819,7 @@ void read_obj(const std::string &path, std::vector<lambda_object> &objects, int 
                 ti.push_back(b.empty() ? -1 : resolve(b, int(us.size()), "vt"));
                 ni.push_back(c.empty() ? -1 : resolve(c, int(normals.size()), "vn"));
             }
-            if (vi.size() < 3) throw error("'f' must have at least 3 vertices");
-            const V3 zero = v3(0, 0, 0);
-            const V3 p0 = vertices[vi[0]];
-            const V3 n0 = ni[0] >= 0 ? normals[ni[0]] : zero;
-            const float u0 = ti[0] >= 0 ? us[ti[0]] : 0, v0 = ti[0] >= 0 ? vs[ti[0]] : 0;
-            for (size_t k = 1; k + 1 < vi.size(); k++) {
-                const V3 p1 = vertices[vi[k]], p2 = vertices[vi[k + 1]];
-                const V3 n1 = ni[k] >= 0 ? normals[ni[k]] : zero;
-                const V3 n2 = ni[k + 1] >= 0 ? normals[ni[k + 1]] : zero;
-                const float u1 = ti[k] >= 0 ? us[ti[k]] : 1, v1 = ti[k] >= 0 ? vs[ti[k]] : 0;
-                const float u2 = ti[k + 1] >= 0 ? us[ti[k + 1]] : 0, v2 = ti[k + 1] >= 0 ? vs[ti[k + 1]] : 1;
-                objects.push_back(make_tri(material, p0, p1 - p0, p2 - p0, n0, n1, n2, u0, u1, u2, v0, v1, v2));
-            }
+            emit_face();
         } else {
             continue;
         }

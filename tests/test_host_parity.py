@@ -102,3 +102,50 @@ def test_scene_generators_are_deterministic(tmp_path):
     assert open(a.lrd).read() == open(b.lrd).read()
     n = scenes.write_perlin_sphere_obj(str(tmp_path / "s.obj"), levels=3)
     assert n == 4 * 4 ** 3
+
+
+OBJ_HEAD = ("Render 8 8 1 1 380 780\nMaterial m lambertian 0.5\nObject o mesh m {obj}\n"
+            "Instance o default (0 0 0) (0 0 0) (1 1 1)\nBackground equirectangular 0\n"
+            "Camera (0 0 -3) (-0.5 0.5 -2) (1 0 0) (0 -1 0)\n")
+OBJ_CASES = [
+    # lines the fast reader takes, and lines it leaves to the stream reader (face
+    # index 0, which the reference reads before its first vertex, is rejected here)
+    "v 1. .5 -0\nv 1e-3 2E+2 3\nv 0.25 -1.5e1 2\nf 1 2 3\n",
+    "v +1 2 3\nv 0 1 0\nv 0 0 1\nvt 0.5 0.25\nvn 0 0 1\nf 1/1/1 2/1/1 3/1/1\nf -3 -2 -1\n",
+    "# comment\r\nv 0 0 0\r\nv 1 0 0 \r\nv 0 1 0\r\no name\r\ng grp\r\nf 1 2 3",
+    "v 1e-40 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n",
+    "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nf 1 2 4 3\nf 1  2\t3\n",
+    "v inf 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n",
+    "v 0 0 0 1\nv 1 0 0\nv 0 1 0\nf 1 2 3\n",
+    "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 4\n",
+    "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2\n",
+    "v 1 2\n",
+]
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference harness not built")
+def test_obj_reader_matches_reference(tmp_path):
+    """OBJ lines on both reading paths give the reference's triangles byte for
+    byte, or its error message."""
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        for i, obj in enumerate(OBJ_CASES):
+            (tmp_path / f"m{i}.obj").write_bytes(obj.encode())
+            lrd = tmp_path / f"s{i}.lrd"
+            lrd.write_text(OBJ_HEAD.format(obj=f"m{i}.obj"))
+            try:
+                want = ref.RefScene(lrd.name).raw("objects")
+                want_err = ""
+            except ref.RefError as e:
+                want, want_err = None, str(e)
+            try:
+                got = lb.HostScene.parse(lrd.name).raw("objects")
+                got_err = ""
+            except lb.LambdaError as e:
+                got, got_err = None, e.message
+            assert got_err == want_err, f"case {i}"
+            if want is not None:
+                assert got.shape == want.shape and (got == want).all(), f"case {i}"
+    finally:
+        os.chdir(cwd)
