@@ -135,14 +135,23 @@ def dist_init(n_gpus: int):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """The largest x over all ranks (device tensor under NCCL, host tensor under gloo)."""
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job(paths_per_rank_step: int, steps: int, rank_ms: float, world: int):
+    """Replicas: every rank renders its own frames, so the job's rate is all ranks'
+    paths over the slowest rank's device time. Returns (paths/s, max ms)."""
+    max_ms = max_over_ranks(rank_ms, world)
+    return world * paths_per_rank_step * steps / (max_ms / 1000.0), max_ms
 
 
 def barrier(world: int):
@@ -331,8 +340,7 @@ def run_batch(args, ctx, scene, lb, torch, rank, world, local):
             st = ctx.stats()
             total_ms += st.render_ms
             launches += st.kernel_launches
-    max_ms = max_over_ranks(total_ms, world)
-    value = world * paths * args.steps / (max_ms / 1000.0)
+    value, max_ms = whole_job(paths, args.steps, total_ms, world)
     # the same jobs one render call at a time
     seq_ms = 0.0
     for d, o in zip(descs, outs):
@@ -440,8 +448,7 @@ def main():
             launches += st.kernel_launches
         torch.cuda.synchronize()
     barrier(world)
-    max_ms = max_over_ranks(total_ms, world)
-    value = world * paths_per_step * args.steps / (max_ms / 1000.0)
+    value, max_ms = whole_job(paths_per_step, args.steps, total_ms, world)
 
     # per-stage kernel times (CUDA events inside the library) for the roofline
     stage = lb.stage_profile(ctx, desc, dev_out)
