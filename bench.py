@@ -468,13 +468,25 @@ def main():
             o_ms += ctx.stats().render_ms
         o_ms = max_over_ranks(o_ms, world)
         o_value = world * paths_per_step * args.steps / (o_ms / 1000.0)
+        sur_ctas = ctx.stats().surrogate_ctas_per_sm if other == "surrogate" else stats[-1].surrogate_ctas_per_sm
         ex_value, su_value = (value, o_value) if mode == "exact" else (o_value, value)
+        # the reference's own arithmetic (complex double transfer matrix per hit)
+        fp64_desc = scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_FP64 | lb.RENDER_OUTPUT_DEVICE)
+        ctx.render(fp64_desc, out=dev_out)
+        f_ms = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ctx.render(fp64_desc, out=dev_out)
+            f_ms += ctx.stats().render_ms
+        f_ms = max_over_ranks(f_ms, world)
+        f_value = world * paths_per_step * args.steps / (f_ms / 1000.0)
         comparison = {"exact_tmm_value": ex_value, "surrogate_value": su_value,
+                      "exact_fp64_reference_form_value": f_value, "surrogate_over_fp64_form": su_value / f_value,
                       "exact_tmm_ms_per_step": (max_ms if mode == "exact" else o_ms) / args.steps,
                       "surrogate_ms_per_step": (o_ms if mode == "exact" else max_ms) / args.steps,
                       "surrogate_over_exact": su_value / ex_value,
-                      "surrogate_ctas_per_sm": ctx.stats().surrogate_ctas_per_sm if other == "surrogate"
-                      else stats[-1].surrogate_ctas_per_sm}
+                      "surrogate_ctas_per_sm": sur_ctas}
         if rank == 0:
             comparison["quality"] = image_quality(ctx, scene, dev_out)
             comparison["surrogate_error_vs_fp64"] = surrogate_error(ctx)

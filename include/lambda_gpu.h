@@ -246,6 +246,7 @@ lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene_desc *scen
 #define LAMBDA_RENDER_THINFILM_SURROGATE 1u   /* BF16 MLP on tensor cores, FP32 fallback per hit */
 #define LAMBDA_RENDER_OUTPUT_DEVICE 2u        /* out_rgb is device memory: no copy back */
 #define LAMBDA_RENDER_PROFILE_STAGES 4u       /* time every kernel launch with CUDA events (no graph replay) */
+#define LAMBDA_RENDER_THINFILM_FP64 8u        /* the reference's complex double transfer matrix per hit */
 
 typedef struct lambda_render_desc {
     lambda_render_settings settings;

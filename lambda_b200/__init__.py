@@ -40,6 +40,7 @@ RENDER_THINFILM_EXACT = N.RENDER_THINFILM_EXACT
 RENDER_THINFILM_SURROGATE = N.RENDER_THINFILM_SURROGATE
 RENDER_OUTPUT_DEVICE = N.RENDER_OUTPUT_DEVICE
 RENDER_PROFILE_STAGES = N.RENDER_PROFILE_STAGES
+RENDER_THINFILM_FP64 = N.RENDER_THINFILM_FP64
 
 
 def _arr(ptr, n, dtype, shape=None):

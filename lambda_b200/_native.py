@@ -36,6 +36,7 @@ RENDER_THINFILM_EXACT = 0
 RENDER_THINFILM_SURROGATE = 1
 RENDER_OUTPUT_DEVICE = 2
 RENDER_PROFILE_STAGES = 4
+RENDER_THINFILM_FP64 = 8
 NUM_STAGES = 12
 STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
                "shadow", "finish", "film_surrogate", "unused10", "unused11")

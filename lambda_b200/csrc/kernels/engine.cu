@@ -671,7 +671,7 @@ struct RenderTotals {
 
 // Renders jobs[order[first..last)] as one wavefront pass (see lambda_render_batch).
 lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::vector<int> &order, size_t first,
-                          size_t last, bool surrogate, StageProfiler *prof, volatile int32_t *completed,
+                          size_t last, bool surrogate, bool fp64, StageProfiler *prof, volatile int32_t *completed,
                           int32_t completed_base, int32_t completed_total, RenderTotals &tot) {
     const size_t nj = last - first;
     std::vector<Job> dj(nj);
@@ -755,7 +755,7 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     };
     const int g_lambert = grid((const void *)k_shade_lambert, sb, 0);
     const int g_spec = grid((const void *)k_shade_specular, sb, 0);
-    const int g_film = grid((const void *)k_shade_film_exact, sb, 0);
+    const int g_film = grid(fp64 ? (const void *)k_shade_film_exact<true> : (const void *)k_shade_film_exact<false>, sb, 0);
     const int pix_blocks = (P + 255) / 256;
 
     // One wave's launches. With a profiler every launch is bracketed by events.
@@ -776,7 +776,8 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
             if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<g_spec, sb, 0, stream>>>(b, rp, sc, ps); });
             if (sc.families & 4u) {
                 if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, pr);
-                else timed(6, [&] { k_shade_film_exact<<<g_film, sb, 0, stream>>>(b, rp, sc, ps); });
+                else if (fp64) timed(6, [&] { k_shade_film_exact<true><<<g_film, sb, 0, stream>>>(b, rp, sc, ps); });
+                else timed(6, [&] { k_shade_film_exact<false><<<g_film, sb, 0, stream>>>(b, rp, sc, ps); });
             }
             if (sc.families & 1u) timed(7, [&] { shadow(b); });
         }
@@ -923,18 +924,22 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
 // a larger single job alone), ordered by decreasing sample count.
 lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volatile int32_t *completed) {
     if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
-    const uint32_t mode = jobs[0].desc.flags & (LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_PROFILE_STAGES);
+    constexpr uint32_t kModeBits = LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_THINFILM_FP64 | LAMBDA_RENDER_PROFILE_STAGES;
+    const uint32_t mode = jobs[0].desc.flags & kModeBits;
+    if ((mode & LAMBDA_RENDER_THINFILM_SURROGATE) && (mode & LAMBDA_RENDER_THINFILM_FP64))
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "the surrogate and the FP64 thin film exclude each other");
     int64_t total_pixels = 0;
     for (int i = 0; i < n; i++) {
         if (!jobs[i].out_rgb) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "job without an output image");
         lambda_status s = check_settings(ctx, jobs[i].desc.settings);
         if (s != LAMBDA_OK) return s;
-        if ((jobs[i].desc.flags & (LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_PROFILE_STAGES)) != mode)
+        if ((jobs[i].desc.flags & kModeBits) != mode)
             return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "the jobs of a batch must share the thin-film mode and profiling flag");
         total_pixels += int64_t(jobs[i].desc.settings.width) * jobs[i].desc.settings.height;
     }
     if (total_pixels > INT32_MAX) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "more than 2^31 pixels in one batch");
     const bool surrogate = (mode & LAMBDA_RENDER_THINFILM_SURROGATE) != 0;
+    const bool fp64 = (mode & LAMBDA_RENDER_THINFILM_FP64) != 0;
     const bool profile = (mode & LAMBDA_RENDER_PROFILE_STAGES) != 0;
     if (surrogate) {
         lambda_status s = ctx->surrogate_ready();
@@ -972,7 +977,7 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
             px += add;
             last++;
         }
-        lambda_status s = render_pass(ctx, jobs, order, first, last, surrogate, profile ? &prof : nullptr, completed,
+        lambda_status s = render_pass(ctx, jobs, order, first, last, surrogate, fp64, profile ? &prof : nullptr, completed,
                                       int32_t(tot.pixels), int32_t(total_pixels), tot);
         if (s != LAMBDA_OK) return s;
         first = last;
@@ -1058,7 +1063,8 @@ extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_de
     DeviceBuffer img;
     CK(img.reserve(P * 12), "allocate probe image");
     lambda_job job{*probe, img.as<float>()};
-    job.desc.flags = (probe->flags & LAMBDA_RENDER_THINFILM_SURROGATE) | LAMBDA_RENDER_OUTPUT_DEVICE;
+    job.desc.flags = (probe->flags & (LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_THINFILM_FP64)) |
+                     LAMBDA_RENDER_OUTPUT_DEVICE;
     const lambda_tuning keep = ctx->tuning;
     lambda_tuning best = keep;
     double best_ms = 1e300;

@@ -243,7 +243,7 @@ __device__ __forceinline__ FilmResult<R> film_stack(int L, const cx<R> *n, const
 // The same product formed one interface at a time (any number of layers, no
 // per-layer arrays): index_of(j) gives n[j], d[j] the layer thicknesses.
 template <typename R, class IndexOf>
-__device__ __forceinline__ R film_reflectance_stream(int L, IndexOf index_of, const R *d, R cos0, R k) {
+__device__ __forceinline__ void film_amplitudes_stream(int L, IndexOf index_of, const R *d, R cos0, R k, R &rs2, R &rp2) {
     cx<R> n0 = index_of(0), n1 = index_of(1);
     cx<R> cos_cur = cmk(cos0, R(0));
     cx<R> sin_next = n0 / n1;
@@ -270,7 +270,15 @@ __device__ __forceinline__ R film_reflectance_stream(int L, IndexOf index_of, co
         ms = mmul(ms, dmul(e_minus, e_plus, interface_matrix(a, n1, cos_cur, cos_next, false)));
         mp = mmul(mp, dmul(e_minus, e_plus, interface_matrix(a, n1, cos_cur, cos_next, true)));
     }
-    return (cabs2(ms.b / ms.a) + cabs2(mp.b / mp.a)) * R(0.5);
+    rs2 = cabs2(ms.b / ms.a);
+    rp2 = cabs2(mp.b / mp.a);
+}
+
+template <typename R, class IndexOf>
+__device__ __forceinline__ R film_reflectance_stream(int L, IndexOf index_of, const R *d, R cos0, R k) {
+    R rs2, rp2;
+    film_amplitudes_stream<R>(L, index_of, d, cos0, k, rs2, rp2);
+    return (rs2 + rp2) * R(0.5);
 }
 
 }  // namespace lambda_dev

@@ -450,6 +450,33 @@ __device__ inline s4 thin_film_r4(const DeviceScene &sc, const int4 &m, bool fro
     return R;
 }
 
+// Thin-film reflectance as the reference evaluates it (material.h:263-309): complex
+// double characteristic matrices from the complex spectra, k = 2 pi / lambda formed
+// in float, |r| rounded to float and squared in float.
+__device__ inline s4 thin_film_r4_fp64(const DeviceScene &sc, const int4 &m, bool front, float cos0, const s4 &lam,
+                                       const float *thickness) {
+    const int L = m.y < kMaxFilmLayers ? m.y : kMaxFilmLayers;
+    double d[kMaxFilmLayers];
+    for (int k = 0; k < L; k++) d[k] = double(thickness[front ? k : L - 1 - k]);
+    s4 R;
+#pragma unroll 1
+    for (int w = 0; w < kHero; w++) {
+        const float lambda = lam.v[w];
+        auto index_of = [&](int k) {
+            const int src = front ? k : L + 1 - k;
+            const double2 c = cspectrum_at(sc, sc.material_props[m.z + src], lambda);
+            return cx<double>{c.x, c.y};
+        };
+        double rs2, rp2;
+        film_amplitudes_stream<double>(L, index_of, d, double(cos0), double((2 * kPi) / lambda), rs2, rp2);
+        float rs = float(sqrt(rs2)), rp = float(sqrt(rp2));
+        rs *= rs;
+        rp *= rp;
+        R.v[w] = (rs + rp) * 0.5f;
+    }
+    return R;
+}
+
 // Hero-wavelength reflect/refract choice and secondary-wavelength weights of the
 // thin film (material.h:228-261), given the four reflectances.
 __device__ __forceinline__ void thin_film_scatter(const DeviceScene &sc, const ShadeIn &s, const s4 &R, Rng &rng,
@@ -477,7 +504,9 @@ __device__ __forceinline__ void thin_film_thickness(const DeviceScene &sc, const
     for (int k = 0; k < L; k++) thick[k] = scalar_texture(sc, sc.material_props[s.m.w + k], s.sp.point);
 }
 
-// Thin film with the exact FP32 transfer matrix over the bounce's thin-film queue.
+// Thin film evaluated exactly over the bounce's thin-film queue: in FP32 (within 1e-5
+// of FP64), or with kFp64 in the reference's complex double arithmetic.
+template <bool kFp64>
 LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
     const int n = ps.counts[queue_slot(bounce, kQFilm)];
     const int *q = ps.mat_queue[2];
@@ -492,7 +521,8 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, Rend
             const ShadeIn s = load_shade(ps, sc, p);
             float thick[kMaxFilmLayers];
             thin_film_thickness(sc, s, thick);
-            const s4 R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+            const s4 R = kFp64 ? thin_film_r4_fp64(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick)
+                               : thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
             Rng rng = path_rng(ps, p);
             s4 att;
             f3 nd;

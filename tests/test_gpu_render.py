@@ -51,3 +51,23 @@ def test_completed_counter(scene_dir, ctx):
     done = ctypes.c_int32(0)
     ctx.render(scene.render_desc(seed=1), completed=ctypes.pointer(done))
     assert done.value == 16 * 16
+
+
+def test_fp64_thin_film_render(scene_dir, ctx):
+    """LAMBDA_RENDER_THINFILM_FP64 evaluates each thin-film hit in the reference's
+    complex double arithmetic: within 1% and at least as close to the reference's
+    render as the FP32 form; the surrogate flag excludes it."""
+    sc = scenes.thinfilm_spheres(scene_dir, 96, 54, 16, name="r64_thinfilm.lrd")
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx.upload(scene)
+    want = ref_scene(sc.lrd).render(sc.seed)[0] if ref.available() else port.render(scene, sc.seed)
+    f32 = ctx.render(scene.render_desc(seed=sc.seed))
+    f64 = ctx.render(scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_FP64))
+    e32, e64 = rel_rmse(f32, want), rel_rmse(f64, want)
+    same32 = float((f32 == want).all(axis=2).mean())
+    same64 = float((f64 == want).all(axis=2).mean())
+    print(f"thin film FP32: relRMSE {e32:.3e}, identical {same32:.3f}; FP64: relRMSE {e64:.3e}, identical {same64:.3f}")
+    assert e64 <= TOL_RELRMSE and e64 <= e32 * 1.01 + 1e-9
+    assert same64 >= same32
+    with pytest.raises(lb.LambdaError):
+        ctx.render(scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_FP64 | lb.RENDER_THINFILM_SURROGATE))
