@@ -285,9 +285,10 @@ def surrogate_error(ctx) -> dict:
 
 
 def film_queries(ctx, local: int, n: int = 1 << 24, reps: int = 5) -> dict:
-    """Film evaluations per second of the two evaluators on device-resident batches
-    of n queries (wall time of the blocking C-ABI call, best of reps): the exact
-    FP32 transfer matrix (R_s, R_p, T_s, T_p) and the tensor-core surrogate."""
+    """Film evaluations per second on device-resident batches of n queries (wall time
+    of the blocking C-ABI call, best of reps): the exact FP32 form (R_s, R_p, T_s,
+    T_p), the FP64 transfer matrix (the reference's arithmetic) and the tensor-core
+    surrogate."""
     import torch
 
     g = torch.Generator(device=f"cuda:{local}").manual_seed(7)
@@ -295,17 +296,20 @@ def film_queries(ctx, local: int, n: int = 1 << 24, reps: int = 5) -> dict:
     hi = torch.tensor([780.0, 1.0, 850.0, 1.8, 2.0], device=f"cuda:{local}")
     q = lo + (hi - lo) * torch.rand((n, 5), generator=g, device=f"cuda:{local}")
     out = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
+    out64 = torch.empty((n, 4), dtype=torch.float64, device=f"cuda:{local}")
     res = {}
-    for name, fn in (("exact_tmm", ctx.thinfilm_exact), ("surrogate", ctx.surrogate_eval)):
+    for name, fn, o in (("exact_tmm", ctx.thinfilm_exact, out), ("exact_fp64_tmm", ctx.thinfilm_fp64, out64),
+                        ("surrogate", ctx.surrogate_eval, out)):
         best = float("inf")
         for _ in range(reps + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            fn(q, out)
+            fn(q, o)
             t1 = time.perf_counter()
             best = min(best, t1 - t0)
         res[f"{name}_queries_per_s"] = n / best
     res["surrogate_over_exact"] = res["surrogate_queries_per_s"] / res["exact_tmm_queries_per_s"]
+    res["surrogate_over_fp64"] = res["surrogate_queries_per_s"] / res["exact_fp64_tmm_queries_per_s"]
     res["batch"] = n
     return res
 
