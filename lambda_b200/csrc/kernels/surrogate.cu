@@ -70,13 +70,18 @@ constexpr int sB2 = sW4 + kOutPad * kH * 2;      // [64][8]: (b2 hi, b2 lo, 0, .
 constexpr int sB3 = sB2 + kH * 16;               // [64][8]
 constexpr int sB4 = sB3 + kH * 16;               // [16][8]
 constexpr int kPackedWeightBytes = sB4 + kOutPad * 16;  // the weight image, copied as is
-constexpr int sHid = kPackedWeightBytes;         // [128][64]; the layer-1 operand [128][16] overlays its start
-constexpr int sOnes = sHid + kTileM * kH * 2;    // [128][8]: (1, 1, 0, ...)
+constexpr int sOnes = kPackedWeightBytes;        // [128][8]: (1, 1, 0, ...), shared by the warpgroups
 constexpr int sZero = sOnes + kTileM * 16;       // [128][8] zeros
-constexpr int sBar = sZero + kTileM * 16;
-constexpr int sTmem = sBar + 8;
-constexpr int kSmemBytes = sTmem + 8;
-constexpr int kTmemCols = 64;
+constexpr int sAct = sZero + kTileM * 16;        // G activation tiles [128][64]; each layer-1 operand
+constexpr int kActBytes = kTileM * kH * 2;       //   [128][16] overlays the start of its tile
+// A CTA of G warpgroups: each runs its own stream of 128-row tiles with its own
+// activation tile, mbarrier and kTmemCols TMEM columns; the weights are shared.
+template <int G> constexpr int kBarOf = sAct + G * kActBytes;
+template <int G> constexpr int kTmemSlotOf = kBarOf<G> + 8 * G;
+template <int G> constexpr int kSmemOf = kTmemSlotOf<G> + 8;
+constexpr int kSmemBytes = kSmemOf<1>;
+constexpr int kTmemCols = 64;  // per warpgroup
+constexpr int kQueryWarpgroups = 4;  // warpgroups per CTA of the batched query kernel
 
 // Input normalisation to [-1, 1] over the trained box.
 struct Range {
@@ -227,19 +232,41 @@ __device__ __forceinline__ void put8(uint8_t *smem, int base, int r, int c, int 
     *reinterpret_cast<uint4 *>(smem + base + core_offset(r, c * 8, K)) = *reinterpret_cast<uint4 *>(p);
 }
 
-// Sets up one CTA of a tensor-core MLP kernel: the weight image and the constant
-// (1, 1) and zero blocks into shared memory, the completion mbarrier, and
-// kTmemCols TMEM columns (warp 0 allocates).
+// Named barrier of one warpgroup (ids 1..G; 0 is __syncthreads).
+__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+// AND of a predicate over one warpgroup, as a barrier.
+__device__ __forceinline__ bool wg_sync_and(int id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 q, %1, 0;\n\t"
+        "barrier.cta.red.and.pred p, %2, 128, q;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r)
+        : "r"(uint32_t(v)), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
+// One warpgroup's slot in a CTA of the tensor-core MLP kernels.
 struct TileCtx {
     uint32_t base;       // shared-memory address of smem[0]
-    uint32_t bar;        // MMA completion mbarrier
-    uint32_t tmem;       // TMEM accumulator base (lane 0, column 0)
-    uint32_t lane_base;  // this warp's 32 TMEM lanes
+    int act;             // byte offset of this warpgroup's activation tile
+    uint32_t bar;        // its MMA completion mbarrier
+    uint32_t tmem;       // its TMEM accumulator (lane 0, first of its kTmemCols columns)
+    uint32_t lane_base;  // this warp's 32 TMEM lanes of it
     uint32_t phase;
+    int sync_id;         // its named barrier
+    int row;             // this thread's row in the warpgroup's tiles (0..127)
 };
 
+// Sets up one CTA of G warpgroups: the weight image and the constant (1, 1) and zero
+// blocks into shared memory, one completion mbarrier per warpgroup, and G *
+// kTmemCols TMEM columns (warp 0 allocates).
+template <int G>
 __device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__restrict__ packed) {
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7;
     for (int i = tid; i < kPackedWeightBytes / 16; i += blockDim.x) reinterpret_cast<uint4 *>(smem)[i] = packed[i];
     constexpr uint32_t kOneOne = 0x3F803F80u;  // bf16 (1, 1)
     for (int r = tid; r < kTileM; r += blockDim.x) {
@@ -248,16 +275,19 @@ __device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__rest
     }
     TileCtx t;
     t.base = smem_u32(smem);
-    t.bar = smem_u32(smem + sBar);
+    t.act = sAct + wg * kActBytes;
+    t.bar = smem_u32(smem + kBarOf<G> + 8 * wg);
     t.phase = 0;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + sTmem);
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(t.bar) : "memory");
+    t.sync_id = 1 + wg;
+    t.row = tid & 127;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kTmemSlotOf<G>);
+    if (tid < G) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(smem + kBarOf<G> + 8 * tid)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(kTmemCols)
+                     "r"(G * kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -265,41 +295,58 @@ __device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__rest
     fence_before();
     __syncthreads();
     fence_after();
-    t.tmem = *tmem_slot;
-    t.lane_base = t.tmem + (uint32_t(warp * 32) << 16);
+    t.tmem = *tmem_slot + uint32_t(wg * kTmemCols);
+    t.lane_base = t.tmem + (uint32_t((warp & 3) * 32) << 16);
     return t;
 }
 
+template <int G>
 __device__ __forceinline__ void tile_teardown(const TileCtx &t) {
     // every TMEM read has completed (tcgen05.ld waits) before the columns are released
     fence_before();
     __syncthreads();
     fence_after();
     if ((threadIdx.x >> 5) == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem - uint32_t((threadIdx.x >> 7) * kTmemCols)),
+                     "r"(G * kTmemCols)
+                     : "memory");
 }
 
-// Four layers over the 128-row operand already stored by put_row (row r = thread r).
-// One CTA barrier per layer: the operand rows are in shared memory, then thread 0
-// issues the layer's MMAs and commits them to the mbarrier every thread waits on.
-// The hidden epilogue is two 32-column TMEM loads, 32 ReLU+BF16 conversions and
-// eight 16-byte stores of the next operand row. On return y holds this thread's four
-// outputs. Returns false, uniformly across the CTA, if an MMA completion wait timed
-// out (the accumulator is then not read as valid).
+// ReLU + BF16 of 32 accumulator columns of this thread's row, stored as columns
+// col0 .. col0 + 31 of the next layer's operand.
+__device__ __forceinline__ void store_relu32(uint8_t *smem, const TileCtx &t, const uint32_t (&a)[32], int col0) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const uint4 v = make_uint4(relu_bf16x2(a[8 * c], a[8 * c + 1]), relu_bf16x2(a[8 * c + 2], a[8 * c + 3]),
+                                   relu_bf16x2(a[8 * c + 4], a[8 * c + 5]), relu_bf16x2(a[8 * c + 6], a[8 * c + 7]));
+        *reinterpret_cast<uint4 *>(smem + t.act + core_offset(t.row, col0 + 8 * c, kH)) = v;
+    }
+}
+
+// Four layers over the 128-row operand put_row stored for this warpgroup. One
+// warpgroup barrier per layer: the operand rows are in shared memory, then the
+// warpgroup's first thread issues the layer's MMAs and commits them to the mbarrier
+// every thread of the warpgroup waits on. The hidden epilogue is two 32-column TMEM
+// loads, 32 ReLU+BF16 conversions and eight 16-byte stores of the next operand row
+// (kLowRegs: one 32-column half at a time, for kernels held to 64 registers). On
+// return y holds this thread's four outputs. Returns false, uniformly across the
+// warpgroup, if an MMA completion wait timed out (the accumulator is then not read
+// as valid).
+template <bool kLowRegs = false>
 __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
-    const int tid = threadIdx.x;
     const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
     const uint32_t kPoll = 1u << 22;
+    const uint32_t act = t.base + uint32_t(t.act);
     bool done = true;
 #pragma unroll 1
     for (int layer = 0; layer < 4; layer++) {
         fence_proxy_async();
         fence_before();
-        __syncthreads();
-        if (tid == 0) {
+        wg_sync(t.sync_id);
+        if (t.row == 0) {
             fence_after();
             if (layer == 0) {
-                mma_bf16(t.tmem, smem_desc(t.base + sHid, 128, 256), smem_desc(t.base + sW1, 128, 256), id64, 0);
+                mma_bf16(t.tmem, smem_desc(act, 128, 256), smem_desc(t.base + sW1, 128, 256), id64, 0);
             } else {
                 const int wofs = layer == 1 ? sW2 : (layer == 2 ? sW3 : sW4);
                 const int bofs = layer == 1 ? sB2 : (layer == 2 ? sB3 : sB4);
@@ -309,8 +356,8 @@ __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
                          smem_desc(t.base + bofs, sZero - bofs, 128), idesc, 0);
 #pragma unroll
                 for (int kk = 0; kk < kH / 16; kk++)
-                    mma_bf16(t.tmem, smem_desc(t.base + sHid + kk * 256, 128, 1024),
-                             smem_desc(t.base + wofs + kk * 256, 128, 1024), idesc, 1);
+                    mma_bf16(t.tmem, smem_desc(act + kk * 256, 128, 1024), smem_desc(t.base + wofs + kk * 256, 128, 1024),
+                             idesc, 1);
             }
             mma_commit(t.bar);
         }
@@ -318,24 +365,22 @@ __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
         t.phase ^= 1u;
         fence_after();
         if (layer < 3) {
-            uint32_t a[32], b[32];
-            tmem_ld32(t.lane_base, a);
-            tmem_ld32(t.lane_base + 32, b);
-            tmem_wait(a);
-            tmem_after_wait(b);
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const uint4 v = make_uint4(relu_bf16x2(a[8 * c], a[8 * c + 1]), relu_bf16x2(a[8 * c + 2], a[8 * c + 3]),
-                                           relu_bf16x2(a[8 * c + 4], a[8 * c + 5]),
-                                           relu_bf16x2(a[8 * c + 6], a[8 * c + 7]));
-                *reinterpret_cast<uint4 *>(smem + sHid + core_offset(tid, 8 * c, kH)) = v;
-            }
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const uint4 v = make_uint4(relu_bf16x2(b[8 * c], b[8 * c + 1]), relu_bf16x2(b[8 * c + 2], b[8 * c + 3]),
-                                           relu_bf16x2(b[8 * c + 4], b[8 * c + 5]),
-                                           relu_bf16x2(b[8 * c + 6], b[8 * c + 7]));
-                *reinterpret_cast<uint4 *>(smem + sHid + core_offset(tid, 32 + 8 * c, kH)) = v;
+            if constexpr (kLowRegs) {
+                uint32_t a[32];
+                tmem_ld32(t.lane_base, a);
+                tmem_wait(a);
+                store_relu32(smem, t, a, 0);
+                tmem_ld32(t.lane_base + 32, a);
+                tmem_wait(a);
+                store_relu32(smem, t, a, 32);
+            } else {
+                uint32_t a[32], b[32];
+                tmem_ld32(t.lane_base, a);
+                tmem_ld32(t.lane_base + 32, b);
+                tmem_wait(a);
+                tmem_after_wait(b);
+                store_relu32(smem, t, a, 0);
+                store_relu32(smem, t, b, 32);
             }
         } else {
             uint32_t o[4];
@@ -344,34 +389,37 @@ __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
             for (int i = 0; i < kOut; i++) y[i] = __uint_as_float(o[i]);
         }
     }
-    return __syncthreads_and(done) != 0;
+    return wg_sync_and(t.sync_id, done);
 }
 
 // Stores one encoded row (5 features, then the two constant-1 bias columns, zero
-// padded to K = 16) as row r of the layer-1 operand.
-__device__ __forceinline__ void put_row(uint8_t *smem, int r, const float *e) {
+// padded to K = 16) as this thread's row of its warpgroup's layer-1 operand.
+__device__ __forceinline__ void put_row(uint8_t *smem, const TileCtx &t, const float *e) {
     float x[16];
 #pragma unroll
     for (int i = 0; i < 16; i++) x[i] = i < kIn ? e[i] : (i < kIn + 2 ? 1.0f : 0.0f);
-    put8(smem, sHid, r, 0, kInPad, x);
-    put8(smem, sHid, r, 1, kInPad, x + 8);
+    put8(smem, t.act, t.row, 0, kInPad, x);
+    put8(smem, t.act, t.row, 1, kInPad, x + 8);
 }
 
 // Inference over `rows` rows: row i's input is kRowStride floats already encoded
 // (kQueries = false) or the i-th lambda_film_query, encoded here (kQueries = true).
-// out: rows x (R_s, R_p, T_s, T_p). Error bit 1 is set if an MMA completion wait
-// timed out.
-template <bool kQueries>
-__global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed, const void *__restrict__ in, int rows,
-                                                Range rg, float4 *__restrict__ out, int *error) {
+// out: rows x (R_s, R_p, T_s, T_p). A CTA holds G warpgroups, each working through
+// its own 128-row tiles with its own accumulator, so G dependent layer chains
+// overlap per CTA while the weights are loaded once. Error bit 1 is set if an MMA
+// completion wait timed out.
+template <bool kQueries, int G>
+__global__ void __launch_bounds__(128 * G, G == 1 ? 1 : 8 / G) k_mlp_tc(const uint4 *__restrict__ packed,
+                                                                   const void *__restrict__ in, int rows, Range rg,
+                                                                   float4 *__restrict__ out, int *error) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    const int tid = threadIdx.x;
     const int tiles = (rows + kTileM - 1) / kTileM;
-    if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
-    TileCtx t = tile_setup(smem, packed);
+    if (int(blockIdx.x) * G >= tiles) return;  // uniform per block, before any TMEM allocation
+    TileCtx t = tile_setup<G>(smem, packed);
     bool ok = true;
-    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const int row = tile * kTileM + tid;
+    const int wg = threadIdx.x >> 7;
+    for (int tile = blockIdx.x * G + wg; tile < tiles && ok; tile += gridDim.x * G) {
+        const int row = tile * kTileM + t.row;
         float e[kIn] = {0, 0, 0, 0, 0};
         if (row < rows) {
             if constexpr (kQueries) {
@@ -388,13 +436,13 @@ __global__ void __launch_bounds__(128) k_mlp_tc(const uint4 *__restrict__ packed
                 e[4] = x[4];
             }
         }
-        put_row(smem, tid, e);
+        put_row(smem, t, e);
         float y[kOut];
-        ok = mlp_tile(smem, t, y);
+        ok = mlp_tile<(G > 2)>(smem, t, y);
         if (ok && row < rows) out[row] = make_float4(y[0], y[1], y[2], y[3]);
     }
-    if (!ok && tid == 0) atomicOr(error, 2);
-    tile_teardown(t);
+    if (!ok && t.row == 0) atomicOr(error, 2);
+    tile_teardown<G>(t);
 }
 
 // ---------------------------------------------------------------------------
@@ -583,7 +631,7 @@ __global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams 
     if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
     const int *q = ps.mat_queue[2];
     int *q_next = ps.queue[(bounce + 1) & 1];
-    TileCtx t = tile_setup(smem, packed);
+    TileCtx t = tile_setup<1>(smem, packed);
     bool ok_tc = true;
     for (int tile = blockIdx.x; tile < tiles && ok_tc; tile += gridDim.x) {
         const int idx = tile * kTileM + tid;
@@ -624,7 +672,7 @@ __global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams 
                 float row[kIn];
 #pragma unroll
                 for (int k = 0; k < kIn; k++) row[k] = ok ? e[w][k] : 0.0f;
-                put_row(smem, tid, row);
+                put_row(smem, t, row);
                 float y[kOut];
                 ok_tc = mlp_tile(smem, t, y);
                 R.v[w] = clampf((y[0] + y[1]) * 0.5f, 0.0f, 1.0f);
@@ -649,7 +697,7 @@ __global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams 
         warp_push(&ps.counts[queue_slot(bounce, kQFilmFallback)], valid && ok_tc && !ok);
     }
     if (!ok_tc && tid == 0) atomicOr(ps.error, 2);
-    tile_teardown(t);
+    tile_teardown<1>(t);
 }
 
 // Host: the FP32 parameters as the BF16 shared-memory image of the MLP kernels
@@ -704,9 +752,10 @@ bool range_ok(const lambda_film_range &r) {
 // Dynamic shared memory of the MLP kernels (below the 48 KB default today; set so
 // that a larger layout needs no other change).
 cudaError_t configure_mlp_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    constexpr int G = kQueryWarpgroups;
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_tc<false, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOf<G>);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        e = cudaFuncSetAttribute(k_mlp_tc<true, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOf<G>);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_film_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     return e;
@@ -746,17 +795,25 @@ lambda_status install(lambda_ctx *ctx, const float *params_host, const lambda_fi
     return LAMBDA_OK;
 }
 
-// Resident CTAs per SM of the tensor-core MLP kernels, capped so their TMEM
-// columns fit the SM's 512 and no allocation ever waits. Computed outside stream
-// capture and cached on the context.
+// Resident CTAs per SM of the render's surrogate kernel (one warpgroup each),
+// capped so their TMEM columns fit the SM's 512 and no allocation ever waits.
+// Computed outside stream capture and cached on the context.
 int mlp_grid(lambda_ctx *ctx) {
     if (ctx->mlp_ctas_per_sm <= 0) {
-        const int per_sm = std::min({resident_ctas((const void *)k_mlp_tc<false>, ctx->device, 128, kSmemBytes),
-                                     resident_ctas((const void *)k_mlp_tc<true>, ctx->device, 128, kSmemBytes),
-                                     resident_ctas((const void *)k_film_fused, ctx->device, 128, kSmemBytes)});
+        const int per_sm = resident_ctas((const void *)k_film_fused, ctx->device, 128, kSmemBytes);
         ctx->mlp_ctas_per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
     }
     return ctx->mlp_ctas_per_sm * ctx->sm_count;
+}
+
+// Grid of the batched query kernel (kQueryWarpgroups warpgroups per CTA) for
+// `tiles` 128-row tiles: resident CTAs per SM, capped by TMEM, on every SM.
+template <bool kQueries>
+int query_grid(lambda_ctx *ctx, int tiles) {
+    constexpr int G = kQueryWarpgroups;
+    const int per_sm = std::min(resident_ctas((const void *)k_mlp_tc<kQueries, G>, ctx->device, 128 * G, kSmemOf<G>),
+                                512 / (G * kTmemCols));
+    return std::max(1, std::min((tiles + G - 1) / G, std::max(1, per_sm) * ctx->sm_count));
 }
 
 // Runs the MLP over n_rows encoded rows (kQueries = false) or film queries
@@ -769,9 +826,9 @@ lambda_status run_mlp(lambda_ctx *ctx, const void *in, int n_rows, float4 *out_d
     CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
     const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
     const int tiles = (n_rows + kTileM - 1) / kTileM;
-    const int grid = std::max(1, std::min(tiles, mlp_grid(ctx)));
-    k_mlp_tc<kQueries><<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w), in, n_rows,
-                                                               to_range(ctx->surrogate_range), out_dev, err);
+    constexpr int G = kQueryWarpgroups;
+    k_mlp_tc<kQueries, G><<<query_grid<kQueries>(ctx, tiles), 128 * G, kSmemOf<G>, ctx->stream>>>(
+        reinterpret_cast<const uint4 *>(w), in, n_rows, to_range(ctx->surrogate_range), out_dev, err);
     CK(cudaGetLastError(), "launch MLP kernel");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");
@@ -1098,8 +1155,8 @@ extern "C" lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lam
     k_encode_queries<<<(n + 255) / 256, 256, 0, ctx->stream>>>(queries, n, to_range(ctx->surrogate_range), sc.rows);
     const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
     const int tiles = (n + kTileM - 1) / kTileM;
-    const int grid = std::max(1, std::min(tiles, mlp_grid(ctx)));
-    k_mlp_tc<false><<<grid, 128, kSmemBytes, ctx->stream>>>(reinterpret_cast<const uint4 *>(w), sc.rows, n, Range{},
+    constexpr int G = kQueryWarpgroups;
+    k_mlp_tc<false, G><<<query_grid<false>(ctx, tiles), 128 * G, kSmemOf<G>, ctx->stream>>>(reinterpret_cast<const uint4 *>(w), sc.rows, n, Range{},
                                                             reinterpret_cast<float4 *>(out), sc.error);
     CK(cudaGetLastError(), "launch MLP kernel");
     int herr = 0;
