@@ -390,8 +390,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
     ap.add_argument("--no-compare", action="store_true", help="skip the surrogate/exact comparison")
-    ap.add_argument("--workload", default="thinfilm1080p", choices=["thinfilm1080p", "batch32"],
-                    help="batch32: 32 random-pose views of the thin-film scene in one batched render")
+    ap.add_argument("--workload", default="thinfilm1080p", choices=["thinfilm1080p", "batch32", "film_queries"],
+                    help="batch32: 32 random-pose views of the thin-film scene in one batched render; "
+                         "film_queries: the three film evaluators on 2^24 device-resident queries")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -429,6 +430,16 @@ def main():
     paths_per_step = W * H * args.spp
     if args.workload == "batch32":
         return run_batch(args, ctx, scene, lb, torch, rank, world, local)
+    if args.workload == "film_queries":
+        if rank == 0:
+            fq = film_queries(ctx, local)
+            print(json.dumps({"metric": "thin-film evaluations/sec (R_s, R_p, T_s, T_p per query)",
+                              "value": fq["surrogate_queries_per_s"], "unit": "queries/s", "n_gpus": world,
+                              "higher_is_better": True, "data": "synthetic",
+                              "config": {"workload": "2^24 uniform queries over the trained box, device-resident"},
+                              "film_queries": fq}))
+        ctx.close()
+        return 0
 
     # launch shapes from the autotuner, timed on a 1-spp frame of the same scene
     tuning = ctx.autotune(scene.render_desc(seed=sc.seed, flags=flags, samples=1))
