@@ -71,3 +71,31 @@ def test_fp64_thin_film_render(scene_dir, ctx):
     assert same64 >= same32
     with pytest.raises(lb.LambdaError):
         ctx.render(scene.render_desc(seed=sc.seed, flags=lb.RENDER_THINFILM_FP64 | lb.RENDER_THINFILM_SURROGATE))
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference harness not built")
+def test_cli_drop_in_matches_reference(scene_dir, ctx):
+    """The command-line renderer (main.cpp's replacement): same progress lines and a
+    PPM, rendered with seed 42, within one 8-bit level of the reference's CPU render
+    written by the reference's own PPM writer."""
+    import os
+    import subprocess
+
+    sc = scenes.cornell(scene_dir, 64, 64, 16, name="cli_cornell.lrd")
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lambda_b200", "bin", "lambda")
+    out = os.path.join(scene_dir, "cli_cornell.ppm")
+    r = subprocess.run([exe, sc.lrd, out], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.rstrip().endswith(f"{exe}: 100% complete")
+    want_path = os.path.join(scene_dir, "cli_cornell_ref.ppm")
+    ref.write_ppm(want_path, ref_scene(sc.lrd).render(42)[0])
+
+    def read(p):
+        tok = open(p).read().split()
+        assert tok[0] == "P3" and tok[1:4] == ["64", "64", "255"]
+        return np.array(tok[4:], dtype=np.int32)
+
+    got, want = read(out), read(want_path)
+    diff = np.abs(got - want)
+    print(f"CLI PPM: {float((diff == 0).mean()):.4f} of values identical, max difference {int(diff.max())}")
+    assert diff.max() <= 1 and (diff == 0).mean() > 0.99
