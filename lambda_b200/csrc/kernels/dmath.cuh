@@ -91,6 +91,7 @@ __device__ __forceinline__ f3 xform(const float *m, f3 v, float w) {
     if (fabsf(den) < kEps) den = 1;
     const f3 r = mk(m[0] * v.x + m[1] * v.y + m[2] * v.z + m[3] * w, m[4] * v.x + m[5] * v.y + m[6] * v.z + m[7] * w,
                     m[8] * v.x + m[9] * v.y + m[10] * v.z + m[11] * w);
+    if (den == 1.0f) return r;  // x / 1 is x exactly: affine transforms skip the divide
     return r / den;
 }
 
@@ -100,6 +101,7 @@ __device__ __forceinline__ f3 xform_t(const float *m, f3 v, float w) {
     if (fabsf(den) < kEps) den = 1;
     const f3 r = mk(m[0] * v.x + m[4] * v.y + m[8] * v.z + m[12] * w, m[1] * v.x + m[5] * v.y + m[9] * v.z + m[13] * w,
                     m[2] * v.x + m[6] * v.y + m[10] * v.z + m[14] * w);
+    if (den == 1.0f) return r;
     return r / den;
 }
 
