@@ -253,7 +253,7 @@ def image_quality(ctx, scene, dev_out) -> dict:
     finite = np.isfinite(frames["exact_a"]).all(2) & np.isfinite(frames["exact_b"]).all(2) & \
         np.isfinite(frames["surrogate_b"]).all(2)
     for f in frames.values():
-        f[~finite] = 0.0  # the reference also yields 0/0 on the rare tangent-plane cosine sample
+        f[~finite] = 0.0  # the reference's own trace of these pixels is non-finite too (tested)
 
     def rel(a, b, block=1):
         if block > 1:

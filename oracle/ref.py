@@ -38,6 +38,7 @@ def load():
         lib.ref_render.argtypes = [P, C.c_uint64, C.c_int, P]
         lib.ref_max_threads.restype = C.c_int
         lib.ref_trace_sample.argtypes = [P, C.c_uint64, C.c_int, C.c_int, C.c_int, P, P]
+        lib.ref_trace_pixel.argtypes = [P, C.c_uint64, C.c_int, C.c_int, P]
         lib.ref_hit.argtypes = [P, P, C.c_int, P, P, P, P, P]
         lib.ref_shadow.argtypes = [P, P, P, P, C.c_int, P]
         lib.ref_thinfilm.restype = C.c_float
@@ -177,6 +178,13 @@ class RefScene:
         lam = np.zeros(4, np.float32)
         self.lib.ref_trace_sample(self.h, seed, px, py, sample, rad.ctypes.data, lam.ctypes.data)
         return rad, lam
+
+    def trace_pixel(self, seed, px, py):
+        """Every sample's radiance (4 hero wavelengths) of one pixel, in order."""
+        n = self.settings()["samples"]
+        rad = np.zeros((n, 4), np.float32)
+        self.lib.ref_trace_pixel(self.h, seed, px, py, rad.ctypes.data)
+        return rad
 
     def thinfilm(self, material, normal, front, point, d, lam) -> float:
         n = np.ascontiguousarray(normal, np.float32)

@@ -240,6 +240,29 @@ void ref_trace_sample(void *p, uint64_t seed, int px, int py, int sample, float 
         }
 }
 
+// Renderer::renderPixel's samples of pixel (px, py) one by one: radiance_out
+// [samples][4] holds each sample's spectrum at its 4 hero wavelengths, before the
+// film average.
+void ref_trace_pixel(void *p, uint64_t seed, int px, int py, float *radiance_out) {
+    auto &s = *static_cast<RefScene *>(p);
+    wire(s);
+    const Renderer &r = s.renderer;
+    Random state(seed, uint64_t(py) * uint64_t(r.width) + uint64_t(px));
+    int k = 0;
+    for (int i = 0; i < r.sqrtSamples; i++)
+        for (int j = 0; j < r.sqrtSamples; j++, k++) {
+            Float u = (Float(px) + (Float(i) + randomFloat(state)) / Float(r.sqrtSamples)) / Float(r.width);
+            Float v = (Float(py) + (Float(j) + randomFloat(state)) / Float(r.sqrtSamples)) / Float(r.height);
+            Float lambda = r.lambdaMin + randomFloat(state) * (r.lambdaMax - r.lambdaMin);
+            SampledSpectrum lambdas;
+            for (int h = 0; h < HERO_COUNT; h++)
+                lambdas[h] = r.lambdaMin + fmodF(lambda - r.lambdaMin + Float(h) * r.lambdaRange / HERO_COUNT, r.lambdaRange);
+            Ray ray = r.camera.getRay(u, v, lambdas);
+            SampledSpectrum spectrum = r.trace(ray, state);
+            for (int h = 0; h < HERO_COUNT; h++) radiance_out[4 * k + h] = spectrum[h];
+        }
+}
+
 // Scene::hit closest-hit queries. rays: [n][6].
 void ref_hit(void *p, const float *rays, int n, int32_t *inst, int32_t *obj, float *t, float *pn /* [n][8]: point, normal, u, v */, int32_t *front) {
     auto &s = *static_cast<RefScene *>(p);

@@ -99,3 +99,22 @@ def test_cli_drop_in_matches_reference(scene_dir, ctx):
     diff = np.abs(got - want)
     print(f"CLI PPM: {float((diff == 0).mean()):.4f} of values identical, max difference {int(diff.max())}")
     assert diff.max() <= 1 and (diff == 0).mean() > 0.99
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference harness not built")
+def test_non_finite_pixels_are_the_references(scene_dir, ctx):
+    """The benchmark frame (1920x1080, 256 spp, seed 3) has a few dozen non-finite
+    pixels. Each one is non-finite in the reference's own trace of that pixel with
+    the same random streams: the NaN comes from the reference's algorithm (a 0/0 on
+    rare samples), and the renderer reproduces it rather than adding any."""
+    sc = scenes.thinfilm_spheres(scene_dir, 1920, 1080, 256, name="nan_thinfilm.lrd")
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx.upload(scene)
+    img = ctx.render(scene.render_desc(seed=sc.seed))
+    bad = np.argwhere(~np.isfinite(img).all(axis=2))
+    print(f"non-finite pixels: {len(bad)} of {img.shape[0] * img.shape[1]}")
+    assert 0 < len(bad) < 1000
+    r = ref_scene(sc.lrd)
+    for py, px in bad:
+        rad = r.trace_pixel(sc.seed, int(px), int(py))
+        assert not np.isfinite(rad).all(), f"pixel ({px}, {py}) is finite in the reference"
