@@ -1,11 +1,11 @@
 // GPU half of the C ABI (include/lambda_gpu.h): context, scene upload, the
 // wavefront render loop, ray queries and thin-film queries.
 //
-// A render is a sequence of sample waves (wavefront.cuh). One wave's kernels
-// (prologue, raygen, then intersect/shade/shadow per bounce) are captured once
-// into a CUDA graph and replayed `samples` times, so the host issues one graph
-// launch per wave; kernels read queue sizes from device counters and exit early
-// when their queue is empty.
+// A render pass is one CUDA graph launch (render_pass): clear + init, a conditional
+// while node whose body is one sample wave (wavefront.cuh: prologue, raygen, then
+// per bounce intersect followed by the material branches, run in parallel), then the
+// film average. Kernels read queue sizes from device counters and exit early when
+// their queue is empty.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -122,6 +122,19 @@ extern "C" lambda_status lambda_ctx_create(int32_t device, lambda_ctx **out) {
     }
     cudaEventCreate(&ctx->ev_start);
     cudaEventCreate(&ctx->ev_stop);
+    for (int i = 0; i < 2; i++) {
+        e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            g_create_error = std::string("cudaStreamCreate failed (") + cudaGetErrorString(e) + ")";
+            return LAMBDA_ERR_CUDA;
+        }
+    }
+    e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("cudaEventCreate failed (") + cudaGetErrorString(e) + ")";
+        return LAMBDA_ERR_CUDA;
+    }
     *out = ctx.release();
     return LAMBDA_OK;
 }
@@ -134,6 +147,11 @@ lambda_ctx::~lambda_ctx() {
     for (DeviceBuffer *b : all_buffers()) b->release();
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    for (int i = 0; i < 2; i++) {
+        if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+        if (side[i]) cudaStreamDestroy(side[i]);
+    }
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -748,18 +766,23 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         else if (bw == 4) k_intersect<4><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
         else k_intersect<8><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
     };
-    auto shadow = [&](int b) {
-        if (bw == 2) k_shadow<2><<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps);
-        else if (bw == 4) k_shadow<4><<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps);
-        else k_shadow<8><<<g_shadow, tb, stack_smem, stream>>>(b, rp, sc, ps);
+    auto shadow = [&](int b, cudaStream_t s) {
+        if (bw == 2) k_shadow<2><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
+        else if (bw == 4) k_shadow<4><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
+        else k_shadow<8><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
     };
     const int g_lambert = grid((const void *)k_shade_lambert, sb, 0);
     const int g_spec = grid((const void *)k_shade_specular, sb, 0);
     const int g_film = grid(fp64 ? (const void *)k_shade_film_exact<true> : (const void *)k_shade_film_exact<false>, sb, 0);
     const int pix_blocks = (P + 255) / 256;
 
-    // One wave's launches. With a profiler every launch is bracketed by events.
-    // Inside the pass graph's loop the prologue sets the loop condition.
+    // One wave's launches. With a profiler every launch is bracketed by events, in
+    // order on the library stream. Inside the pass graph's loop the prologue sets the
+    // loop condition, and a bounce's shading runs as parallel branches: Lambertian
+    // shade then its shadow rays, mirror/dielectric shade, thin-film shade. They touch
+    // disjoint paths (each path is in one material queue), so only the queue order
+    // depends on their interleaving, and the next intersect waits for all of them.
+    cudaError_t fork_err = cudaSuccess;
     auto wave = [&](StageProfiler *pr, cudaGraphConditionalHandle loop, int waves) -> int {
         int n = 0;
         auto timed = [&](int stage, auto &&launch) {
@@ -770,16 +793,41 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         };
         timed(1, [&] { k_wave_prologue<<<1, 256, 0, stream>>>(d_max, ps, loop, waves, ctx->progress_dev); });
         timed(2, [&] { k_raygen<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
+        // branch k: 0 Lambertian + shadow, 1 specular, 2 thin film
+        auto branch = [&](int k, int b, cudaStream_t s) {
+            if (k == 0) {
+                timed(4, [&] { k_shade_lambert<<<g_lambert, sb, 0, s>>>(b, rp, sc, ps); });
+                timed(7, [&] { shadow(b, s); });
+            } else if (k == 1) {
+                timed(5, [&] { k_shade_specular<<<g_spec, sb, 0, s>>>(b, rp, sc, ps); });
+            } else if (surrogate) {
+                n += ctx->launch_shade_surrogate(b, rp, sc, ps, pr, s);
+            } else if (fp64) {
+                timed(6, [&] { k_shade_film_exact<true><<<g_film, sb, 0, s>>>(b, rp, sc, ps); });
+            } else {
+                timed(6, [&] { k_shade_film_exact<false><<<g_film, sb, 0, s>>>(b, rp, sc, ps); });
+            }
+        };
+        int branches[3], nb = 0;
+        for (int k = 0; k < 3; k++)
+            if (sc.families & (1u << k)) branches[nb++] = k;
         for (int b = 0; b <= d_max; b++) {
             timed(3, [&] { intersect(b); });
-            if (sc.families & 1u) timed(4, [&] { k_shade_lambert<<<g_lambert, sb, 0, stream>>>(b, rp, sc, ps); });
-            if (sc.families & 2u) timed(5, [&] { k_shade_specular<<<g_spec, sb, 0, stream>>>(b, rp, sc, ps); });
-            if (sc.families & 4u) {
-                if (surrogate) n += ctx->launch_shade_surrogate(b, rp, sc, ps, pr);
-                else if (fp64) timed(6, [&] { k_shade_film_exact<true><<<g_film, sb, 0, stream>>>(b, rp, sc, ps); });
-                else timed(6, [&] { k_shade_film_exact<false><<<g_film, sb, 0, stream>>>(b, rp, sc, ps); });
+            if (pr || nb < 2) {
+                for (int i = 0; i < nb; i++) branch(branches[i], b, stream);
+                continue;
             }
-            if (sc.families & 1u) timed(7, [&] { shadow(b); });
+            auto keep = [&](cudaError_t e) {
+                if (fork_err == cudaSuccess) fork_err = e;
+            };
+            keep(cudaEventRecord(ctx->ev_fork, stream));
+            for (int i = 1; i < nb; i++) {
+                keep(cudaStreamWaitEvent(ctx->side[i - 1], ctx->ev_fork, 0));
+                branch(branches[i], b, ctx->side[i - 1]);
+                keep(cudaEventRecord(ctx->ev_join[i - 1], ctx->side[i - 1]));
+            }
+            branch(branches[0], b, stream);
+            for (int i = 1; i < nb; i++) keep(cudaStreamWaitEvent(stream, ctx->ev_join[i - 1], 0));
         }
         return n;
     };
@@ -860,6 +908,7 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         if (e != cudaSuccess) return fail(e, "begin capture of the wave");
         const int wave_launches = wave(nullptr, loop, s_max);
         ce = cudaStreamEndCapture(stream, &body);
+        if (fork_err != cudaSuccess) return fail(fork_err, "capture the wave's branches");
         if (ce != cudaSuccess) return fail(ce, "capture wave");
         e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return fail(e, "begin capture");

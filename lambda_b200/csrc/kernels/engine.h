@@ -64,6 +64,10 @@ struct lambda_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // Branches of a bounce that run beside the main stream's inside the pass graph
+    // (fork and join events, no timing).
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     std::string last_error;
 
     bool has_scene = false;
@@ -97,7 +101,7 @@ struct lambda_ctx {
     lambda_status surrogate_ready();
     lambda_status ensure_surrogate_state();
     int launch_shade_surrogate(int bounce, const lambda_dev::RenderParams &rp, const lambda_dev::DeviceScene &sc,
-                               const lambda_dev::PathState &ps, StageProfiler *prof);
+                               const lambda_dev::PathState &ps, StageProfiler *prof, cudaStream_t s);
 
     std::vector<DeviceBuffer *> all_buffers() {
         SceneBuffers &s = scene;

@@ -232,21 +232,34 @@ __device__ __forceinline__ void put8(uint8_t *smem, int base, int r, int c, int 
     *reinterpret_cast<uint4 *>(smem + base + core_offset(r, c * 8, K)) = *reinterpret_cast<uint4 *>(p);
 }
 
-// Named barrier of one warpgroup (ids 1..G; 0 is __syncthreads).
-__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+// Barrier of warpgroup wg of a CTA of G: the CTA barrier when it is the only one,
+// else named barrier 1 + wg. A barrier id in a register makes ptxas reserve all 16
+// of the CTA's barriers, which limits how many CTAs an SM holds; that is paid only
+// by the multi-warpgroup query kernel (two CTAs per SM), never by the render's
+// single-warpgroup kernel, which runs several CTAs per SM.
+template <int G>
+__device__ __forceinline__ void wg_sync(int wg) {
+    if constexpr (G == 1) __syncthreads();
+    else asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
+}
 
-// AND of a predicate over one warpgroup, as a barrier.
-__device__ __forceinline__ bool wg_sync_and(int id, bool v) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.b32 q, %1, 0;\n\t"
-        "barrier.cta.red.and.pred p, %2, 128, q;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(r)
-        : "r"(uint32_t(v)), "r"(id)
-        : "memory");
-    return r != 0;
+// AND of a predicate over warpgroup wg, as its barrier.
+template <int G>
+__device__ __forceinline__ bool wg_sync_and(int wg, bool v) {
+    if constexpr (G == 1) {
+        return __syncthreads_and(v) != 0;
+    } else {
+        uint32_t r;
+        asm volatile(
+            "{\n\t.reg .pred p, q;\n\t"
+            "setp.ne.b32 q, %1, 0;\n\t"
+            "barrier.cta.red.and.pred p, %2, 128, q;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(r)
+            : "r"(uint32_t(v)), "r"(1 + wg)
+            : "memory");
+        return r != 0;
+    }
 }
 
 // One warpgroup's slot in a CTA of the tensor-core MLP kernels.
@@ -257,7 +270,7 @@ struct TileCtx {
     uint32_t tmem;       // its TMEM accumulator (lane 0, first of its kTmemCols columns)
     uint32_t lane_base;  // this warp's 32 TMEM lanes of it
     uint32_t phase;
-    int sync_id;         // its named barrier
+    int wg;              // its index in the CTA (its barrier, see wg_sync)
     int row;             // this thread's row in the warpgroup's tiles (0..127)
 };
 
@@ -278,7 +291,7 @@ __device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__rest
     t.act = sAct + wg * kActBytes;
     t.bar = smem_u32(smem + kBarOf<G> + 8 * wg);
     t.phase = 0;
-    t.sync_id = 1 + wg;
+    t.wg = wg;
     t.row = tid & 127;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kTmemSlotOf<G>);
     if (tid < G) {
@@ -332,7 +345,7 @@ __device__ __forceinline__ void store_relu32(uint8_t *smem, const TileCtx &t, co
 // return y holds this thread's four outputs. Returns false, uniformly across the
 // warpgroup, if an MMA completion wait timed out (the accumulator is then not read
 // as valid).
-template <bool kLowRegs = false>
+template <int G, bool kLowRegs = false>
 __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
     const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
     const uint32_t kPoll = 1u << 22;
@@ -342,7 +355,7 @@ __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
     for (int layer = 0; layer < 4; layer++) {
         fence_proxy_async();
         fence_before();
-        wg_sync(t.sync_id);
+        wg_sync<G>(t.wg);
         if (t.row == 0) {
             fence_after();
             if (layer == 0) {
@@ -389,7 +402,7 @@ __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
             for (int i = 0; i < kOut; i++) y[i] = __uint_as_float(o[i]);
         }
     }
-    return wg_sync_and(t.sync_id, done);
+    return wg_sync_and<G>(t.wg, done);
 }
 
 // Stores one encoded row (5 features, then the two constant-1 bias columns, zero
@@ -438,7 +451,7 @@ __global__ void __launch_bounds__(128 * G, G == 1 ? 1 : 8 / G) k_mlp_tc(const ui
         }
         put_row(smem, t, e);
         float y[kOut];
-        ok = mlp_tile<(G > 2)>(smem, t, y);
+        ok = mlp_tile<G, (G > 2)>(smem, t, y);
         if (ok && row < rows) out[row] = make_float4(y[0], y[1], y[2], y[3]);
     }
     if (!ok && t.row == 0) atomicOr(error, 2);
@@ -674,7 +687,7 @@ __global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams 
                 for (int k = 0; k < kIn; k++) row[k] = ok ? e[w][k] : 0.0f;
                 put_row(smem, t, row);
                 float y[kOut];
-                ok_tc = mlp_tile(smem, t, y);
+                ok_tc = mlp_tile<1>(smem, t, y);
                 R.v[w] = clampf((y[0] + y[1]) * 0.5f, 0.0f, 1.0f);
             }
         }
@@ -840,7 +853,7 @@ lambda_status run_mlp(lambda_ctx *ctx, const void *in, int n_rows, float4 *out_d
 }  // namespace
 
 int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const DeviceScene &sc, const PathState &ps,
-                                       StageProfiler *prof) {
+                                       StageProfiler *prof, cudaStream_t s) {
     FilmSurrogate fs;
     fs.rg = to_range(surrogate_range);
     fs.lam_lo = surrogate_range.lambda_nm[0];
@@ -855,7 +868,7 @@ int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const
     fs.ns_hi = surrogate_range.n_sub[1];
     const uint8_t *w = static_cast<const uint8_t *>(sbuf.weights_bf16.ptr);
     if (prof) prof->begin(9);
-    k_film_fused<<<mlp_grid(this), 128, kSmemBytes, stream>>>(bounce, rp, sc, ps, fs, reinterpret_cast<const uint4 *>(w));
+    k_film_fused<<<mlp_grid(this), 128, kSmemBytes, s>>>(bounce, rp, sc, ps, fs, reinterpret_cast<const uint4 *>(w));
     if (prof) prof->end();
     return 1;
 }
