@@ -316,9 +316,9 @@ lambda_status lambda_get_render_stats(const lambda_ctx *ctx, lambda_render_stats
 /* Per-stage device time of the last render made with LAMBDA_RENDER_PROFILE_STAGES.
  * Stages: 0 init, 1 wave prologue, 2 raygen, 3 intersect, 4 Lambertian shade,
  * 5 mirror/dielectric shade, 6 thin-film shade (exact), 7 shadow rays, 8 finish,
- * 9 thin-film shade with the surrogate (inputs, tensor-core MLP, the exact transfer
- * matrix for hits outside the surrogate's domain, and scatter, in one kernel),
- * 10 and 11 unused. items = paths or rays the stage processed over
+ * 9-11 thin-film shade with the surrogate: 9 the hits' queries encoded as MLP rows,
+ * 10 the tensor-core MLP, 11 the scatter (with the exact transfer matrix for hits
+ * outside the surrogate's domain). items = paths, rays or hits the stage processed over
  * the whole render. No reference counterpart (the reference's single kernel has
  * no stages). */
 #define LAMBDA_NUM_STAGES 12

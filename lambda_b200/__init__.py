@@ -401,6 +401,10 @@ STAGE_BYTES = {
     "shade_film": 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
     "shadow": 4 + 16 * 3 + 8 + 16 * 2,                     # queue, NEE ray + weights, light ids, radiance rw
     "finish": 16 * 3 + 12,
+    # surrogate thin film: queue, dir, hit, T/lam, then 4 rows of 32 B and a domain flag
+    "film_encode": 4 + 16 + 48 + 16 * 2 + 4 * 32 + 1,
+    # queue, dir, hit, T/lam, 4 outputs of 16 B, domain flag, rng rw, ray w, T w, push
+    "film_scatter": 4 + 16 + 48 + 16 * 2 + 4 * 16 + 1 + 8 * 2 + 32 + 16 + 4,
 }
 
 
@@ -422,12 +426,12 @@ def stage_profile(ctx: "Context", desc, out) -> dict:
 def stage_rooflines(stages: dict, hbm_gbs: float, bf16_tflops: float) -> dict:
     """Every timed stage as a fraction of its roofline: algorithmic bytes (STAGE_BYTES
     per item) over its device time against the measured HBM bandwidth, and for the
-    surrogate stage MLP FLOPs against the measured BF16 tensor peak."""
+    surrogate's MLP stage FLOPs against the measured BF16 tensor peak."""
     out = {}
     for name, s in stages.items():
         if s["ms"] <= 0 or not s["items"]:
             continue
-        if name == "film_surrogate":
+        if name == "film_mlp":
             tf = 17536.0 * s["items"] * 4 / (s["ms"] / 1000.0) / 1e12
             out[name] = {"bound": "tensor", "achieved_tflops": tf, "frac": tf / bf16_tflops}
         elif name in STAGE_BYTES:
@@ -439,7 +443,7 @@ def stage_rooflines(stages: dict, hbm_gbs: float, bf16_tflops: float) -> dict:
 def roofline(stages: dict, hbm_gbs: float, bf16_tflops: float, peak_kind: str) -> dict:
     """Roofline entry for the stage with the largest device time."""
     name, s = max(((k, v) for k, v in stages.items() if v["ms"] > 0), key=lambda kv: kv[1]["ms"])
-    if name == "film_surrogate":
+    if name == "film_mlp":
         flops = 17536.0 * s["items"] * 4  # 2*(5*64+64*64+64*64+64*4) per (hit, wavelength)
         achieved = flops / (s["ms"] / 1000.0) / 1e12
         return {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": bf16_tflops, "unit": "TFLOP/s",

@@ -39,7 +39,7 @@ RENDER_PROFILE_STAGES = 4
 RENDER_THINFILM_FP64 = 8
 NUM_STAGES = 12
 STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
-               "shadow", "finish", "film_surrogate", "unused10", "unused11")
+               "shadow", "finish", "film_encode", "film_mlp", "film_scatter")
 
 
 class LambdaError(RuntimeError):

@@ -714,6 +714,12 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
 
     lambda_status st = ctx->ensure_state(P, d_max);
     if (st != LAMBDA_OK) return st;
+    if (surrogate) {
+        // four MLP rows per thin-film hit, counted in int
+        if (P > INT32_MAX / 4) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "more than 2^29 pixels in one surrogate pass");
+        st = ctx->ensure_surrogate_state(P);
+        if (st != LAMBDA_OK) return st;
+    }
     RenderBuffers &r = ctx->rbuf;
     CK(r.out.reserve(size_t(std::max<int64_t>(host_pixels, 1)) * 12), "allocate output");
     int64_t host_off = 0;
@@ -998,10 +1004,6 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
     for (int i = 0; i < n; i++)
         if ((jobs[i].desc.flags & LAMBDA_RENDER_OUTPUT_DEVICE) && !is_device_pointer(jobs[i].out_rgb))
             return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "LAMBDA_RENDER_OUTPUT_DEVICE given a host pointer");
-    if (surrogate) {
-        lambda_status s = ctx->ensure_surrogate_state();
-        if (s != LAMBDA_OK) return s;
-    }
     if (!ctx->progress_host) {
         CK(cudaHostAlloc(reinterpret_cast<void **>(&ctx->progress_host), sizeof(int), cudaHostAllocMapped),
            "allocate progress counter");
@@ -1056,7 +1058,7 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
         ctx->stage_times[6].items = surrogate ? 0 : ctx->stats.thinfilm_hits;
         ctx->stage_times[7].items = ctx->stats.shadow_rays;
         ctx->stage_times[8].items = tot.pixels;
-        ctx->stage_times[9].items = surrogate ? ctx->stats.thinfilm_hits : 0;
+        for (int i = 9; i <= 11; i++) ctx->stage_times[i].items = surrogate ? ctx->stats.thinfilm_hits : 0;
     }
     if (tot.err & 1) return ctx->fail(LAMBDA_ERR_QUEUE_OVERFLOW, "BVH traversal stack overflow");
     if (tot.err & 2) return ctx->fail(LAMBDA_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
@@ -1162,7 +1164,8 @@ extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_de
             }
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-        constexpr size_t kBytesPerPixel = 8 + 16 * 13 + 8 + 8 + 4 * 6 + 12;  // path state, queues, staged image
+        // path state, queues, staged image, the surrogate's MLP rows, outputs and domain flags
+        constexpr size_t kBytesPerPixel = 8 + 16 * 13 + 8 + 8 + 4 * 6 + 12 + 4 * 32 + 4 * 16 + 1;
         best.max_pixels = int32_t(std::min<size_t>((free_b / 2) / kBytesPerPixel, size_t(1) << 30));
     }
     img.release();

@@ -51,7 +51,8 @@ struct SceneBuffers {
 
 struct RenderBuffers {
     DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
-        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out, path_info, jobs, active;
+        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out, path_info, jobs, active, film_rows, film_out,
+        film_in_domain;
 };
 
 struct SurrogateBuffers {
@@ -88,6 +89,7 @@ struct lambda_ctx {
     // surrogate
     bool has_surrogate = false;
     int mlp_ctas_per_sm = 0;  // resident CTAs of the tensor-core MLP kernel per SM
+    int film_encode_ctas = 0, film_scatter_ctas = 0;  // resident CTAs per SM of the surrogate's shade kernels
     lambda_film_range surrogate_range{};
     SurrogateBuffers sbuf;
 
@@ -99,7 +101,7 @@ struct lambda_ctx {
     lambda_status cuda_fail(cudaError_t e, const char *what);
     lambda_status ensure_state(int pixels, int depth);
     lambda_status surrogate_ready();
-    lambda_status ensure_surrogate_state();
+    lambda_status ensure_surrogate_state(int pixels);
     int launch_shade_surrogate(int bounce, const lambda_dev::RenderParams &rp, const lambda_dev::DeviceScene &sc,
                                const lambda_dev::PathState &ps, StageProfiler *prof, cudaStream_t s);
 
@@ -113,7 +115,8 @@ struct lambda_ctx {
                 &s.wide_code[0], &s.wide_code[1], &s.wide_code[2],
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
                 &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
-                &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &sbuf.weights_bf16, &sbuf.weights_f32};
+                &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &r.film_rows, &r.film_out,
+                &r.film_in_domain, &sbuf.weights_bf16, &sbuf.weights_f32};
     }
 };
 

@@ -14,10 +14,10 @@
 //                    layout, no swizzle), tcgen05.mma with FP32 accumulators in tensor
 //                    memory, tcgen05.ld epilogues (bias, ReLU, BF16) writing the next
 //                    layer's operand back to shared memory
-//   k_film_fused     the render's thin-film shade: rows of four hero wavelengths per
-//                    hit built in shared memory, the same tensor-core MLP tile, and
-//                    the scatter, in one kernel; hits outside the trained domain go
-//                    to the exact FP32 path's queue
+//   k_film_encode    the render's thin-film shade, in three kernels per bounce: the
+//   k_mlp_tc         hits' four hero-wavelength queries encoded as MLP rows, the
+//   k_film_scatter   tensor-core MLP over them, then the scatter; hits outside the
+//                    trained domain take the exact FP32 transfer matrix in the scatter
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -415,17 +415,21 @@ __device__ __forceinline__ void put_row(uint8_t *smem, const TileCtx &t, const f
     put8(smem, t.act, t.row, 1, kInPad, x + 8);
 }
 
-// Inference over `rows` rows: row i's input is kRowStride floats already encoded
-// (kQueries = false) or the i-th lambda_film_query, encoded here (kQueries = true).
+// Inference over n_rows rows, or rows_per_count * *count rows when count is given
+// (a count the GPU produced, such as a bounce's thin-film hits): row i's input is
+// kRowStride floats already encoded (kQueries = false) or the i-th
+// lambda_film_query, encoded here (kQueries = true).
 // out: rows x (R_s, R_p, T_s, T_p). A CTA holds G warpgroups, each working through
 // its own 128-row tiles with its own accumulator, so G dependent layer chains
 // overlap per CTA while the weights are loaded once. Error bit 1 is set if an MMA
 // completion wait timed out.
 template <bool kQueries, int G>
 __global__ void __launch_bounds__(128 * G, G == 1 ? 1 : 8 / G) k_mlp_tc(const uint4 *__restrict__ packed,
-                                                                   const void *__restrict__ in, int rows, Range rg,
-                                                                   float4 *__restrict__ out, int *error) {
+                                                                   const void *__restrict__ in, int n_rows, Range rg,
+                                                                   float4 *__restrict__ out, int *error,
+                                                                   const int *count = nullptr, int rows_per_count = 0) {
     extern __shared__ __align__(1024) uint8_t smem[];
+    const int rows = count ? rows_per_count * *count : n_rows;
     const int tiles = (rows + kTileM - 1) / kTileM;
     if (int(blockIdx.x) * G >= tiles) return;  // uniform per block, before any TMEM allocation
     TileCtx t = tile_setup<G>(smem, packed);
@@ -621,80 +625,87 @@ struct FilmSurrogate {
     float lam_lo, lam_hi, cos_lo, cos_hi, d_lo, d_hi, nf_lo, nf_hi, ns_lo, ns_hi;
 };
 
-// Thin-film shade with the surrogate, one kernel per bounce: persistent CTAs of
-// four warps take 128 thin-film hits at a time, one per thread. Each thread loads
-// its hit, evaluates the film thickness and encodes the four hero-wavelength
-// queries (lambda, cos, thickness, n_film, n_sub) in registers; the CTA then runs
-// four 128-row tiles through the tensor-core MLP, tile k holding every hit's
-// wavelength k, so thread t reads its own four (R_s + R_p)/2 back from TMEM lane t;
-// finally each thread makes its hit's thin-film scatter (material.h:228-261) and
-// Russian roulette. The surrogate covers a single film with real indices between
-// air (index exactly 1) and a substrate inside the trained box. A back-face hit
-// (light inside the substrate) is mapped to the equivalent incidence from air by
-// Snell's law, since a lossless stack reflects the same from both sides. Hits
-// outside the domain, and back-face hits past the critical angle (where the
-// transfer matrix of material.h:263-309 does not return the physical R = 1), take
-// the exact FP32 transfer matrix in the same thread.
-__global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
-                                                       FilmSurrogate fs, const uint4 *__restrict__ packed) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    const int tid = threadIdx.x;
+// Thin-film shade with the surrogate, step 1 of 3 (k_film_encode, k_mlp_tc,
+// k_film_scatter): for thin-film hit i of the bounce, the film thickness and the
+// four hero-wavelength queries (lambda, cos, thickness, n_film, n_sub), encoded as
+// MLP input rows 4i .. 4i + 3, and whether the surrogate's domain covers the hit.
+// The domain is a single film with real indices between air (index exactly 1) and
+// a substrate inside the trained box. A back-face hit (light inside the substrate)
+// is mapped to the equivalent incidence from air by Snell's law, since a lossless
+// stack reflects the same from both sides. Hits outside the domain, and back-face
+// hits past the critical angle (where the transfer matrix of material.h:263-309
+// does not return the physical R = 1), are left to the exact FP32 transfer matrix
+// in step 3; their rows are zeros.
+__global__ void __launch_bounds__(256) k_film_encode(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
+                                                     FilmSurrogate fs, float *__restrict__ rows,
+                                                     uint8_t *__restrict__ in_domain) {
     const int n = ps.counts[queue_slot(bounce, kQFilm)];
-    const int tiles = (n + kTileM - 1) / kTileM;
-    if (int(blockIdx.x) >= tiles) return;  // uniform per block, before any TMEM allocation
     const int *q = ps.mat_queue[2];
-    int *q_next = ps.queue[(bounce + 1) & 1];
-    TileCtx t = tile_setup<1>(smem, packed);
-    bool ok_tc = true;
-    for (int tile = blockIdx.x; tile < tiles && ok_tc; tile += gridDim.x) {
-        const int idx = tile * kTileM + tid;
-        const bool valid = idx < n;
-        const int p = valid ? q[idx] : 0;
-        bool ok = false;
+    const int stride = gridDim.x * blockDim.x;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
+        const int p = q[idx];
+        const ShadeIn s = load_shade(ps, sc, p);
+        bool ok = s.m.y == 1;
+        const float d = ok ? scalar_texture(sc, sc.material_props[s.m.w], s.sp.point) : 0.0f;
+        const float cos_in = dot(s.nrm, -s.d);
+        ok = ok && d >= fs.d_lo && d <= fs.d_hi;
         float e[kHero][kIn];
-        if (valid) {
-            const ShadeIn s = load_shade(ps, sc, p);
-            ok = s.m.y == 1;
-            const float d = ok ? scalar_texture(sc, sc.material_props[s.m.w], s.sp.point) : 0.0f;
-            const float cos_in = dot(s.nrm, -s.d);
-            ok = ok && d >= fs.d_lo && d <= fs.d_hi;
-#pragma unroll
-            for (int w = 0; w < kHero; w++) {
-                const float lam = s.lam.v[w];
-                const double2 a = cspectrum_at(sc, sc.material_props[s.m.z], lam);
-                const double2 b = cspectrum_at(sc, sc.material_props[s.m.z + 1], lam);
-                const double2 c = cspectrum_at(sc, sc.material_props[s.m.z + 2], lam);
-                const float nf = float(b.x), ns = float(c.x);
-                float c0 = cos_in;
-                if (!s.front) {
-                    const float sin2 = ns * ns * (1 - cos_in * cos_in);
-                    ok = ok && sin2 < 1.0f;
-                    c0 = sqrtf(fmaxf(1 - sin2, 0.0f));
-                }
-                ok = ok && a.x == 1.0 && a.y == 0.0 && b.y == 0.0 && c.y == 0.0 && nf >= fs.nf_lo && nf <= fs.nf_hi &&
-                     ns >= fs.ns_lo && ns <= fs.ns_hi && c0 >= fs.cos_lo && c0 <= fs.cos_hi && lam >= fs.lam_lo &&
-                     lam <= fs.lam_hi;
-                const float v[kIn] = {lam, c0, d, nf, ns};
-                encode(v, fs.rg, e[w]);
-            }
-        }
-        s4 R = s4_fill(0.0f);
 #pragma unroll
         for (int w = 0; w < kHero; w++) {
-            if (ok_tc) {
-                float row[kIn];
-#pragma unroll
-                for (int k = 0; k < kIn; k++) row[k] = ok ? e[w][k] : 0.0f;
-                put_row(smem, t, row);
-                float y[kOut];
-                ok_tc = mlp_tile<1>(smem, t, y);
-                R.v[w] = clampf((y[0] + y[1]) * 0.5f, 0.0f, 1.0f);
+            const float lam = s.lam.v[w];
+            const double2 a = cspectrum_at(sc, sc.material_props[s.m.z], lam);
+            const double2 b = cspectrum_at(sc, sc.material_props[s.m.z + 1], lam);
+            const double2 c = cspectrum_at(sc, sc.material_props[s.m.z + 2], lam);
+            const float nf = float(b.x), ns = float(c.x);
+            float c0 = cos_in;
+            if (!s.front) {
+                const float sin2 = ns * ns * (1 - cos_in * cos_in);
+                ok = ok && sin2 < 1.0f;
+                c0 = sqrtf(fmaxf(1 - sin2, 0.0f));
             }
+            ok = ok && a.x == 1.0 && a.y == 0.0 && b.y == 0.0 && c.y == 0.0 && nf >= fs.nf_lo && nf <= fs.nf_hi &&
+                 ns >= fs.ns_lo && ns <= fs.ns_hi && c0 >= fs.cos_lo && c0 <= fs.cos_hi && lam >= fs.lam_lo &&
+                 lam <= fs.lam_hi;
+            const float v[kIn] = {lam, c0, d, nf, ns};
+            encode(v, fs.rg, e[w]);
         }
-        bool alive = false;
-        if (valid && ok_tc) {
+        float4 *r = reinterpret_cast<float4 *>(rows + size_t(idx) * (kHero * kRowStride));
+#pragma unroll
+        for (int w = 0; w < kHero; w++) {
+            r[2 * w] = ok ? make_float4(e[w][0], e[w][1], e[w][2], e[w][3]) : make_float4(0, 0, 0, 0);
+            r[2 * w + 1] = make_float4(ok ? e[w][4] : 0.0f, 0, 0, 0);
+        }
+        in_domain[idx] = ok ? 1 : 0;
+    }
+}
+
+// Step 3: each hit's reflectance (R_s + R_p) / 2 at its four wavelengths from the
+// MLP's outputs (or, outside the domain, the exact FP32 transfer matrix), then the
+// thin-film scatter (material.h:228-261) and Russian roulette.
+__global__ void __launch_bounds__(256, 3) k_film_scatter(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
+                                                         const float4 *__restrict__ out,
+                                                         const uint8_t *__restrict__ in_domain) {
+    const int n = ps.counts[queue_slot(bounce, kQFilm)];
+    const int *q = ps.mat_queue[2];
+    int *q_next = ps.queue[(bounce + 1) & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int idx = base + threadIdx.x;
+        const bool valid = idx < n;
+        bool alive = false, ok = false;
+        int p = 0;
+        if (valid) {
+            p = q[idx];
             const ShadeIn s = load_shade(ps, sc, p);
-            if (!ok) {
+            ok = in_domain[idx] != 0;
+            s4 R;
+            if (ok) {
+#pragma unroll
+                for (int w = 0; w < kHero; w++) {
+                    const float4 y = out[size_t(idx) * kHero + w];
+                    R.v[w] = clampf((y.x + y.y) * 0.5f, 0.0f, 1.0f);
+                }
+            } else {
                 float thick[kMaxFilmLayers];
                 thin_film_thickness(sc, s, thick);
                 R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
@@ -707,10 +718,8 @@ __global__ void __launch_bounds__(128, 5) k_film_fused(int bounce, RenderParams 
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
-        warp_push(&ps.counts[queue_slot(bounce, kQFilmFallback)], valid && ok_tc && !ok);
+        warp_push(&ps.counts[queue_slot(bounce, kQFilmFallback)], valid && !ok);
     }
-    if (!ok_tc && tid == 0) atomicOr(ps.error, 2);
-    tile_teardown<1>(t);
 }
 
 // Host: the FP32 parameters as the BF16 shared-memory image of the MLP kernels
@@ -769,8 +778,6 @@ cudaError_t configure_mlp_kernels() {
     cudaError_t e = cudaFuncSetAttribute(k_mlp_tc<false, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOf<G>);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_mlp_tc<true, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOf<G>);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_film_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     return e;
 }
 
@@ -806,17 +813,6 @@ lambda_status install(lambda_ctx *ctx, const float *params_host, const lambda_fi
     ctx->surrogate_range = r;
     ctx->has_surrogate = true;
     return LAMBDA_OK;
-}
-
-// Resident CTAs per SM of the render's surrogate kernel (one warpgroup each),
-// capped so their TMEM columns fit the SM's 512 and no allocation ever waits.
-// Computed outside stream capture and cached on the context.
-int mlp_grid(lambda_ctx *ctx) {
-    if (ctx->mlp_ctas_per_sm <= 0) {
-        const int per_sm = resident_ctas((const void *)k_film_fused, ctx->device, 128, kSmemBytes);
-        ctx->mlp_ctas_per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
-    }
-    return ctx->mlp_ctas_per_sm * ctx->sm_count;
 }
 
 // Grid of the batched query kernel (kQueryWarpgroups warpgroups per CTA) for
@@ -866,18 +862,47 @@ int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const
     fs.nf_hi = surrogate_range.n_film[1];
     fs.ns_lo = surrogate_range.n_sub[0];
     fs.ns_hi = surrogate_range.n_sub[1];
-    const uint8_t *w = static_cast<const uint8_t *>(sbuf.weights_bf16.ptr);
+    const uint4 *w = static_cast<const uint4 *>(sbuf.weights_bf16.ptr);
+    float *rows = rbuf.film_rows.as<float>();
+    float4 *out = rbuf.film_out.as<float4>();
+    uint8_t *in_domain = rbuf.film_in_domain.as<uint8_t>();
+    // grids for the pass's largest thin-film queue, one hit per pixel
+    const int64_t hits = std::max(1, rp.num_pixels);
+    auto grid = [&](int per_sm, int block) {
+        return int(std::max<int64_t>(1, std::min<int64_t>((hits + block - 1) / block, int64_t(per_sm) * sm_count)));
+    };
+    constexpr int G = kQueryWarpgroups;
+    const int64_t tiles = (hits * kHero + kTileM - 1) / kTileM;
+    const int mlp_grid = int(std::max<int64_t>(1, std::min<int64_t>((tiles + G - 1) / G, int64_t(mlp_ctas_per_sm) * sm_count)));
     if (prof) prof->begin(9);
-    k_film_fused<<<mlp_grid(this), 128, kSmemBytes, s>>>(bounce, rp, sc, ps, fs, reinterpret_cast<const uint4 *>(w));
+    k_film_encode<<<grid(film_encode_ctas, 256), 256, 0, s>>>(bounce, rp, sc, ps, fs, rows, in_domain);
     if (prof) prof->end();
-    return 1;
+    if (prof) prof->begin(10);
+    k_mlp_tc<false, G><<<mlp_grid, 128 * G, kSmemOf<G>, s>>>(w, rows, 0, Range{}, out, ps.error,
+                                                             ps.counts + queue_slot(bounce, kQFilm), kHero);
+    if (prof) prof->end();
+    if (prof) prof->begin(11);
+    k_film_scatter<<<grid(film_scatter_ctas, 256), 256, 0, s>>>(bounce, rp, sc, ps, out, in_domain);
+    if (prof) prof->end();
+    return 3;
 }
 
-// Kernel attributes and the MLP grid, set up before any stream capture.
-lambda_status lambda_ctx::ensure_surrogate_state() {
+// Kernel attributes, grids and the path-state buffers of the surrogate's render
+// kernels for `pixels` paths, set up before any stream capture.
+lambda_status lambda_ctx::ensure_surrogate_state(int pixels) {
     lambda_ctx *ctx = this;
     CK(configure_mlp_kernels(), "configure MLP kernels");
-    mlp_grid(this);
+    constexpr int G = kQueryWarpgroups;
+    if (mlp_ctas_per_sm <= 0) {
+        const int per_sm = resident_ctas((const void *)k_mlp_tc<false, G>, device, 128 * G, kSmemOf<G>);
+        mlp_ctas_per_sm = std::max(1, std::min(per_sm, 512 / (G * kTmemCols)));
+        film_encode_ctas = resident_ctas((const void *)k_film_encode, device, 256, 0);
+        film_scatter_ctas = resident_ctas((const void *)k_film_scatter, device, 256, 0);
+    }
+    const size_t P = size_t(std::max(pixels, 1));
+    CK(rbuf.film_rows.reserve(P * kHero * kRowStride * sizeof(float)), "allocate surrogate rows");
+    CK(rbuf.film_out.reserve(P * kHero * sizeof(float4)), "allocate surrogate rows");
+    CK(rbuf.film_in_domain.reserve(P), "allocate surrogate rows");
     return LAMBDA_OK;
 }
 
