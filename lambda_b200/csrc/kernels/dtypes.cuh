@@ -76,7 +76,8 @@ struct PathState {
     float4 *ray_o;        // origin xyz, w = pdf of the last scatter
     float4 *ray_d;        // direction xyz, w = 1 if the last scatter was specular
     float4 *throughput;
-    float4 *radiance;
+    float4 *radiance;     // NEE terms of the running sample
+    float4 *emit;         // emission term of a sample that ended at a miss or an emitter
     float4 *hit_p;        // world point xyz, w = u
     float4 *hit_n;        // shading normal xyz, w = v
     int4 *hit_id;         // instance (-1 = miss), object, front facing, 0

@@ -122,15 +122,17 @@ extern "C" lambda_status lambda_ctx_create(int32_t device, lambda_ctx **out) {
     }
     cudaEventCreate(&ctx->ev_start);
     cudaEventCreate(&ctx->ev_stop);
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < 3; i++) {
         e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming);
+        if (e == cudaSuccess && i < 2) e = cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming);
         if (e != cudaSuccess) {
             g_create_error = std::string("cudaStreamCreate failed (") + cudaGetErrorString(e) + ")";
             return LAMBDA_ERR_CUDA;
         }
     }
     e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_lambert, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_shadow, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         g_create_error = std::string("cudaEventCreate failed (") + cudaGetErrorString(e) + ")";
         return LAMBDA_ERR_CUDA;
@@ -148,10 +150,12 @@ lambda_ctx::~lambda_ctx() {
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
     if (ev_fork) cudaEventDestroy(ev_fork);
-    for (int i = 0; i < 2; i++) {
+    if (ev_lambert) cudaEventDestroy(ev_lambert);
+    if (ev_shadow) cudaEventDestroy(ev_shadow);
+    for (int i = 0; i < 2; i++)
         if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+    for (int i = 0; i < 3; i++)
         if (side[i]) cudaStreamDestroy(side[i]);
-    }
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -580,6 +584,7 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     CK(r.ray_d.reserve(P * 16), "allocate path state");
     CK(r.throughput.reserve(P * 16), "allocate path state");
     CK(r.radiance.reserve(P * 16), "allocate path state");
+    CK(r.emit.reserve(P * 16), "allocate path state");
     CK(r.hit_p.reserve(P * 16), "allocate path state");
     CK(r.hit_n.reserve(P * 16), "allocate path state");
     CK(r.hit_id.reserve(P * 16), "allocate path state");
@@ -606,6 +611,7 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     ps.ray_d = r.ray_d.as<float4>();
     ps.throughput = r.throughput.as<float4>();
     ps.radiance = r.radiance.as<float4>();
+    ps.emit = r.emit.as<float4>();
     ps.hit_p = r.hit_p.as<float4>();
     ps.hit_n = r.hit_n.as<float4>();
     ps.hit_id = r.hit_id.as<int4>();
@@ -785,9 +791,13 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     // One wave's launches. With a profiler every launch is bracketed by events, in
     // order on the library stream. Inside the pass graph's loop the prologue sets the
     // loop condition, and a bounce's shading runs as parallel branches: Lambertian
-    // shade then its shadow rays, mirror/dielectric shade, thin-film shade. They touch
-    // disjoint paths (each path is in one material queue), so only the queue order
-    // depends on their interleaving, and the next intersect waits for all of them.
+    // shade, mirror/dielectric shade and thin-film shade touch disjoint paths (each
+    // path is in one material queue), so only the queue order depends on their
+    // interleaving, and the next intersect waits for all three. The Lambertian
+    // shade's shadow rays run on a stream of their own beside the next intersect:
+    // they add to the NEE radiance, which intersect no longer touches (it records a
+    // path's final emission apart), and the next Lambertian shade, which refills the
+    // NEE buffers, waits for them.
     cudaError_t fork_err = cudaSuccess;
     auto wave = [&](StageProfiler *pr, cudaGraphConditionalHandle loop, int waves) -> int {
         int n = 0;
@@ -799,12 +809,9 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         };
         timed(1, [&] { k_wave_prologue<<<1, 256, 0, stream>>>(d_max, ps, loop, waves, ctx->progress_dev); });
         timed(2, [&] { k_raygen<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
-        // branch k: 0 Lambertian + shadow, 1 specular, 2 thin film
+        // branch k: 1 specular, 2 thin film
         auto branch = [&](int k, int b, cudaStream_t s) {
-            if (k == 0) {
-                timed(4, [&] { k_shade_lambert<<<g_lambert, sb, 0, s>>>(b, rp, sc, ps); });
-                timed(7, [&] { shadow(b, s); });
-            } else if (k == 1) {
+            if (k == 1) {
                 timed(5, [&] { k_shade_specular<<<g_spec, sb, 0, s>>>(b, rp, sc, ps); });
             } else if (surrogate) {
                 n += ctx->launch_shade_surrogate(b, rp, sc, ps, pr, s);
@@ -814,27 +821,44 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
                 timed(6, [&] { k_shade_film_exact<false><<<g_film, sb, 0, s>>>(b, rp, sc, ps); });
             }
         };
-        int branches[3], nb = 0;
-        for (int k = 0; k < 3; k++)
+        const bool lambert_on = (sc.families & 1u) != 0;
+        int branches[2], nb = 0;
+        for (int k = 1; k < 3; k++)
             if (sc.families & (1u << k)) branches[nb++] = k;
+        auto keep = [&](cudaError_t e) {
+            if (fork_err == cudaSuccess) fork_err = e;
+        };
+        cudaStream_t shadow_stream = ctx->side[2];
+        bool shadow_pending = false;
         for (int b = 0; b <= d_max; b++) {
             timed(3, [&] { intersect(b); });
-            if (pr || nb < 2) {
+            if (pr) {
+                if (lambert_on) {
+                    timed(4, [&] { k_shade_lambert<<<g_lambert, sb, 0, stream>>>(b, rp, sc, ps); });
+                    timed(7, [&] { shadow(b, stream); });
+                }
                 for (int i = 0; i < nb; i++) branch(branches[i], b, stream);
                 continue;
             }
-            auto keep = [&](cudaError_t e) {
-                if (fork_err == cudaSuccess) fork_err = e;
-            };
-            keep(cudaEventRecord(ctx->ev_fork, stream));
-            for (int i = 1; i < nb; i++) {
-                keep(cudaStreamWaitEvent(ctx->side[i - 1], ctx->ev_fork, 0));
-                branch(branches[i], b, ctx->side[i - 1]);
-                keep(cudaEventRecord(ctx->ev_join[i - 1], ctx->side[i - 1]));
+            if (nb > 0) keep(cudaEventRecord(ctx->ev_fork, stream));
+            for (int i = 0; i < nb; i++) {
+                keep(cudaStreamWaitEvent(ctx->side[i], ctx->ev_fork, 0));
+                branch(branches[i], b, ctx->side[i]);
+                keep(cudaEventRecord(ctx->ev_join[i], ctx->side[i]));
             }
-            branch(branches[0], b, stream);
-            for (int i = 1; i < nb; i++) keep(cudaStreamWaitEvent(stream, ctx->ev_join[i - 1], 0));
+            if (lambert_on) {
+                if (shadow_pending) keep(cudaStreamWaitEvent(stream, ctx->ev_shadow, 0));
+                timed(4, [&] { k_shade_lambert<<<g_lambert, sb, 0, stream>>>(b, rp, sc, ps); });
+                keep(cudaEventRecord(ctx->ev_lambert, stream));
+                keep(cudaStreamWaitEvent(shadow_stream, ctx->ev_lambert, 0));
+                timed(7, [&] { shadow(b, shadow_stream); });
+                keep(cudaEventRecord(ctx->ev_shadow, shadow_stream));
+                shadow_pending = true;
+            }
+            for (int i = 0; i < nb; i++) keep(cudaStreamWaitEvent(stream, ctx->ev_join[i], 0));
         }
+        // the last shadow rays finish inside the wave
+        if (shadow_pending) keep(cudaStreamWaitEvent(stream, ctx->ev_shadow, 0));
         return n;
     };
     auto clear = [&]() -> cudaError_t {

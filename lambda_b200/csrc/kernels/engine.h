@@ -50,7 +50,7 @@ struct SceneBuffers {
 };
 
 struct RenderBuffers {
-    DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
+    DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, emit, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
         q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out, path_info, jobs, active, film_rows, film_out,
         film_in_domain;
 };
@@ -65,10 +65,11 @@ struct lambda_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
-    // Branches of a bounce that run beside the main stream's inside the pass graph
-    // (fork and join events, no timing).
-    cudaStream_t side[2] = {nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    // Branches of a bounce that run beside the main stream's inside the pass graph:
+    // specular and thin-film shading, and the shadow rays (fork and join events, no
+    // timing).
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr}, ev_lambert = nullptr, ev_shadow = nullptr;
     std::string last_error;
 
     bool has_scene = false;
@@ -113,7 +114,7 @@ struct lambda_ctx {
                 &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &s.wide[0], &s.wide[1], &s.wide[2], &s.wide_leaves[0], &s.wide_leaves[1], &s.wide_leaves[2],
                 &s.wide_code[0], &s.wide_code[1], &s.wide_code[2],
-                &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.hit_p, &r.hit_n,
+                &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.emit, &r.hit_p, &r.hit_n,
                 &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
                 &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &r.film_rows, &r.film_out,
                 &r.film_in_domain, &sbuf.weights_bf16, &sbuf.weights_f32};

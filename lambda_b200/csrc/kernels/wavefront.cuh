@@ -11,7 +11,12 @@
 //   specular    mirror and dielectric scatter + Russian roulette
 //   thin film   transfer-matrix reflectance of the four hero wavelengths, scatter
 //   shadow      occlusion of the NEE rays and their radiance (renderer.h:166-173)
-// so every kernel runs one material's code over a coherent batch. Queue pushes
+// so every kernel runs one material's code over a coherent batch. A sample's last
+// term, the emission of the miss or emitter that ends it, is kept apart (emit) and
+// added to the NEE terms (radiance) when the sample is banked: that is the
+// reference's order of additions (renderer.h:105-131 comes after the previous
+// bounce's NEE), and it lets bounce i's shadow rays run beside bounce i+1's
+// intersect. Queue pushes
 // cost one atomic per warp (ballot + popc). All path state is structure-of-arrays
 // indexed by pixel; queues hold pixel ids.
 #pragma once
@@ -72,6 +77,7 @@ LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
     ps.path_info[p] = make_int2(local, job.depth);
     ps.film[p] = make_float4(0, 0, 0, 0);
     ps.radiance[p] = make_float4(0, 0, 0, 0);
+    ps.emit[p] = make_float4(0, 0, 0, 0);
     ps.lam[p] = make_float4(job.lambda_min, job.lambda_min, job.lambda_min, job.lambda_min);
     if (p == 0) {
         ps.wave[0] = 0;
@@ -110,6 +116,11 @@ LAMBDA_KERNEL void k_wave_prologue(int depth, PathState ps, cudaGraphConditional
     }
 }
 
+// Radiance of a finished sample: its NEE terms, then the emission that ended it.
+__device__ __forceinline__ s4 sample_radiance(const PathState &ps, int p) {
+    return from_f4(ps.radiance[p]) + from_f4(ps.emit[p]);
+}
+
 // Film += linear sRGB of the finished sample (renderer.h:84), then start the
 // next sample: stratified jitter, hero wavelength, camera ray (renderer.h:69-81).
 // Pixels of jobs whose last sample was the previous wave only bank that sample.
@@ -122,7 +133,7 @@ LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
     if (p >= n_prev) return;
     const Job &job = rp.jobs[job_of(rp, p)];
 
-    const f3 rgb = spectrum_to_rgb(sc, from_f4(ps.radiance[p]), from_f4(ps.lam[p]), job.lambda_range);
+    const f3 rgb = spectrum_to_rgb(sc, sample_radiance(ps, p), from_f4(ps.lam[p]), job.lambda_range);
     float4 film = ps.film[p];
     film.x += rgb.x;
     film.y += rgb.y;
@@ -130,6 +141,7 @@ LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
     ps.film[p] = film;
     if (p >= n_now) {
         ps.radiance[p] = make_float4(0, 0, 0, 0);
+        ps.emit[p] = make_float4(0, 0, 0, 0);
         return;
     }
 
@@ -149,6 +161,7 @@ LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
     ps.ray_d[p] = make_float4(dir.x, dir.y, dir.z, 1.0f);
     ps.throughput[p] = make_float4(1, 1, 1, 1);
     ps.radiance[p] = make_float4(0, 0, 0, 0);
+    ps.emit[p] = make_float4(0, 0, 0, 0);
     ps.queue[0][p] = p;
 }
 
@@ -157,8 +170,8 @@ __device__ __forceinline__ int material_of(const DeviceScene &sc, int inst_mater
     return inst_material >= 0 ? inst_material : prim_material(load_prim(sc, obj));
 }
 
-// Closest hit; misses and emitter hits add their radiance and end the path
-// (renderer.h:105-131); other hits go to their material's queue.
+// Closest hit; misses and emitter hits record their emission term and end the
+// path (renderer.h:105-131); other hits go to their material's queue.
 template <int K>
 LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
     extern __shared__ int stack_smem[];
@@ -187,7 +200,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParam
                 if (!specular && lights)
                     w = power_heuristic(prev_pdf, (1 / (4 * kPi)) * sc.light_power[sc.num_lights - 1] / sc.total_light_power);
                 const s4 T = from_f4(ps.throughput[p]);
-                ps.radiance[p] = to_f4(from_f4(ps.radiance[p]) + T * background_eval(sc, d, lam) * w);
+                ps.emit[p] = to_f4(T * background_eval(sc, d, lam) * w);
             } else {
                 const InstanceRef ir = instance_ref(sc, h.instance);
                 const int4 ih = ir.header();
@@ -211,7 +224,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParam
                     sp.v = h.v;
                     const s4 lam = from_f4(ps.lam[p]);
                     const s4 T = from_f4(ps.throughput[p]);
-                    ps.radiance[p] = to_f4(from_f4(ps.radiance[p]) + T * spectrum_texture4(sc, m.y, sp, lam) * w);
+                    ps.emit[p] = to_f4(T * spectrum_texture4(sc, m.y, sp, lam) * w);
                 } else {
                     ps.hit_p[p] = make_float4(h.point.x, h.point.y, h.point.z, h.u);
                     ps.hit_n[p] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.v);
@@ -578,7 +591,7 @@ LAMBDA_KERNEL void k_finish(RenderParams rp, DeviceScene sc, PathState ps) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= rp.num_pixels) return;
     const Job &job = rp.jobs[job_of(rp, p)];
-    const f3 rgb = spectrum_to_rgb(sc, from_f4(ps.radiance[p]), from_f4(ps.lam[p]), job.lambda_range);
+    const f3 rgb = spectrum_to_rgb(sc, sample_radiance(ps, p), from_f4(ps.lam[p]), job.lambda_range);
     float4 film = ps.film[p];
     film.x += rgb.x;
     film.y += rgb.y;

@@ -123,9 +123,10 @@ def cornell(directory: str, width: int = 256, height: int = 256, spp: int = 16, 
 
 def thinfilm_spheres(directory: str, width: int = 1920, height: int = 1080, spp: int = 256, depth: int = 16,
                      seed: int = 3, name: str = "thinfilm.lrd", film: str = "thinfilm",
-                     background: str = "0") -> SceneFiles:
+                     background: str = "0", thickness: str = "worley 200 800 3") -> SceneFiles:
     """64 thin-film spheres on a jittered grid. `film` may be "dielectric" to swap
-    the film for a plain 1.0/1.5 dielectric (same geometry)."""
+    the film for a plain 1.0/1.5 dielectric (same geometry); `thickness` is the
+    film's scalar thickness texture in nm."""
     rng = np.random.default_rng(seed)
     jitter = rng.uniform(-0.1, 0.1, size=(8, 8, 2))
     path = os.path.join(directory, name)
@@ -134,7 +135,7 @@ def thinfilm_spheres(directory: str, width: int = 1920, height: int = 1080, spp:
     lines = [
         "# 64 thin-film spheres (r=0.4) on a jittered 8x8 grid, Lambertian ground, one quad light",
         f"Render {width} {height} {depth} {spp} 380 780",
-        "Texture thickness scalar worley 200 800 3",
+        f"Texture thickness scalar {thickness}",
         "Material ground lambertian 0.5",
         "Material lamp emissive 10",
     ]

@@ -153,3 +153,28 @@ def test_surrogate_render_unbiased(scene_dir, ctx):
     assert st.thinfilm_hits > 0 and st.thinfilm_fallback < 0.05 * st.thinfilm_hits
     assert err <= floor + 0.01
     assert abs(ratio - 1) < 0.02
+
+
+def test_surrogate_render_outside_domain_is_exact(scene_dir, ctx):
+    """Films thicker than the surrogate's trained box (900-1000 nm against 150-850 nm)
+    are all evaluated by the exact FP32 transfer matrix inside the surrogate's scatter
+    kernel, so the render equals the exact render bit for bit and every thin-film hit
+    counts as a fallback. A box that straddles the limit (700-1000 nm) sends only part
+    of the hits there."""
+    surrogate.install(ctx)
+    sc = scenes.thinfilm_spheres(scene_dir, 64, 36, 16, thickness="worley 900 1000 3", name="s_thick.lrd")
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx.upload(scene)
+    exact = ctx.render(scene.render_desc(seed=5, flags=lb.RENDER_THINFILM_EXACT))
+    sur = ctx.render(scene.render_desc(seed=5, flags=lb.RENDER_THINFILM_SURROGATE))
+    st = ctx.stats()
+    assert st.thinfilm_hits > 0 and st.thinfilm_fallback == st.thinfilm_hits
+    assert np.array_equal(sur, exact, equal_nan=True)
+
+    sc = scenes.thinfilm_spheres(scene_dir, 64, 36, 16, thickness="worley 700 1000 3", name="s_mixed.lrd")
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx.upload(scene)
+    ctx.render(scene.render_desc(seed=5, flags=lb.RENDER_THINFILM_SURROGATE))
+    st = ctx.stats()
+    print(f"straddling box: {st.thinfilm_fallback} of {st.thinfilm_hits} thin-film hits exact")
+    assert 0 < st.thinfilm_fallback < st.thinfilm_hits
