@@ -164,12 +164,14 @@ def thinfilm_spheres(directory: str, width: int = 1920, height: int = 1080, spp:
 
 
 def random_pose_jobs(scene, n: int, seed: int = 4, resolutions=(128, 256, 512, 1024), spps=(1, 4, 16, 64, 256),
-                     depth=(4, 24), flags: int = 0, target=(0.0, 0.3, 0.0)) -> list:
+                     depth=(4, 24), flags: int = 0, target=(0.0, 0.3, 0.0), distance=(8.0, 11.0),
+                     height=(2.5, 6.0), jitter: float = 0.5) -> list:
     """Render descriptors of `n` views of an uploaded scene for a batch: square
     resolutions and sample counts drawn uniformly from the given sets, depth
-    uniform in [depth[0], depth[1]], and a camera at a random azimuth, distance
-    8-11 and height 2.5-6 looking at `target` (jittered by up to 0.5) with a
-    35-50 degree field of view. Render seed of job i is seed * 1000 + i."""
+    uniform in [depth[0], depth[1]], and a camera at a random azimuth, at a
+    horizontal distance and height uniform in the given ranges, looking at `target`
+    (jittered by up to `jitter` per axis) with a 35-50 degree field of view. The
+    defaults frame the thin-film sphere grid. Render seed of job i is seed * 1000 + i."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
@@ -177,10 +179,10 @@ def random_pose_jobs(scene, n: int, seed: int = 4, resolutions=(128, 256, 512, 1
         spp = int(rng.choice(spps))
         dep = int(rng.integers(depth[0], depth[1] + 1))
         az = rng.uniform(0, 2 * math.pi)
-        dist = rng.uniform(8.0, 11.0)
-        height = rng.uniform(2.5, 6.0)
-        tgt = np.asarray(target) + rng.uniform(-0.5, 0.5, 3)
-        pos = (dist * math.sin(az), height, dist * math.cos(az))
+        dist = rng.uniform(*distance)
+        h = rng.uniform(*height)
+        tgt = np.asarray(target) + rng.uniform(-jitter, jitter, 3)
+        pos = (dist * math.sin(az), h, dist * math.cos(az))
         cam = look_at_camera(pos, tgt, (0.0, 1.0, 0.0), rng.uniform(35.0, 50.0), 1.0)
         d = scene.render_desc(seed=seed * 1000 + i, flags=flags)
         st = d.settings
