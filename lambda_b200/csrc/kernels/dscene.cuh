@@ -410,13 +410,19 @@ struct WideStack {
     }
 };
 
-// World -> instance space (instance.h:50-52). An identity instance's transform
-// reduces exactly to adding +0 (which only turns -0 into +0), so it is done that way.
-__device__ __forceinline__ Ray3 to_local(const DeviceScene &s, int inst, const InstanceRef &ir, f3 o, f3 d) {
-    if (s.instance_flags[inst] & 1u) return make_ray(o + mk(0.0f, 0.0f, 0.0f), d + mk(0.0f, 0.0f, 0.0f));
+// World ray wr -> instance space (instance.h:50-52), given the instance's flags. An
+// identity instance's transform reduces exactly to adding +0 (which only turns -0
+// into +0), so it is done that way; when no direction component is zero the
+// direction, and so its reciprocals, are the world ray's.
+__device__ __forceinline__ Ray3 to_local(uint32_t flags, const InstanceRef &ir, const Ray3 &wr) {
+    const f3 zero = mk(0.0f, 0.0f, 0.0f);
+    if (flags & 1u) {
+        if (wr.d.x != 0.0f && wr.d.y != 0.0f && wr.d.z != 0.0f) return Ray3{wr.o + zero, wr.d, wr.inv};
+        return make_ray(wr.o + zero, wr.d + zero);
+    }
     float mi[16];
     ir.load_m(mi, 1);
-    return make_ray(xform(mi, o, 1), xform(mi, d, 0));
+    return make_ray(xform(mi, wr.o, 1), xform(mi, wr.d, 0));
 }
 
 // Instance space -> world for a hit (instance.h:42, :48).
@@ -473,17 +479,21 @@ __device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, 
     while (sp > 0) {
         --sp;
         const int code = st.code[sp * st.stride];
-        if (st.te[sp * st.stride] > best) continue;
+        te = st.te[sp * st.stride];
+        if (te > best) continue;
         if (code >= 0) {
             sp = wide_expand<K>(s, code, wr, best, st, sp, overflow);
             if (overflow) break;
             continue;
         }
         const int inst = __ldg(&s.wide_leaves[-code - 1]).x;
+        const uint32_t flags = s.instance_flags[inst];
         const InstanceRef ir = instance_ref(s, inst);
         const int root = ir.header().z;
-        const Ray3 lr = to_local(s, inst, ir, o, d);
-        if (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best) continue;
+        const Ray3 lr = to_local(flags, ir, wr);
+        // a root box equal to the leaf's, under the same ray, was just tested (te)
+        if (!(flags & 2u) && (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best))
+            continue;
         int ssp = 0;
         sub.put(ssp++, __ldg(&s.wide_code[root]), te);
         while (ssp > 0) {
@@ -514,7 +524,7 @@ __device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, 
         return false;
     }
     const InstanceRef ir = instance_ref(s, best_inst);
-    const Ray3 lr = to_local(s, best_inst, ir, o, d);
+    const Ray3 lr = to_local(s.instance_flags[best_inst], ir, wr);
     prim_attributes(s, best_obj, load_prim(s, best_obj), lr.o, lr.d, best, h);
     h.instance = best_inst;
     h.object = best_obj;
@@ -534,7 +544,7 @@ __device__ __forceinline__ bool occluded_w(const DeviceScene &s, f3 o, f3 d, int
     float best = kMax;
     if (light_inst != -1) {
         const InstanceRef ir = instance_ref(s, light_inst);
-        const Ray3 lr = to_local(s, light_inst, ir, o, d);
+        const Ray3 lr = to_local(s.instance_flags[light_inst], ir, wr);
         const Prim p = load_prim(s, light_obj);
         const float t = intersect_t(p, lr, kMax);
         if (t < 0) return true;
@@ -550,17 +560,20 @@ __device__ __forceinline__ bool occluded_w(const DeviceScene &s, f3 o, f3 d, int
     while (sp > 0) {
         --sp;
         const int code = st.code[sp * st.stride];
-        if (st.te[sp * st.stride] > best) continue;
+        te = st.te[sp * st.stride];
+        if (te > best) continue;
         if (code >= 0) {
             sp = wide_expand<K>(s, code, wr, best, st, sp, overflow);
             if (overflow) return true;
             continue;
         }
         const int inst = __ldg(&s.wide_leaves[-code - 1]).x;
+        const uint32_t flags = s.instance_flags[inst];
         const InstanceRef ir = instance_ref(s, inst);
         const int root = ir.header().z;
-        const Ray3 lr = to_local(s, inst, ir, o, d);
-        if (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best) continue;
+        const Ray3 lr = to_local(flags, ir, wr);
+        if (!(flags & 2u) && (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best))
+            continue;
         int ssp = 0;
         sub.put(ssp++, __ldg(&s.wide_code[root]), te);
         while (ssp > 0) {

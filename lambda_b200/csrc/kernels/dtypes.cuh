@@ -33,7 +33,8 @@ struct DeviceScene {
     const float *light_power;
     const float *light_cdf;      // running sums of light_power in list order
     const float *material_emission;  // per material: average emission (0 if not emissive)
-    const uint32_t *instance_flags;  // bit 0: transform and inverse are exactly the identity
+    const uint32_t *instance_flags;  // bit 0: transform and inverse are exactly the identity; bit 1: also
+                                     // alone in its TLAS leaf, whose box is its BLAS root's box
     const float *cie;            // [471][3] as float
     const int *perm;             // [256]
     const float4 *worley_cells;  // feature offsets of lattice cells (xyz), cell-major

@@ -469,6 +469,29 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
         }
         iflags[i] = ident ? 1u : 0u;
     }
+    // bit 1: the instance is the only one of its TLAS leaf and that leaf's box is its
+    // BLAS root's box, so (with an identity transform) the root's box test repeats
+    // the leaf's and is skipped
+    if (d.num_nodes > 0) {
+        std::vector<int> todo = {0};
+        while (!todo.empty()) {
+            const int n = todo.back();
+            todo.pop_back();
+            const lambda_bvh_node &nd = d.nodes[n];
+            if (nd.count <= 0) {
+                todo.push_back(nd.index);
+                todo.push_back(n + 1);
+                continue;
+            }
+            if (nd.count != 1 || nd.index < 0 || nd.index >= d.num_instances || !(iflags[nd.index] & 1u)) continue;
+            const int root = d.instances[nd.index].node;
+            if (root < 0 || root >= d.num_nodes) continue;
+            const lambda_bvh_node &r = d.nodes[root];
+            bool same = true;
+            for (int k = 0; k < 3; k++) same = same && nd.min[k] == r.min[k] && nd.max[k] == r.max[k];
+            if (same) iflags[nd.index] |= 2u;
+        }
+    }
     CK(b.instance_flags.upload(iflags.data(), iflags.size() * sizeof(uint32_t), s), "upload instances");
     uint32_t families = 0;
     for (int i = 0; i < d.num_materials; i++) {
