@@ -136,6 +136,28 @@ template <typename R, int MAXL>
 __device__ __forceinline__ void film_prepare(int L, const cx<R> *n, R cos0, FilmPrep<R, MAXL> &f) {
     f.L = L < MAXL ? L : MAXL;
     f.cos0 = cos0;
+    if constexpr (sizeof(R) == 4 && MAXL >= 1) {
+        // One film with real indices: Snell's law in real arithmetic. Without total
+        // internal reflection every cosine is real, and the Airy form in film_apply
+        // needs only the four Fresnel coefficients, not the interface matrices.
+        if (L == 1 && n[0].im == R(0) && n[1].im == R(0) && n[2].im == R(0)) {
+            const R n0 = n[0].re, n1 = n[1].re, n2 = n[2].re, c0 = cos0;
+            const R q01 = n0 / n1, q12 = n1 / n2;
+            const R sin1 = q01 * (q01 * (R(1) - c0 * c0));  // sin^2 in the film
+            const R sin2 = q12 * (q12 * sin1);              // and in the substrate
+            if (sin1 <= R(1) && sin2 <= R(1)) {
+                const R c1 = sqrtf(R(1) - sin1), c2 = sqrtf(R(1) - sin2);
+                f.airy = true;
+                f.n_layer[0] = cmk(n1, R(0));
+                f.cos_layer[0] = cmk(c1, R(0));
+                f.rs01 = (n0 * c0 - n1 * c1) / (n0 * c0 + n1 * c1);
+                f.rs12 = (n1 * c1 - n2 * c2) / (n1 * c1 + n2 * c2);
+                f.rp01 = (n1 * c0 - n0 * c1) / (n1 * c0 + n0 * c1);
+                f.rp12 = (n2 * c1 - n1 * c2) / (n2 * c1 + n1 * c2);
+                return;
+            }
+        }
+    }
     cx<R> cos_cur = cmk(cos0, R(0));
     cx<R> sin_next = n[0] / n[1];
     sin_next = sin_next * (sin_next * (cmk(R(1), R(0)) - cos_cur * cos_cur));
@@ -161,24 +183,15 @@ __device__ __forceinline__ void film_prepare(int L, const cx<R> *n, R cos0, Film
     f.n_out = n[f.L + 1];
     f.cos_out = cos_next;
     f.airy = false;
-    if constexpr (sizeof(R) == 4 && MAXL >= 1) {
-        if (f.L == 1 && n[0].im == R(0) && n[1].im == R(0) && n[2].im == R(0) && f.cos_layer[0].im == R(0) &&
-            cos_next.im == R(0)) {
-            const R n0 = n[0].re, n1 = n[1].re, n2 = n[2].re, c0 = cos0, c1 = f.cos_layer[0].re, c2 = cos_next.re;
-            f.airy = true;
-            f.rs01 = (n0 * c0 - n1 * c1) / (n0 * c0 + n1 * c1);
-            f.rs12 = (n1 * c1 - n2 * c2) / (n1 * c1 + n2 * c2);
-            f.rp01 = (n1 * c0 - n0 * c1) / (n1 * c0 + n0 * c1);
-            f.rp12 = (n2 * c1 - n1 * c2) / (n2 * c1 + n1 * c2);
-        }
-    }
 }
 
 // Reflectance of one film from its two interface coefficients and the cosine of the
-// round-trip phase (Airy summation, the closed form of the 2x2 product), ratio in double.
+// round-trip phase (Airy summation, the closed form of the 2x2 product). The
+// denominator is at least (1 - |r01 r12|)^2, far from zero for real indices, so FP32
+// keeps it within a few 1e-7 of FP64.
 __device__ __forceinline__ float airy_r(float r01, float r12, float cos2phi) {
-    const double a = r01, b = r12, ab = a * b, c = cos2phi;
-    return float((a * a + b * b + 2 * ab * c) / (1 + ab * ab + 2 * ab * c));
+    const float ab = r01 * r12, t = 2 * ab * cos2phi;
+    return (r01 * r01 + r12 * r12 + t) / (1 + ab * ab + t);
 }
 
 // Layer phases at one wavelength; k = 2 pi / lambda, d[j] in nm.
