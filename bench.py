@@ -47,7 +47,7 @@ W, H, SPP, DEPTH = 1920, 1080, 256, 16
 # capture summarised in the named profile (one launch of the same kernel on the same
 # scene); the JSON line scales the bytes to the average launch as `traffic`.
 PROFILED = {
-    "intersect": {"dram_bytes_per_item": (96.875264e6 + 51.161856e6) / 2073600, "issue_slot_utilisation": 0.6192,
+    "intersect": {"dram_bytes_per_item": (89.418496e6 + 56.283136e6) / 2073600, "issue_slot_utilisation": 0.5631,
                   "profile": "profiles/k_intersect_thinfilm_1080p.md"},
 }
 
