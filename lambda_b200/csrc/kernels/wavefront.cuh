@@ -170,6 +170,63 @@ __device__ __forceinline__ int material_of(const DeviceScene &sc, int inst_mater
     return inst_material >= 0 ? inst_material : prim_material(load_prim(sc, obj));
 }
 
+// Closest hit of path p (renderer.h:94-131). A miss or an emitter hit records the
+// path's emission term and returns -1: the path ends. Any other hit is stored for the
+// shade kernels and its material family returned: 0 Lambertian, 1 mirror or
+// dielectric, 2 thin film.
+template <int K>
+__device__ __forceinline__ int trace_path(const DeviceScene &sc, const PathState &ps, int p, const WideStack &st_a,
+                                          const WideStack &st_b) {
+    const float4 o4 = ps.ray_o[p], d4 = ps.ray_d[p];
+    const f3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
+    Hit h;
+    bool overflow = false;
+    const bool hit = closest_hit_w<K>(sc, o, d, h, overflow, st_a, st_b);
+    if (overflow) atomicOr(ps.error, 1);
+    const bool specular = d4.w != 0.0f;
+    const float prev_pdf = o4.w;
+    const bool lights = sc.total_light_power > 0;
+    if (!hit) {
+        const s4 lam = from_f4(ps.lam[p]);
+        float w = 1;
+        if (!specular && lights)
+            w = power_heuristic(prev_pdf, (1 / (4 * kPi)) * sc.light_power[sc.num_lights - 1] / sc.total_light_power);
+        const s4 T = from_f4(ps.throughput[p]);
+        ps.emit[p] = to_f4(T * background_eval(sc, d, lam) * w);
+    } else {
+        const InstanceRef ir = instance_ref(sc, h.instance);
+        const int4 ih = ir.header();
+        const int mat = material_of(sc, ih.w, h.object);
+        const int4 m = __ldg(&sc.materials[mat]);
+        if (m.x == kEmissive) {
+            float w = 1;
+            if (!specular && lights) {
+                float M[16], Mi[16];
+                ir.load_m(M, 0);
+                ir.load_m(Mi, 1);
+                const Prim pr = load_prim(sc, h.object);
+                const f3 c0 = mk(M[0], M[4], M[8]);
+                const float light_power = prim_area(pr) * length_sq(c0) * sc.material_emission[mat];
+                const float pdf = prim_pdf(pr, xform(Mi, o, 1), normalize(xform(Mi, d, 0)));
+                w = power_heuristic(prev_pdf, pdf * light_power / sc.total_light_power);
+            }
+            ShadePoint sp;
+            sp.point = h.point;
+            sp.u = h.u;
+            sp.v = h.v;
+            const s4 lam = from_f4(ps.lam[p]);
+            const s4 T = from_f4(ps.throughput[p]);
+            ps.emit[p] = to_f4(T * spectrum_texture4(sc, m.y, sp, lam) * w);
+        } else {
+            ps.hit_p[p] = make_float4(h.point.x, h.point.y, h.point.z, h.u);
+            ps.hit_n[p] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.v);
+            ps.hit_id[p] = make_int4(mat, h.object, h.front ? 1 : 0, h.instance);
+            return m.x == kLambertian ? 0 : (m.x == kThinFilm ? 2 : 1);
+        }
+    }
+    return -1;
+}
+
 // Closest hit; misses and emitter hits record their emission term and end the
 // path (renderer.h:105-131); other hits go to their material's queue.
 template <int K>
@@ -185,53 +242,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParam
         int p = 0, family = -1;
         if (idx < n) {
             p = q[idx];
-            const float4 o4 = ps.ray_o[p], d4 = ps.ray_d[p];
-            const f3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
-            Hit h;
-            bool overflow = false;
-            const bool hit = closest_hit_w<K>(sc, o, d, h, overflow, st_a, st_b);
-            if (overflow) atomicOr(ps.error, 1);
-            const bool specular = d4.w != 0.0f;
-            const float prev_pdf = o4.w;
-            const bool lights = sc.total_light_power > 0;
-            if (!hit) {
-                const s4 lam = from_f4(ps.lam[p]);
-                float w = 1;
-                if (!specular && lights)
-                    w = power_heuristic(prev_pdf, (1 / (4 * kPi)) * sc.light_power[sc.num_lights - 1] / sc.total_light_power);
-                const s4 T = from_f4(ps.throughput[p]);
-                ps.emit[p] = to_f4(T * background_eval(sc, d, lam) * w);
-            } else {
-                const InstanceRef ir = instance_ref(sc, h.instance);
-                const int4 ih = ir.header();
-                const int mat = material_of(sc, ih.w, h.object);
-                const int4 m = __ldg(&sc.materials[mat]);
-                if (m.x == kEmissive) {
-                    float w = 1;
-                    if (!specular && lights) {
-                        float M[16], Mi[16];
-                        ir.load_m(M, 0);
-                        ir.load_m(Mi, 1);
-                        const Prim pr = load_prim(sc, h.object);
-                        const f3 c0 = mk(M[0], M[4], M[8]);
-                        const float light_power = prim_area(pr) * length_sq(c0) * sc.material_emission[mat];
-                        const float pdf = prim_pdf(pr, xform(Mi, o, 1), normalize(xform(Mi, d, 0)));
-                        w = power_heuristic(prev_pdf, pdf * light_power / sc.total_light_power);
-                    }
-                    ShadePoint sp;
-                    sp.point = h.point;
-                    sp.u = h.u;
-                    sp.v = h.v;
-                    const s4 lam = from_f4(ps.lam[p]);
-                    const s4 T = from_f4(ps.throughput[p]);
-                    ps.emit[p] = to_f4(T * spectrum_texture4(sc, m.y, sp, lam) * w);
-                } else {
-                    ps.hit_p[p] = make_float4(h.point.x, h.point.y, h.point.z, h.u);
-                    ps.hit_n[p] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.v);
-                    ps.hit_id[p] = make_int4(mat, h.object, h.front ? 1 : 0, h.instance);
-                    family = m.x == kLambertian ? 0 : (m.x == kThinFilm ? 2 : 1);
-                }
-            }
+            family = trace_path<K>(sc, ps, p, st_a, st_b);
         }
         for (int f = 0; f < 3; f++) {
             const int slot = warp_push(&ps.counts[queue_slot(bounce, kQLambert + f)], family == f);
@@ -293,6 +304,67 @@ __device__ __forceinline__ bool finish_scatter(const PathState &ps, const ShadeI
     return alive;
 }
 
+// Lambertian hit of path p: next-event estimation (renderer.h:133-175), leaving the
+// NEE ray in the path state and setting `nee`, then cosine-weighted scatter
+// (material.h:151-172). Returns whether the path continues.
+__device__ __forceinline__ bool lambert_path(const DeviceScene &sc, const PathState &ps, int p, int bounce, bool &nee) {
+    const ShadeIn s = load_shade(ps, sc, p);
+    Rng rng = path_rng(ps, p);
+    const s4 albedo = spectrum_texture4(sc, s.m.y, s.sp, s.lam);
+    if (sc.total_light_power > 0) {
+        const float target = sc.total_light_power * rng.next();
+        int li = sc.light_inst[0], lo = sc.light_obj[0];
+        float lp = sc.light_power[0];
+        for (int j = 0; j < sc.num_lights; j++) {
+            if (sc.light_cdf[j] >= target) {
+                li = sc.light_inst[j];
+                lo = sc.light_obj[j];
+                lp = sc.light_power[j];
+                break;
+            }
+        }
+        f3 ldir;
+        float lpdf;
+        if (li != -1) {
+            const Prim pr = load_prim(sc, lo);
+            if (sc.instance_flags[li] & 1u) {
+                const f3 zero = mk(0.0f, 0.0f, 0.0f);
+                const f3 local = s.sp.point + zero;
+                ldir = normalize(prim_sample(pr, local, rng) + zero);
+                lpdf = prim_pdf(pr, local, normalize(ldir + zero));
+            } else {
+                const InstanceRef lr = instance_ref(sc, li);
+                float M[16], Mi[16];
+                lr.load_m(M, 0);
+                lr.load_m(Mi, 1);
+                const f3 local = xform(Mi, s.sp.point, 1);
+                ldir = normalize(xform(M, prim_sample(pr, local, rng), 0));
+                lpdf = prim_pdf(pr, local, normalize(xform(Mi, ldir, 0)));
+            }
+        } else {
+            ldir = random_unit_vector(rng);
+            lpdf = 1 / (4 * kPi);
+        }
+        const float cos_t = dot(s.nrm, ldir);
+        if (lpdf > 0 && cos_t > 0) {
+            lpdf *= lp / sc.total_light_power;
+            const s4 att = cos_t <= 0 ? s4_fill(0) : albedo / kPi;
+            const float spdf = cos_t > 0 ? cos_t / kPi : 0;
+            const float w = power_heuristic(lpdf, spdf);
+            ps.sh_o[p] = make_float4(s.sp.point.x, s.sp.point.y, s.sp.point.z, w);
+            ps.sh_d[p] = make_float4(ldir.x, ldir.y, ldir.z, lpdf);
+            ps.sh_a[p] = to_f4((s.T * att) * cos_t);
+            ps.sh_light[p] = make_int2(li, lo);
+            nee = true;
+        }
+    }
+    const f3 nd = random_in_hemisphere(s.nrm, rng);
+    const float cl = dot(s.nrm, nd);
+    const s4 att = cl <= 0 ? s4_fill(0) : albedo / kPi;
+    const float pdf = cl > 0 ? cl / kPi : 0;
+    return finish_scatter(ps, s, rng, bounce, att, nd, pdf, false);
+}
+
 // Lambertian: next-event estimation (renderer.h:133-175), then cosine-weighted
 // scatter (material.h:151-172).
 LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_lambert(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
@@ -306,61 +378,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_lambert(int bounce, RenderP
         int p = 0;
         if (idx < n) {
             p = q[idx];
-            const ShadeIn s = load_shade(ps, sc, p);
-            Rng rng = path_rng(ps, p);
-            const s4 albedo = spectrum_texture4(sc, s.m.y, s.sp, s.lam);
-            if (sc.total_light_power > 0) {
-                const float target = sc.total_light_power * rng.next();
-                int li = sc.light_inst[0], lo = sc.light_obj[0];
-                float lp = sc.light_power[0];
-                for (int j = 0; j < sc.num_lights; j++) {
-                    if (sc.light_cdf[j] >= target) {
-                        li = sc.light_inst[j];
-                        lo = sc.light_obj[j];
-                        lp = sc.light_power[j];
-                        break;
-                    }
-                }
-                f3 ldir;
-                float lpdf;
-                if (li != -1) {
-                    const Prim pr = load_prim(sc, lo);
-                    if (sc.instance_flags[li] & 1u) {
-                        const f3 zero = mk(0.0f, 0.0f, 0.0f);
-                        const f3 local = s.sp.point + zero;
-                        ldir = normalize(prim_sample(pr, local, rng) + zero);
-                        lpdf = prim_pdf(pr, local, normalize(ldir + zero));
-                    } else {
-                        const InstanceRef lr = instance_ref(sc, li);
-                        float M[16], Mi[16];
-                        lr.load_m(M, 0);
-                        lr.load_m(Mi, 1);
-                        const f3 local = xform(Mi, s.sp.point, 1);
-                        ldir = normalize(xform(M, prim_sample(pr, local, rng), 0));
-                        lpdf = prim_pdf(pr, local, normalize(xform(Mi, ldir, 0)));
-                    }
-                } else {
-                    ldir = random_unit_vector(rng);
-                    lpdf = 1 / (4 * kPi);
-                }
-                const float cos_t = dot(s.nrm, ldir);
-                if (lpdf > 0 && cos_t > 0) {
-                    lpdf *= lp / sc.total_light_power;
-                    const s4 att = cos_t <= 0 ? s4_fill(0) : albedo / kPi;
-                    const float spdf = cos_t > 0 ? cos_t / kPi : 0;
-                    const float w = power_heuristic(lpdf, spdf);
-                    ps.sh_o[p] = make_float4(s.sp.point.x, s.sp.point.y, s.sp.point.z, w);
-                    ps.sh_d[p] = make_float4(ldir.x, ldir.y, ldir.z, lpdf);
-                    ps.sh_a[p] = to_f4((s.T * att) * cos_t);
-                    ps.sh_light[p] = make_int2(li, lo);
-                    nee = true;
-                }
-            }
-            const f3 nd = random_in_hemisphere(s.nrm, rng);
-            const float cl = dot(s.nrm, nd);
-            const s4 att = cl <= 0 ? s4_fill(0) : albedo / kPi;
-            const float pdf = cl > 0 ? cl / kPi : 0;
-            alive = finish_scatter(ps, s, rng, bounce, att, nd, pdf, false);
+            alive = lambert_path(sc, ps, p, bounce, nee);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
@@ -376,6 +394,39 @@ __device__ __forceinline__ float pow5(float x) {
     return float(x2 * x2 * double(x));
 }
 
+// Mirror or dielectric hit of path p (material.h:174-226). Returns whether the path
+// continues.
+__device__ __forceinline__ bool specular_path(const DeviceScene &sc, const PathState &ps, int p, int bounce) {
+    const ShadeIn s = load_shade(ps, sc, p);
+    Rng rng = path_rng(ps, p);
+    s4 att;
+    f3 nd;
+    if (s.m.x == kMirror) {
+        nd = reflected(s.d, s.nrm);
+        att = spectrum_texture4(sc, s.m.y, s.sp, s.lam);
+    } else {
+        const float factor = pow5(1 + dot(s.d, s.nrm));
+        const float n0h = spectrum_at(sc, s.m.y, s.lam.v[0]);
+        const float n1h = spectrum_at(sc, s.m.z, s.lam.v[0]);
+        const float ratio = s.front ? n0h / n1h : n1h / n0h;
+        float r0 = (n0h - n1h) / (n0h + n1h);
+        r0 *= r0;
+        const float rh = r0 + (1 - r0) * factor;
+        const bool refl = rng.next() < rh;
+        nd = refl ? reflected(s.d, s.nrm) : refracted(s.d, s.nrm, ratio);
+        att.v[0] = 1;
+        for (int k = 1; k < kHero; k++) {
+            const float a0 = spectrum_at(sc, s.m.y, s.lam.v[k]);
+            const float a1 = spectrum_at(sc, s.m.z, s.lam.v[k]);
+            float rr = (a0 - a1) / (a0 + a1);
+            rr *= rr;
+            const float r = rr + (1 - rr) * factor;
+            att.v[k] = refl ? r / rh : (fabsf(a0 - n0h) < kEps && fabsf(a1 - n1h) < kEps) ? (1 - r) / (1 - rh) : 0;
+        }
+    }
+    return finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
+}
+
 // Mirror and dielectric (material.h:174-226).
 LAMBDA_KERNEL void __launch_bounds__(256) k_shade_specular(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
     const int n = ps.counts[queue_slot(bounce, kQSpecular)];
@@ -388,34 +439,7 @@ LAMBDA_KERNEL void __launch_bounds__(256) k_shade_specular(int bounce, RenderPar
         int p = 0;
         if (idx < n) {
             p = q[idx];
-            const ShadeIn s = load_shade(ps, sc, p);
-            Rng rng = path_rng(ps, p);
-            s4 att;
-            f3 nd;
-            if (s.m.x == kMirror) {
-                nd = reflected(s.d, s.nrm);
-                att = spectrum_texture4(sc, s.m.y, s.sp, s.lam);
-            } else {
-                const float factor = pow5(1 + dot(s.d, s.nrm));
-                const float n0h = spectrum_at(sc, s.m.y, s.lam.v[0]);
-                const float n1h = spectrum_at(sc, s.m.z, s.lam.v[0]);
-                const float ratio = s.front ? n0h / n1h : n1h / n0h;
-                float r0 = (n0h - n1h) / (n0h + n1h);
-                r0 *= r0;
-                const float rh = r0 + (1 - r0) * factor;
-                const bool refl = rng.next() < rh;
-                nd = refl ? reflected(s.d, s.nrm) : refracted(s.d, s.nrm, ratio);
-                att.v[0] = 1;
-                for (int k = 1; k < kHero; k++) {
-                    const float a0 = spectrum_at(sc, s.m.y, s.lam.v[k]);
-                    const float a1 = spectrum_at(sc, s.m.z, s.lam.v[k]);
-                    float rr = (a0 - a1) / (a0 + a1);
-                    rr *= rr;
-                    const float r = rr + (1 - rr) * factor;
-                    att.v[k] = refl ? r / rh : (fabsf(a0 - n0h) < kEps && fabsf(a1 - n1h) < kEps) ? (1 - r) / (1 - rh) : 0;
-                }
-            }
-            alive = finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
+            alive = specular_path(sc, ps, p, bounce);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
@@ -517,6 +541,23 @@ __device__ __forceinline__ void thin_film_thickness(const DeviceScene &sc, const
     for (int k = 0; k < L; k++) thick[k] = scalar_texture(sc, sc.material_props[s.m.w + k], s.sp.point);
 }
 
+// Thin-film hit of path p, evaluated exactly: in FP32 (within 1e-5 of FP64), or with
+// kFp64 in the reference's complex double arithmetic. Returns whether the path
+// continues.
+template <bool kFp64>
+__device__ __forceinline__ bool film_path(const DeviceScene &sc, const PathState &ps, int p, int bounce) {
+    const ShadeIn s = load_shade(ps, sc, p);
+    float thick[kMaxFilmLayers];
+    thin_film_thickness(sc, s, thick);
+    const s4 R = kFp64 ? thin_film_r4_fp64(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick)
+                       : thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+    Rng rng = path_rng(ps, p);
+    s4 att;
+    f3 nd;
+    thin_film_scatter(sc, s, R, rng, att, nd);
+    return finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
+}
+
 // Thin film evaluated exactly over the bounce's thin-film queue: in FP32 (within 1e-5
 // of FP64), or with kFp64 in the reference's complex double arithmetic.
 template <bool kFp64>
@@ -531,20 +572,43 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, Rend
         int p = 0;
         if (idx < n) {
             p = q[idx];
-            const ShadeIn s = load_shade(ps, sc, p);
-            float thick[kMaxFilmLayers];
-            thin_film_thickness(sc, s, thick);
-            const s4 R = kFp64 ? thin_film_r4_fp64(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick)
-                               : thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
-            Rng rng = path_rng(ps, p);
-            s4 att;
-            f3 nd;
-            thin_film_scatter(sc, s, R, rng, att, nd);
-            alive = finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
+            alive = film_path<kFp64>(sc, ps, p, bounce);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
         if (alive) q_next[slot] = p;
     }
+}
+
+// The NEE shadow ray of path p (renderer.h:166-173): if nothing occludes the light,
+// its emission times the stored weights is added to the path's NEE radiance.
+template <int K>
+__device__ __forceinline__ void shadow_path(const DeviceScene &sc, const PathState &ps, int p, const WideStack &st_a,
+                                            const WideStack &st_b) {
+    const float4 o = ps.sh_o[p], dd = ps.sh_d[p];
+    const int2 light = ps.sh_light[p];
+    const f3 d = mk(dd.x, dd.y, dd.z);
+    Hit lh;
+    bool overflow = false;
+    if (!occluded_w<K>(sc, mk(o.x, o.y, o.z), d, light.x, light.y, lh, overflow, st_a, st_b)) {
+        const s4 lam = from_f4(ps.lam[p]);
+        s4 e;
+        if (light.x != -1) {
+            const int4 ih = instance_ref(sc, light.x).header();
+            const int mat = material_of(sc, ih.w, light.y);
+            const int4 m = __ldg(&sc.materials[mat]);
+            ShadePoint sp;
+            sp.point = lh.point;
+            sp.u = lh.u;
+            sp.v = lh.v;
+            e = m.x == kEmissive ? spectrum_texture4(sc, m.y, sp, lam) : s4_fill(0);
+        } else {
+            e = background_eval(sc, d, lam);
+        }
+        const s4 a = from_f4(ps.sh_a[p]);
+        const s4 contrib = ((a * e) * o.w) / dd.w;
+        ps.radiance[p] = to_f4(from_f4(ps.radiance[p]) + contrib);
+    }
+    if (overflow) atomicOr(ps.error, 1);
 }
 
 template <int K>
@@ -556,31 +620,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams r
     const int stride = gridDim.x * blockDim.x;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
         const int p = ps.shadow_queue[idx];
-        const float4 o = ps.sh_o[p], dd = ps.sh_d[p];
-        const int2 light = ps.sh_light[p];
-        const f3 d = mk(dd.x, dd.y, dd.z);
-        Hit lh;
-        bool overflow = false;
-        if (!occluded_w<K>(sc, mk(o.x, o.y, o.z), d, light.x, light.y, lh, overflow, st_a, st_b)) {
-            const s4 lam = from_f4(ps.lam[p]);
-            s4 e;
-            if (light.x != -1) {
-                const int4 ih = instance_ref(sc, light.x).header();
-                const int mat = material_of(sc, ih.w, light.y);
-                const int4 m = __ldg(&sc.materials[mat]);
-                ShadePoint sp;
-                sp.point = lh.point;
-                sp.u = lh.u;
-                sp.v = lh.v;
-                e = m.x == kEmissive ? spectrum_texture4(sc, m.y, sp, lam) : s4_fill(0);
-            } else {
-                e = background_eval(sc, d, lam);
-            }
-            const s4 a = from_f4(ps.sh_a[p]);
-            const s4 contrib = ((a * e) * o.w) / dd.w;
-            ps.radiance[p] = to_f4(from_f4(ps.radiance[p]) + contrib);
-        }
-        if (overflow) atomicOr(ps.error, 1);
+        shadow_path<K>(sc, ps, p, st_a, st_b);
     }
 }
 
