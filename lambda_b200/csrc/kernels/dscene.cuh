@@ -349,16 +349,19 @@ struct InstanceRef {
 
 __device__ __forceinline__ InstanceRef instance_ref(const DeviceScene &s, int i) { return InstanceRef{s.instances + 9 * size_t(i)}; }
 
-// Full attributes of a hit on primitive p in instance space (object.h:301-400).
-__device__ __forceinline__ void prim_attributes(const DeviceScene &s, int obj, const Prim &p, f3 o, f3 d, float t, Hit &h) {
+// Full attributes of a hit on primitive p in instance space (object.h:301-400). A
+// sphere's (u, v) takes an atan2 and an acos; without want_uv (its material reads
+// no (u, v)) they are left 0.
+__device__ __forceinline__ void prim_attributes(const DeviceScene &s, int obj, const Prim &p, f3 o, f3 d, float t, Hit &h,
+                                                bool want_uv = true) {
     const int type = prim_type(p);
     h.t = t;
     h.point = o + t * d;
     if (type == 0) {
         const f3 c = mk(p.p0.x, p.p0.y, p.p0.z);
         h.normal = normalize(h.point - c);
-        h.u = (atan2f(-h.normal.z, h.normal.x) + kPi) / (2 * kPi);
-        h.v = acosf(-h.normal.y) / kPi;
+        h.u = want_uv ? (atan2f(-h.normal.z, h.normal.x) + kPi) / (2 * kPi) : 0.0f;
+        h.v = want_uv ? acosf(-h.normal.y) / kPi : 0.0f;
         h.front = dot(d, h.normal) < 0;
         if (!h.front) h.normal = h.normal * -1.0f;
         return;
@@ -525,7 +528,10 @@ __device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, 
     }
     const InstanceRef ir = instance_ref(s, best_inst);
     const Ray3 lr = to_local(s.instance_flags[best_inst], ir, wr);
-    prim_attributes(s, best_obj, load_prim(s, best_obj), lr.o, lr.d, best, h);
+    const Prim pr = load_prim(s, best_obj);
+    const int inst_material = ir.header().w;
+    const int mat = inst_material >= 0 ? inst_material : prim_material(pr);
+    prim_attributes(s, best_obj, pr, lr.o, lr.d, best, h, s.material_uv[mat] != 0);
     h.instance = best_inst;
     h.object = best_obj;
     to_world(s, best_inst, ir, h);

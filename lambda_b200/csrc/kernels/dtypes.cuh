@@ -33,6 +33,7 @@ struct DeviceScene {
     const float *light_power;
     const float *light_cdf;      // running sums of light_power in list order
     const float *material_emission;  // per material: average emission (0 if not emissive)
+    const uint8_t *material_uv;      // per material: 1 if a texture it evaluates reads the hit's (u, v)
     const uint32_t *instance_flags;  // bit 0: transform and inverse are exactly the identity; bit 1: also
                                      // alone in its TLAS leaf, whose box is its BLAS root's box
     const float *cie;            // [471][3] as float

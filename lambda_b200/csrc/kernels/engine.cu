@@ -414,6 +414,16 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
         std::memcpy(&sc, &t.scale, 4);
         sptex[i] = make_int4(t.type, t.value1, t.value2, sc);
     }
+    // materials whose spectrum texture (albedo or emission) is a checker read the hit's
+    // (u, v); no other texture does (scalar textures read the point)
+    std::vector<uint8_t> muv(std::max(d.num_materials, 1), 0);
+    for (int i = 0; i < d.num_materials; i++) {
+        const lambda_material &m = d.materials[i];
+        if (m.type != LAMBDA_MATERIAL_LAMBERTIAN && m.type != LAMBDA_MATERIAL_MIRROR && m.type != LAMBDA_MATERIAL_EMISSIVE)
+            continue;
+        const int t = m.p[0];
+        muv[i] = (t < 0 || t >= d.num_spectrum_textures || d.spectrum_textures[t].type == LAMBDA_SPECTRUM_CHECKER) ? 1 : 0;
+    }
     std::vector<float> cdf(d.num_lights);
     float run = 0;
     for (int i = 0; i < d.num_lights; i++) {
@@ -446,6 +456,7 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     CK(b.light_power.upload(d.light_powers, size_t(d.num_lights) * sizeof(float), s), "upload lights");
     CK(b.light_cdf.upload(cdf.data(), cdf.size() * sizeof(float), s), "upload lights");
     CK(b.material_emission.upload(emission.data(), emission.size() * sizeof(float), s), "upload materials");
+    CK(b.material_uv.upload(muv.data(), muv.size(), s), "upload materials");
     CK(b.cie.upload(cie.data(), cie.size() * sizeof(float), s), "upload CIE table");
     CK(b.perm.upload(kPerlinPermutation, sizeof(kPerlinPermutation), s), "upload permutation");
     CK(b.worley.upload(worley.data(), worley.size() * sizeof(float4), s), "upload Worley lattice");
@@ -518,6 +529,7 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     ds.light_power = b.light_power.as<float>();
     ds.light_cdf = b.light_cdf.as<float>();
     ds.material_emission = b.material_emission.as<float>();
+    ds.material_uv = b.material_uv.as<uint8_t>();
     ds.instance_flags = b.instance_flags.as<uint32_t>();
     ds.families = families;
     ds.cie = b.cie.as<float>();
