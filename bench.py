@@ -380,7 +380,8 @@ def run_batch(args, ctx, lb, torch, rank, world, local):
             "config": {"workload": BATCH_WORKLOAD, "paths_per_step": paths, "jobs": len(descs),
                        "l2": "flushed between timed steps (256 MB write)",
                        "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
-                                  "grid_scale": tuning.grid_scale, "max_pixels": tuning.max_pixels}},
+                                  "grid_scale": tuning.grid_scale, "max_pixels": tuning.max_pixels,
+                                  "bvh_width": tuning.bvh_width}},
             "e2e": {"value": world * paths * args.steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": len(hdescs) * C.sizeof(N.Job), "scene": "resident",
                     "d2h_bytes_per_step": sum(d.settings.width * d.settings.height * 12 for d in descs)},
@@ -552,7 +553,8 @@ def main():
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
                        "paths_per_step": paths_per_step,
                        "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
-                                  "grid_scale": tuning.grid_scale, "source": "lambda_autotune, 1-spp probe"}},
+                                  "grid_scale": tuning.grid_scale, "bvh_width": tuning.bvh_width,
+                                  "source": "lambda_autotune, 1-spp probe"}},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 12},
             "gpu_launches": launches,
