@@ -47,7 +47,7 @@ W, H, SPP, DEPTH = 1920, 1080, 256, 16
 # capture summarised in the named profile (one launch of the same kernel on the same
 # scene); the JSON line scales the bytes to the average launch as `traffic`.
 PROFILED = {
-    "intersect": {"dram_bytes_per_item": (89.418496e6 + 56.283136e6) / 2073600, "issue_slot_utilisation": 0.5631,
+    "intersect": {"dram_bytes_per_item": (89.619968e6 + 50.342656e6) / 2073600, "issue_slot_utilisation": 0.6455,
                   "profile": "profiles/k_intersect_thinfilm_1080p.md"},
 }
 
@@ -322,6 +322,15 @@ BATCH_WORKLOAD = ("batch32: 32 views of the 1,048,576-triangle Perlin-displaced 
 BATCH_POSES = {"target": (0.0, 0.0, 0.0), "distance": (2.6, 4.0), "height": (-1.0, 1.5), "jitter": 0.2}
 
 
+def launch_shapes(args, ctx, probe):
+    """The autotuner's pick on `probe`, or the shapes --tuning fixes."""
+    if args.tuning:
+        tb, sb, gs, width = (int(v) for v in args.tuning.split(","))
+        ctx.set_tuning(tb, sb, gs, 0, width)
+        return ctx.tuning(), "fixed by --tuning"
+    return ctx.autotune(probe), "lambda_autotune, 1-spp probe"
+
+
 def run_batch(args, ctx, lb, torch, rank, world, local):
     """Batched workload: one lambda_render_batch of 32 views of the 1,048,576-triangle
     mesh scene (device outputs), timed on the device, against the same 32 jobs
@@ -340,7 +349,8 @@ def run_batch(args, ctx, lb, torch, rank, world, local):
     outs = [torch.empty((d.settings.height, d.settings.width, 3), dtype=torch.float32, device=f"cuda:{local}")
             for d in descs]
     paths = sum(d.settings.width * d.settings.height * d.settings.samples for d in descs)
-    tuning = ctx.autotune(scene.render_desc(seed=3, flags=lb.RENDER_THINFILM_SURROGATE, samples=1))
+    tuning, tuning_source = launch_shapes(args, ctx, scene.render_desc(seed=3, flags=lb.RENDER_THINFILM_SURROGATE,
+                                                                       samples=1))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(args.warmup):
         ctx.render_batch(descs, outs)
@@ -381,7 +391,7 @@ def run_batch(args, ctx, lb, torch, rank, world, local):
                        "l2": "flushed between timed steps (256 MB write)",
                        "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
                                   "grid_scale": tuning.grid_scale, "max_pixels": tuning.max_pixels,
-                                  "bvh_width": tuning.bvh_width}},
+                                  "bvh_width": tuning.bvh_width, "source": tuning_source}},
             "e2e": {"value": world * paths * args.steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": len(hdescs) * C.sizeof(N.Job), "scene": "resident",
                     "d2h_bytes_per_step": sum(d.settings.width * d.settings.height * 12 for d in descs)},
@@ -403,6 +413,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
     ap.add_argument("--no-compare", action="store_true", help="skip the surrogate/exact comparison")
+    ap.add_argument("--tuning", default="", metavar="TB,SB,GS,WIDTH",
+                    help="fixed launch shapes (trace block, shade block, grid scale, BVH width) instead of the "
+                         "autotuner's, e.g. for reproducible profiler captures")
     ap.add_argument("--workload", default="thinfilm1080p", choices=["thinfilm1080p", "batch32", "film_queries"],
                     help="batch32: 32 random-pose views of the 1M-triangle mesh scene in one batched render; "
                          "film_queries: the three film evaluators on 2^24 device-resident queries")
@@ -455,7 +468,7 @@ def main():
         return 0
 
     # launch shapes from the autotuner, timed on a 1-spp frame of the same scene
-    tuning = ctx.autotune(scene.render_desc(seed=sc.seed, flags=flags, samples=1))
+    tuning, tuning_source = launch_shapes(args, ctx, scene.render_desc(seed=sc.seed, flags=flags, samples=1))
 
     for _ in range(args.warmup):
         ctx.render(desc, out=dev_out)
@@ -554,7 +567,7 @@ def main():
                        "paths_per_step": paths_per_step,
                        "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
                                   "grid_scale": tuning.grid_scale, "bvh_width": tuning.bvh_width,
-                                  "source": "lambda_autotune, 1-spp probe"}},
+                                  "source": tuning_source}},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 12},
             "gpu_launches": launches,
