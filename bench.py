@@ -328,7 +328,7 @@ def launch_shapes(args, ctx, probe):
         tb, sb, gs, width = (int(v) for v in args.tuning.split(","))
         ctx.set_tuning(tb, sb, gs, 0, width)
         return ctx.tuning(), "fixed by --tuning"
-    return ctx.autotune(probe), "lambda_autotune, 1-spp probe"
+    return ctx.autotune(probe), f"lambda_autotune, {probe.settings.samples}-spp probe"
 
 
 def run_batch(args, ctx, lb, torch, rank, world, local):
@@ -349,8 +349,18 @@ def run_batch(args, ctx, lb, torch, rank, world, local):
     outs = [torch.empty((d.settings.height, d.settings.width, 3), dtype=torch.float32, device=f"cuda:{local}")
             for d in descs]
     paths = sum(d.settings.width * d.settings.height * d.settings.samples for d in descs)
-    tuning, tuning_source = launch_shapes(args, ctx, scene.render_desc(seed=3, flags=lb.RENDER_THINFILM_SURROGATE,
-                                                                       samples=1))
+    # the batch autotuner on the same 32 views at 1/16 of their samples (256 -> 16,
+    # 64 -> 4, fewer -> 1): the probe keeps the batch's shape, late waves holding only
+    # the jobs with the most samples (a single probe view does not tell shapes apart)
+    probes = scenes.random_pose_jobs(scene, 32, seed=4, flags=lb.RENDER_THINFILM_SURROGATE, **BATCH_POSES)
+    for p in probes:
+        spp = max(1, p.settings.samples // 16)
+        root = int(round(spp ** 0.5))
+        p.settings.samples, p.settings.sqrt_samples = root * root, root
+    if args.tuning:
+        tuning, tuning_source = launch_shapes(args, ctx, None)
+    else:
+        tuning, tuning_source = ctx.autotune_batch(probes), "lambda_autotune_batch, the 32 views at 1/16 of their spp"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(args.warmup):
         ctx.render_batch(descs, outs)

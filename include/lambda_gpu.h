@@ -294,6 +294,10 @@ typedef struct lambda_tuning {
 } lambda_tuning;
 
 lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out);
+/* The same search over a batch: each candidate times lambda_render_batch of the n
+ * probe views (same thin-film mode; images in device memory allocated here), so the
+ * shapes suit many small and uneven jobs rendered together. */
+lambda_status lambda_autotune_batch(lambda_ctx *ctx, const lambda_render_desc *probes, int32_t n, lambda_tuning *out);
 lambda_status lambda_set_tuning(lambda_ctx *ctx, const lambda_tuning *tuning);
 lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning *tuning);
 

@@ -272,6 +272,14 @@ class Context:
         self._check(self._lib.lambda_autotune(self._h, C.byref(probe), C.byref(t)))
         return t
 
+    def autotune_batch(self, probes) -> N.Tuning:
+        """Picks the launch shapes by timing batched renders of `probes`
+        (lambda_autotune_batch)."""
+        arr = (N.RenderDesc * len(probes))(*probes)
+        t = N.Tuning()
+        self._check(self._lib.lambda_autotune_batch(self._h, arr, len(probes), C.byref(t)))
+        return t
+
     def set_tuning(self, trace_block: int, shade_block: int, grid_scale: int = 1, max_pixels: int = 0,
                    bvh_width: int = 4) -> None:
         t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels, bvh_width)

@@ -161,6 +161,7 @@ _SIGNATURES = {
     "lambda_render": (C.c_int, [_P, C.POINTER(RenderDesc), _P, _P]),
     "lambda_render_batch": (C.c_int, [_P, C.POINTER(Job), C.c_int32, _P]),
     "lambda_autotune": (C.c_int, [_P, C.POINTER(RenderDesc), C.POINTER(Tuning)]),
+    "lambda_autotune_batch": (C.c_int, [_P, C.POINTER(RenderDesc), C.c_int32, C.POINTER(Tuning)]),
     "lambda_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "lambda_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "lambda_get_render_stats": (C.c_int, [_P, C.POINTER(RenderStats)]),

@@ -1158,79 +1158,84 @@ extern "C" lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning 
     return LAMBDA_OK;
 }
 
-// Times the probe render (its output stays in device memory): first the three BVH
-// widths, then every block-shape candidate at the fastest width, each as the best
-// of three renders after one warm-up, and keeps the fastest. The
-// path-state capacity is set from free device memory: half of it, at the bytes of
-// path state and queues a pixel needs.
-extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out) {
-    if (!ctx || !probe) return LAMBDA_ERR_INVALID_ARGUMENT;
-    lambda_status s = check_settings(ctx, probe->settings);
-    if (s != LAMBDA_OK) return s;
+namespace {
+
+// Times renders of the probe views (their images stay in device memory) under every
+// combination of BVH width, traversal block, shading block and grid scale, each as
+// the best of three renders after one warm-up, and keeps the fastest. The path-state
+// capacity is set from free device memory: half of it, at the bytes of path state
+// and queues a pixel needs.
+lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, int n, lambda_tuning *out) {
+    if (!ctx || !probes || n < 1) return LAMBDA_ERR_INVALID_ARGUMENT;
+    size_t pixels = 0;
+    for (int i = 0; i < n; i++) {
+        lambda_status s = check_settings(ctx, probes[i].settings);
+        if (s != LAMBDA_OK) return s;
+        pixels += size_t(probes[i].settings.width) * probes[i].settings.height;
+    }
     if (!ctx->has_scene) return ctx->fail(LAMBDA_ERR_NO_SCENE, "no scene uploaded");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-    const size_t P = size_t(probe->settings.width) * probe->settings.height;
     DeviceBuffer img;
-    CK(img.reserve(P * 12), "allocate probe image");
-    lambda_job job{*probe, img.as<float>()};
-    job.desc.flags = (probe->flags & (LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_THINFILM_FP64)) |
-                     LAMBDA_RENDER_OUTPUT_DEVICE;
+    CK(img.reserve(pixels * 12), "allocate probe images");
+    std::vector<lambda_job> jobs(n);
+    size_t off = 0;
+    for (int i = 0; i < n; i++) {
+        jobs[i] = lambda_job{probes[i], img.as<float>() + off * 3};
+        jobs[i].desc.flags = (probes[0].flags & (LAMBDA_RENDER_THINFILM_SURROGATE | LAMBDA_RENDER_THINFILM_FP64)) |
+                             LAMBDA_RENDER_OUTPUT_DEVICE;
+        off += size_t(probes[i].settings.width) * probes[i].settings.height;
+    }
     const lambda_tuning keep = ctx->tuning;
     lambda_tuning best = keep;
     double best_ms = 1e300;
-    // the BVH width first, at the current block shapes, then the block shapes at that width
     // one warm-up render, then the best of three timed ones
     auto trial = [&](const lambda_tuning &t, double &ms) -> lambda_status {
         ctx->tuning = t;
-        lambda_status r = render_jobs(ctx, &job, 1, nullptr);
+        lambda_status r = render_jobs(ctx, jobs.data(), n, nullptr);
         ms = 1e300;
         for (int rep = 0; rep < 3 && r == LAMBDA_OK; rep++) {
-            r = render_jobs(ctx, &job, 1, nullptr);
+            r = render_jobs(ctx, jobs.data(), n, nullptr);
             ms = std::min(ms, ctx->stats.render_ms);
         }
         return r;
     };
-    for (int bw : {2, 4, 8}) {
-        double ms = 0;
-        const lambda_status r = trial(lambda_tuning{keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, bw}, ms);
-        if (r == LAMBDA_ERR_UNSUPPORTED) continue;  // stacks too deep for shared memory at this block size
-        if (r != LAMBDA_OK) {
-            ctx->tuning = keep;
-            img.release();
-            return r;
-        }
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = ctx->tuning;
-        }
-    }
-    const int width = best.bvh_width;
-    for (int tb : {64, 128, 256})
-        for (int sb : {64, 128, 256})
-            for (int gs : {1, 2}) {
-                double ms = 0;
-                const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, width}, ms);
-                if (r == LAMBDA_ERR_UNSUPPORTED) continue;
-                if (r != LAMBDA_OK) {
-                    ctx->tuning = keep;
-                    img.release();
-                    return r;
+    // every BVH width with every block shape: the best width can depend on the blocks
+    for (int bw : {2, 4, 8})
+        for (int tb : {64, 128, 256})
+            for (int sb : {64, 128, 256})
+                for (int gs : {1, 2}) {
+                    double ms = 0;
+                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw}, ms);
+                    if (r == LAMBDA_ERR_UNSUPPORTED) continue;  // stacks too deep for shared memory at this block size
+                    if (r != LAMBDA_OK) {
+                        ctx->tuning = keep;
+                        return r;
+                    }
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = ctx->tuning;
+                    }
                 }
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best = ctx->tuning;
-                }
-            }
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         // path state, queues, staged image, the surrogate's MLP rows, outputs and domain flags
         constexpr size_t kBytesPerPixel = 8 + 16 * 14 + 8 + 8 + 4 * 6 + 12 + 4 * 32 + 4 * 16 + 1;
         best.max_pixels = int32_t(std::min<size_t>((free_b / 2) / kBytesPerPixel, size_t(1) << 30));
     }
-    img.release();
     ctx->tuning = best;
     if (out) *out = best;
     return LAMBDA_OK;
+}
+
+}  // namespace
+
+extern "C" lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out) {
+    return autotune_views(ctx, probe, 1, out);
+}
+
+extern "C" lambda_status lambda_autotune_batch(lambda_ctx *ctx, const lambda_render_desc *probes, int32_t n,
+                                               lambda_tuning *out) {
+    return autotune_views(ctx, probes, n, out);
 }
 
 extern "C" lambda_status lambda_get_stage_times(const lambda_ctx *ctx, lambda_stage_time *out) {

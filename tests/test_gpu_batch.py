@@ -143,3 +143,23 @@ def test_batch_of_mesh_views_equals_single_renders(scene_dir, ctx):
     for d, img in zip(descs, imgs):
         assert img.mean() > 0
         assert _same(img, ctx.render(d)), f"job {d.settings.width}x{d.settings.height} spp {d.settings.samples}"
+
+
+def test_autotune_batch(film, ctx):
+    """The batch autotuner times batched renders of the probe views, installs a valid
+    choice, and launch shapes change no image."""
+    ctx.upload(film)
+    descs = _jobs(film, n=4, seed=8)
+    keep = ctx.tuning()
+    want = ctx.render_batch(descs)
+    try:
+        t = ctx.autotune_batch(descs)
+        assert t.trace_block in (64, 128, 256) and t.shade_block in (64, 128, 256)
+        assert t.grid_scale in (1, 2) and t.bvh_width in (2, 4, 8) and t.max_pixels > 0
+        got = ctx.tuning()
+        assert (got.trace_block, got.shade_block, got.grid_scale, got.bvh_width) == \
+            (t.trace_block, t.shade_block, t.grid_scale, t.bvh_width)
+        for w, g in zip(want, ctx.render_batch(descs)):
+            assert _same(w, g)
+    finally:
+        ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width)
