@@ -165,10 +165,11 @@ def barrier(world: int):
 # CPU baseline: the reference's CPU renderer (oracle/_ref), else the C port
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(lrd: str, seed: int, target_s: float = 15.0):
+def cpu_baseline(lrd: str, seed: int, target_s: float = 15.0, width: int = W, height: int = H,
+                 max_spp: int = SPP):
     """Times the reference's Renderer::renderImage on all host threads over a
-    bounded sample: the full 1920x1080 frame at a reduced, perfect-square spp
-    chosen so the timed render takes about target_s seconds."""
+    bounded sample: the full frame at a reduced, perfect-square spp chosen so the
+    timed render takes about target_s seconds."""
     from oracle import ref
 
     if not ref.available():
@@ -178,12 +179,13 @@ def cpu_baseline(lrd: str, seed: int, target_s: float = 15.0):
     r.set_samples(1)
     _, t1 = r.render(seed, threads)
     spp = max(1, int(math.floor(math.sqrt(max(1.0, target_s / max(t1, 1e-3))))) ** 2)
-    spp = min(spp, SPP)
+    spp = min(spp, max_spp)
     r.set_samples(spp)
     _, secs = r.render(seed, threads)
-    paths = W * H * spp
+    paths = width * height * spp
     return {"value": paths / secs, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"full 1920x1080 frame at {spp} spp of the 256-spp workload ({paths} paths, {secs:.2f} s)",
+            "sample": f"full {width}x{height} frame at {spp} spp of the {max_spp}-spp workload "
+                      f"({paths} paths, {secs:.2f} s)",
             "seconds": secs}
 
 
@@ -413,6 +415,99 @@ def run_batch(args, ctx, lb, torch, rank, world, local):
     return 0
 
 
+def run_configs(args, ctx, lb, torch, rank, world, local):
+    """The plain-method configurations, one JSON line each: the Cornell box (256x256,
+    depth 8, 16 spp), the 1,048,576-triangle mesh (1024x1024, depth 12, 64 spp) and
+    the 10,000-instance scene (3840x2160, depth 32, --instanced-spp of its 1024 spp,
+    surrogate on). Per scene: the autotuner's shapes on a 1-spp probe, device time of
+    full frames (L2 flushed between steps), the same render with a host image
+    (scene resident), the stage shares, and the reference's CPU renderer on a
+    bounded sample of the same frame."""
+    from lambda_b200 import scenes
+
+    d = tempfile.mkdtemp()
+    cases = [
+        ("cornell", "Cornell box: five 2x2 quad walls, ceiling light 15, dielectric 1.0/1.5 and mirror 0.9 "
+                    "spheres r=0.3; 256x256 depth 8 16 spp 380-780 nm, seed 1",
+         lambda: scenes.cornell(d), lb.RENDER_THINFILM_EXACT),
+        ("mesh", "1,048,576-triangle Perlin-displaced sphere mesh (amplitude 0.1, frequency 4, seed 2), checker "
+                 "0.8/0.2 scale 10, Perlin sky 0.2-1.0; 1024x1024 depth 12 64 spp 360-830 nm",
+         lambda: scenes.perlin_sphere(d, 1024, 1024, 64, 12, levels=9), lb.RENDER_THINFILM_EXACT),
+        ("instanced", f"10,000 instances of a 100,000-triangle Perlin-displaced mesh (seed 5), 40 % thin film / "
+                      f"30 % dielectric / 30 % checker, Perlin sky; 3840x2160 depth 32 at {args.instanced_spp} of "
+                      f"its 1024 spp, surrogate on",
+         lambda: scenes.instanced_meshes(d, spp=args.instanced_spp), lb.RENDER_THINFILM_SURROGATE),
+    ]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    hbm, tf, _, peak_kind = peaks()
+    for name, text, make, flags in cases:
+        sc = make()
+        t0 = time.perf_counter()
+        scene = lb.HostScene.parse(sc.lrd)
+        parse_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ctx.upload(scene)
+        upload_s = time.perf_counter() - t0
+        w, h, spp = sc.width, sc.height, sc.spp
+        paths = w * h * spp
+        tuning, tuning_source = launch_shapes(args, ctx, scene.render_desc(seed=sc.seed, flags=flags, samples=1))
+        desc = scene.render_desc(seed=sc.seed, flags=flags | lb.RENDER_OUTPUT_DEVICE)
+        out = torch.empty((h, w, 3), dtype=torch.float32, device=f"cuda:{local}")
+        for _ in range(args.warmup):
+            ctx.render(desc, out=out)
+        torch.cuda.synchronize()
+        barrier(world)
+        total_ms, launches = 0.0, 0
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                ctx.render(desc, out=out)
+                st = ctx.stats()
+                total_ms += st.render_ms
+                launches += st.kernel_launches
+        value, max_ms = whole_job(paths, args.steps, total_ms, world)
+        stage = lb.stage_profile(ctx, desc, out)
+        host = torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
+        hdesc = scene.render_desc(seed=sc.seed, flags=flags)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.render(hdesc, out=host)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+        if rank == 0:
+            line = {
+                "metric": f"spectral paths/sec, {name} configuration", "value": value, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+bf16" if flags & lb.RENDER_THINFILM_SURROGATE else "f32", "data": "synthetic",
+                "config": {"workload": text, "paths_per_step": paths, "l2": "flushed between timed steps (256 MB write)",
+                           "host_parse_and_bvh_s": parse_s, "upload_s": upload_s,
+                           "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
+                                      "grid_scale": tuning.grid_scale, "bvh_width": tuning.bvh_width,
+                                      "source": tuning_source}},
+                "e2e": {"value": world * paths * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": w * h * 12, "scene": "resident"},
+                "gpu_launches": launches, "clocks": clocks.summary(),
+                "roofline": lb.roofline(stage, hbm, tf, peak_kind),
+                "stage_shares": {k: round(v["share"], 4) for k, v in stage.items() if v["ms"] > 0},
+                "segments_per_path": st.segments / st.paths,
+            }
+            if name == "instanced":
+                line["cpu_baseline"] = None
+                line["cpu_baseline_note"] = ("not timed: the reference's sequential BVH build of this scene "
+                                             "alone takes minutes")
+            elif not args.no_cpu_baseline:
+                cb = cpu_baseline(sc.lrd, sc.seed, width=w, height=h, max_spp=spp)
+                if cb is not None:
+                    cb.pop("seconds", None)
+                    line["cpu_baseline"] = cb
+            print(json.dumps(line), flush=True)
+        del out, host
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,9 +521,14 @@ def main():
     ap.add_argument("--tuning", default="", metavar="TB,SB,GS,WIDTH",
                     help="fixed launch shapes (trace block, shade block, grid scale, BVH width) instead of the "
                          "autotuner's, e.g. for reproducible profiler captures")
-    ap.add_argument("--workload", default="thinfilm1080p", choices=["thinfilm1080p", "batch32", "film_queries"],
+    ap.add_argument("--workload", default="thinfilm1080p",
+                    choices=["thinfilm1080p", "batch32", "film_queries", "configs"],
                     help="batch32: 32 random-pose views of the 1M-triangle mesh scene in one batched render; "
-                         "film_queries: the three film evaluators on 2^24 device-resident queries")
+                         "film_queries: the three film evaluators on 2^24 device-resident queries; "
+                         "configs: the Cornell, 1M-triangle mesh and 10,000-instance scenes, one line each")
+    ap.add_argument("--instanced-spp", type=int, default=16,
+                    help="samples per pixel of the 10,000-instance scene under --workload configs (a perfect "
+                         "square; its configuration asks 1024)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -440,6 +540,16 @@ def main():
 
     import lambda_b200 as lb
     from lambda_b200 import scenes
+
+    if args.workload == "configs":
+        ctx = lb.Context(local)
+        try:
+            from lambda_b200 import surrogate as lbs
+
+            lbs.install(ctx)
+        except Exception as e:  # the instanced scene renders with the surrogate
+            raise SystemExit(f"surrogate weights unavailable: {e}")
+        return run_configs(args, ctx, lb, torch, rank, world, local)
 
     d = tempfile.mkdtemp()
     sc = scenes.thinfilm_spheres(d, W, H, args.spp, DEPTH)

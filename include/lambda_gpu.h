@@ -282,16 +282,30 @@ typedef struct lambda_job {
  * renderKernel (renderer.h:200-213) renders one image per launch. */
 lambda_status lambda_render_batch(lambda_ctx *ctx, const lambda_job *jobs, int32_t n, volatile int32_t *completed);
 
-/* Launch shapes of the wavefront kernels. lambda_autotune times a probe render
- * under every candidate and keeps the fastest on the context; lambda_set_tuning
- * installs given values. No counterpart in the reference. */
+/* Launch shapes of the wavefront kernels and the choice of the path kernel for small
+ * passes. lambda_autotune times a probe render under every candidate (the path kernel
+ * among them, unless the probe renders thin films with the surrogate) and keeps the
+ * fastest on the context: a winning
+ * path kernel covers passes up to the probe's pixels, a winning wavefront sets
+ * path_kernel_pixels to 0. lambda_set_tuning installs given values. No counterpart in
+ * the reference. */
 typedef struct lambda_tuning {
     int32_t trace_block; /* threads per CTA of the traversal kernels (intersect, shadow): 64, 128 or 256 */
     int32_t shade_block; /* threads per CTA of the shading kernels: 64, 128 or 256 */
     int32_t grid_scale;  /* persistent grids hold grid_scale x the CTAs that fit on all SMs at once: 1 or 2 */
     int32_t max_pixels;  /* path-state capacity: a batch above it runs as several passes of whole jobs */
     int32_t bvh_width;   /* children per node of the traversed BVH: 2, 4 or 8 (every width finds the same hits) */
+    int32_t path_kernel_pixels; /* a pass of at most this many pixels runs as one kernel in which each thread traces
+                                   every sample of its pixel (same image, no launch per bounce), unless it renders
+                                   thin films with the surrogate; 0: always the wavefront. Default
+                                   LAMBDA_PATH_KERNEL_PIXELS */
 } lambda_tuning;
+
+/* Default path_kernel_pixels. Below it a sample wave holds too few paths to hide a
+ * launch per bounce on any scene measured; above it the winner depends on the scene
+ * (the wavefront's per-material kernels win where materials mix, the path kernel
+ * where one material and deep traversal dominate), which lambda_autotune decides. */
+#define LAMBDA_PATH_KERNEL_PIXELS 32768
 
 lambda_status lambda_autotune(lambda_ctx *ctx, const lambda_render_desc *probe, lambda_tuning *out);
 /* The same search over a batch: each candidate times lambda_render_batch of the n
@@ -322,10 +336,11 @@ lambda_status lambda_get_render_stats(const lambda_ctx *ctx, lambda_render_stats
  * 5 mirror/dielectric shade, 6 thin-film shade (exact), 7 shadow rays, 8 finish,
  * 9-11 thin-film shade with the surrogate: 9 the hits' queries encoded as MLP rows,
  * 10 the tensor-core MLP, 11 the scatter (with the exact transfer matrix for hits
- * outside the surrogate's domain). items = paths, rays or hits the stage processed over
- * the whole render. No reference counterpart (the reference's single kernel has
- * no stages). */
-#define LAMBDA_NUM_STAGES 12
+ * outside the surrogate's domain), 12 the path kernel of small passes (every sample
+ * and bounce of a pixel in one thread; items = segments). items = paths, rays or hits
+ * the stage processed over the whole render. No reference counterpart (the
+ * reference's single kernel has no stages). */
+#define LAMBDA_NUM_STAGES 13
 typedef struct lambda_stage_time {
     double ms;
     int64_t launches;

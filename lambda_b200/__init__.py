@@ -281,8 +281,8 @@ class Context:
         return t
 
     def set_tuning(self, trace_block: int, shade_block: int, grid_scale: int = 1, max_pixels: int = 0,
-                   bvh_width: int = 4) -> None:
-        t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels, bvh_width)
+                   bvh_width: int = 4, path_kernel_pixels: int = N.PATH_KERNEL_PIXELS) -> None:
+        t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels, bvh_width, path_kernel_pixels)
         self._check(self._lib.lambda_set_tuning(self._h, C.byref(t)))
 
     def tuning(self) -> N.Tuning:
@@ -413,6 +413,9 @@ STAGE_BYTES = {
     "film_encode": 4 + 16 + 48 + 16 * 2 + 4 * 32 + 1,
     # queue, dir, hit, T/lam, 4 outputs of 16 B, domain flag, rng rw, ray w, T w, push
     "film_scatter": 4 + 16 + 48 + 16 * 2 + 4 * 16 + 1 + 8 * 2 + 32 + 16 + 4,
+    # per segment: the ray and hit state of intersect plus a scatter's reads and writes
+    # (the path kernel keeps a pixel's state in one thread, mostly in L1/L2)
+    "path": 4 + 32 + 48 + 4 + 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
 }
 
 

@@ -37,9 +37,10 @@ RENDER_THINFILM_SURROGATE = 1
 RENDER_OUTPUT_DEVICE = 2
 RENDER_PROFILE_STAGES = 4
 RENDER_THINFILM_FP64 = 8
-NUM_STAGES = 12
+NUM_STAGES = 13
+PATH_KERNEL_PIXELS = 32768  # LAMBDA_PATH_KERNEL_PIXELS
 STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
-               "shadow", "finish", "film_encode", "film_mlp", "film_scatter")
+               "shadow", "finish", "film_encode", "film_mlp", "film_scatter", "path")
 
 
 class LambdaError(RuntimeError):
@@ -112,7 +113,7 @@ class Job(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("trace_block", C.c_int32), ("shade_block", C.c_int32), ("grid_scale", C.c_int32),
-                ("max_pixels", C.c_int32), ("bvh_width", C.c_int32)]
+                ("max_pixels", C.c_int32), ("bvh_width", C.c_int32), ("path_kernel_pixels", C.c_int32)]
 
 
 class RenderStats(C.Structure):

@@ -911,7 +911,40 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     };
     int launches = 0;
     std::vector<Progress> progress(completed ? size_t(s_max) : 0);
-    if (prof) {
+    // the surrogate flag changes nothing on a scene without thin films
+    const bool film_surrogate = surrogate && (sc.families & (1u << 2)) != 0;
+    if (!film_surrogate && P <= tu.path_kernel_pixels) {
+        // A small pass: k_init, one k_path over all samples and bounces, k_finish.
+        const void *f_path =
+            fp64 ? (bw == 2 ? (const void *)k_path<2, true> : bw == 4 ? (const void *)k_path<4, true> : (const void *)k_path<8, true>)
+                 : (bw == 2 ? (const void *)k_path<2, false> : bw == 4 ? (const void *)k_path<4, false> : (const void *)k_path<8, false>);
+        CK(cudaFuncSetAttribute(f_path, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)), "configure kernels");
+        const int g_path = (P + tb - 1) / tb;
+        auto timed = [&](int stage, auto &&launch) {
+            if (prof) prof->begin(stage);
+            launch();
+            if (prof) prof->end();
+        };
+        *ctx->progress_host = 0;
+        CK(clear(), "clear counters");
+        CK(cudaEventRecord(ctx->ev_start, stream), "event");
+        timed(0, [&] { k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps); });
+        timed(12, [&] {
+            if (fp64) {
+                if (bw == 2) k_path<2, true><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
+                else if (bw == 4) k_path<4, true><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
+                else k_path<8, true><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
+            } else {
+                if (bw == 2) k_path<2, false><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
+                else if (bw == 4) k_path<4, false><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
+                else k_path<8, false><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
+            }
+        });
+        timed(8, [&] { k_finish<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
+        CK(cudaGetLastError(), "launch path kernel");
+        CK(cudaEventRecord(ctx->ev_stop, stream), "event");
+        launches = 3;
+    } else if (prof) {
         CK(clear(), "clear counters");
         CK(cudaEventRecord(ctx->ev_start, stream), "event");
         prof->begin(0);
@@ -1111,7 +1144,8 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
         ctx->stage_times[0].items = tot.pixels;
         ctx->stage_times[1].items = tot.waves;
         ctx->stage_times[2].items = tot.paths;
-        ctx->stage_times[3].items = ctx->stats.segments;
+        ctx->stage_times[3].items = prof.counts[3] ? ctx->stats.segments : 0;
+        ctx->stage_times[12].items = prof.counts[12] ? ctx->stats.segments : 0;
         ctx->stage_times[4].items = int64_t(tot.stats[4]);
         ctx->stage_times[5].items = int64_t(tot.stats[5]);
         ctx->stage_times[6].items = surrogate ? 0 : ctx->stats.thinfilm_hits;
@@ -1127,7 +1161,7 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
 bool tuning_ok(const lambda_tuning &t) {
     auto block_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
     return block_ok(t.trace_block) && block_ok(t.shade_block) && (t.grid_scale == 1 || t.grid_scale == 2) &&
-           t.max_pixels >= 0 && (t.bvh_width == 2 || t.bvh_width == 4 || t.bvh_width == 8);
+           t.max_pixels >= 0 && (t.bvh_width == 2 || t.bvh_width == 4 || t.bvh_width == 8) && t.path_kernel_pixels >= 0;
 }
 
 }  // namespace
@@ -1161,8 +1195,9 @@ extern "C" lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning 
 namespace {
 
 // Times renders of the probe views (their images stay in device memory) under every
-// combination of BVH width, traversal block, shading block and grid scale, each as
-// the best of three renders after one warm-up, and keeps the fastest. The path-state
+// combination of BVH width, traversal block, shading block and grid scale of the
+// wavefront, and of BVH width and block size of the path kernel, each as the best of
+// three renders after one warm-up, and keeps the fastest. The path-state
 // capacity is set from free device memory: half of it, at the bytes of path state
 // and queues a pixel needs.
 lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, int n, lambda_tuning *out) {
@@ -1205,7 +1240,7 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
             for (int sb : {64, 128, 256})
                 for (int gs : {1, 2}) {
                     double ms = 0;
-                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw}, ms);
+                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw, 0}, ms);
                     if (r == LAMBDA_ERR_UNSUPPORTED) continue;  // stacks too deep for shared memory at this block size
                     if (r != LAMBDA_OK) {
                         ctx->tuning = keep;
@@ -1216,6 +1251,31 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
                         best = ctx->tuning;
                     }
                 }
+    // the path kernel at every BVH width and block size (not for surrogate renders of
+    // thin films, which it does not run); if one wins, passes up to the probe's pixels
+    // use it
+    if (!(probes[0].flags & LAMBDA_RENDER_THINFILM_SURROGATE) || !(ctx->dscene.families & (1u << 2))) {
+        const lambda_tuning wave_best = best;
+        for (int bw : {2, 4, 8})
+            for (int tb : {64, 128, 256}) {
+                lambda_tuning t = wave_best;
+                t.trace_block = tb;
+                t.bvh_width = bw;
+                t.path_kernel_pixels = INT32_MAX;
+                double ms = 0;
+                const lambda_status r = trial(t, ms);
+                if (r == LAMBDA_ERR_UNSUPPORTED) continue;
+                if (r != LAMBDA_OK) {
+                    ctx->tuning = keep;
+                    return r;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                    best.path_kernel_pixels = int32_t(std::min<size_t>(pixels, INT32_MAX));
+                }
+            }
+    }
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         // path state, queues, staged image, the surrogate's MLP rows, outputs and domain flags

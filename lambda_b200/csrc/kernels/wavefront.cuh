@@ -121,30 +121,19 @@ __device__ __forceinline__ s4 sample_radiance(const PathState &ps, int p) {
     return from_f4(ps.radiance[p]) + from_f4(ps.emit[p]);
 }
 
-// Film += linear sRGB of the finished sample (renderer.h:84), then start the
-// next sample: stratified jitter, hero wavelength, camera ray (renderer.h:69-81).
-// Pixels of jobs whose last sample was the previous wave only bank that sample.
-LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = ps.wave[1];
-    const int n_now = rp.active[s];
-    const int n_prev = s > 0 ? rp.active[s - 1] : n_now;
-    if (p == 0) ps.counts[queue_slot(0, kQActive)] = n_now;
-    if (p >= n_prev) return;
-    const Job &job = rp.jobs[job_of(rp, p)];
-
+// Film += linear sRGB of pixel p's finished sample (renderer.h:84).
+__device__ __forceinline__ void bank_sample(const DeviceScene &sc, const PathState &ps, int p, const Job &job) {
     const f3 rgb = spectrum_to_rgb(sc, sample_radiance(ps, p), from_f4(ps.lam[p]), job.lambda_range);
     float4 film = ps.film[p];
     film.x += rgb.x;
     film.y += rgb.y;
     film.z += rgb.z;
     ps.film[p] = film;
-    if (p >= n_now) {
-        ps.radiance[p] = make_float4(0, 0, 0, 0);
-        ps.emit[p] = make_float4(0, 0, 0, 0);
-        return;
-    }
+}
 
+// Sample s of pixel p: stratified jitter, hero wavelength and camera ray
+// (renderer.h:69-81), unit throughput, no radiance yet.
+__device__ __forceinline__ void start_sample(const PathState &ps, int p, const Job &job, int s) {
     const int local = p - job.base;
     const int i = s / job.sqrt_samples, j = s % job.sqrt_samples;
     const int px = local % job.width, py = local / job.width;
@@ -162,6 +151,25 @@ LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
     ps.throughput[p] = make_float4(1, 1, 1, 1);
     ps.radiance[p] = make_float4(0, 0, 0, 0);
     ps.emit[p] = make_float4(0, 0, 0, 0);
+}
+
+// Banks the finished sample of every pixel, then starts the next one.
+// Pixels of jobs whose last sample was the previous wave only bank that sample.
+LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = ps.wave[1];
+    const int n_now = rp.active[s];
+    const int n_prev = s > 0 ? rp.active[s - 1] : n_now;
+    if (p == 0) ps.counts[queue_slot(0, kQActive)] = n_now;
+    if (p >= n_prev) return;
+    const Job &job = rp.jobs[job_of(rp, p)];
+    bank_sample(sc, ps, p, job);
+    if (p >= n_now) {
+        ps.radiance[p] = make_float4(0, 0, 0, 0);
+        ps.emit[p] = make_float4(0, 0, 0, 0);
+        return;
+    }
+    start_sample(ps, p, job, s);
     ps.queue[0][p] = p;
 }
 
@@ -621,6 +629,58 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams r
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
         const int p = ps.shadow_queue[idx];
         shadow_path<K>(sc, ps, p, st_a, st_b);
+    }
+}
+
+// A whole pass in one launch, for passes whose pixels are too few to fill the GPU
+// with one sample wave: thread p runs every sample of its pixel to the end, bounce
+// by bounce, through the same per-path steps as the wavefront kernels and in the
+// same order (bank and start a sample, closest hit, the material's shade, the NEE
+// shadow ray), so the image equals the wavefront's bit for bit with no launch per
+// bounce. k_finish banks the last sample. Thin films are evaluated exactly (FP32,
+// or complex double with kFp64); surrogate renders of thin films need the
+// wavefront, which batches a bounce's thin-film hits for the tensor cores. The
+// statistics are the ones the wave prologue keeps from the queue sizes.
+template <int K, bool kFp64>
+LAMBDA_KERNEL void __launch_bounds__(256) k_path(RenderParams rp, DeviceScene sc, PathState ps) {
+    extern __shared__ int stack_smem[];
+    WideStack st_a, st_b;
+    wide_stacks(stack_smem, sc, st_a, st_b);
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned n_seg = 0, n_nee = 0, n_film = 0, n_lam = 0, n_spec = 0;
+    if (p < rp.num_pixels) {
+        const Job &job = rp.jobs[job_of(rp, p)];
+        for (int s = 0; s < job.samples; s++) {
+            bank_sample(sc, ps, p, job);
+            start_sample(ps, p, job, s);
+            for (int b = 0; b <= rp.depth_max; b++) {
+                n_seg++;
+                const int family = trace_path<K>(sc, ps, p, st_a, st_b);
+                if (family < 0) break;
+                bool alive, nee = false;
+                if (family == 0) {
+                    n_lam++;
+                    alive = lambert_path(sc, ps, p, b, nee);
+                    if (nee) {
+                        n_nee++;
+                        shadow_path<K>(sc, ps, p, st_a, st_b);
+                    }
+                } else if (family == 1) {
+                    n_spec++;
+                    alive = specular_path(sc, ps, p, b);
+                } else {
+                    n_film++;
+                    alive = film_path<kFp64>(sc, ps, p, b);
+                }
+                if (!alive) break;
+            }
+        }
+    }
+    // segments, NEE rays, thin-film hits, (fallback), Lambertian hits, specular hits
+    const unsigned c[6] = {n_seg, n_nee, n_film, 0u, n_lam, n_spec};
+    for (int i = 0; i < 6; i++) {
+        const unsigned sum = __reduce_add_sync(0xffffffffu, c[i]);
+        if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&ps.stats[i], (unsigned long long)sum);
     }
 }
 
