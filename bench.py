@@ -327,8 +327,8 @@ BATCH_POSES = {"target": (0.0, 0.0, 0.0), "distance": (2.6, 4.0), "height": (-1.
 def launch_shapes(args, ctx, probe):
     """The autotuner's pick on `probe`, or the shapes --tuning fixes."""
     if args.tuning:
-        tb, sb, gs, width = (int(v) for v in args.tuning.split(","))
-        ctx.set_tuning(tb, sb, gs, 0, width)
+        vals = [int(v) for v in args.tuning.split(",")]
+        ctx.set_tuning(*vals[:3], 0, *vals[3:])
         return ctx.tuning(), "fixed by --tuning"
     return ctx.autotune(probe), f"lambda_autotune, {probe.settings.samples}-spp probe"
 
@@ -426,13 +426,17 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
     from lambda_b200 import scenes
 
     d = tempfile.mkdtemp()
+    c_res, c_spp, m_res, m_spp = 256, 16, 1024, 64
+    if args.config_size:
+        c_res, c_spp = (int(v) for v in args.config_size.split(","))
+        m_res, m_spp = c_res, c_spp
     cases = [
-        ("cornell", "Cornell box: five 2x2 quad walls, ceiling light 15, dielectric 1.0/1.5 and mirror 0.9 "
-                    "spheres r=0.3; 256x256 depth 8 16 spp 380-780 nm, seed 1",
-         lambda: scenes.cornell(d), lb.RENDER_THINFILM_EXACT),
-        ("mesh", "1,048,576-triangle Perlin-displaced sphere mesh (amplitude 0.1, frequency 4, seed 2), checker "
-                 "0.8/0.2 scale 10, Perlin sky 0.2-1.0; 1024x1024 depth 12 64 spp 360-830 nm",
-         lambda: scenes.perlin_sphere(d, 1024, 1024, 64, 12, levels=9), lb.RENDER_THINFILM_EXACT),
+        ("cornell", f"Cornell box: five 2x2 quad walls, ceiling light 15, dielectric 1.0/1.5 and mirror 0.9 "
+                    f"spheres r=0.3; {c_res}x{c_res} depth 8 {c_spp} spp 380-780 nm, seed 1",
+         lambda: scenes.cornell(d, c_res, c_res, c_spp), lb.RENDER_THINFILM_EXACT),
+        ("mesh", f"1,048,576-triangle Perlin-displaced sphere mesh (amplitude 0.1, frequency 4, seed 2), checker "
+                 f"0.8/0.2 scale 10, Perlin sky 0.2-1.0; {m_res}x{m_res} depth 12 {m_spp} spp 360-830 nm",
+         lambda: scenes.perlin_sphere(d, m_res, m_res, m_spp, 12, levels=9), lb.RENDER_THINFILM_EXACT),
         ("instanced", f"10,000 instances of a 100,000-triangle Perlin-displaced mesh (seed 5), 40 % thin film / "
                       f"30 % dielectric / 30 % checker, Perlin sky; 3840x2160 depth 32 at {args.instanced_spp} of "
                       f"its 1024 spp, surrogate on",
@@ -440,7 +444,10 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
     ]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     hbm, tf, _, peak_kind = peaks()
+    wanted = set(args.configs.split(","))
     for name, text, make, flags in cases:
+        if name not in wanted:
+            continue
         sc = make()
         t0 = time.perf_counter()
         scene = lb.HostScene.parse(sc.lrd)
@@ -518,14 +525,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
     ap.add_argument("--no-compare", action="store_true", help="skip the surrogate/exact comparison")
-    ap.add_argument("--tuning", default="", metavar="TB,SB,GS,WIDTH",
-                    help="fixed launch shapes (trace block, shade block, grid scale, BVH width) instead of the "
-                         "autotuner's, e.g. for reproducible profiler captures")
+    ap.add_argument("--tuning", default="", metavar="TB,SB,GS,WIDTH[,PATH_PIXELS]",
+                    help="fixed launch shapes (trace block, shade block, grid scale, BVH width, and the largest "
+                         "pass the path kernel runs) instead of the autotuner's, e.g. for reproducible profiler "
+                         "captures")
     ap.add_argument("--workload", default="thinfilm1080p",
                     choices=["thinfilm1080p", "batch32", "film_queries", "configs"],
                     help="batch32: 32 random-pose views of the 1M-triangle mesh scene in one batched render; "
                          "film_queries: the three film evaluators on 2^24 device-resident queries; "
                          "configs: the Cornell, 1M-triangle mesh and 10,000-instance scenes, one line each")
+    ap.add_argument("--configs", default="cornell,mesh,instanced",
+                    help="--workload configs: which configurations, comma-separated")
+    ap.add_argument("--config-size", default="", metavar="RES,SPP",
+                    help="--workload configs: render the Cornell and mesh configurations at RES x RES and SPP "
+                         "instead of their own sizes (small cases for profiler captures)")
     ap.add_argument("--instanced-spp", type=int, default=16,
                     help="samples per pixel of the 10,000-instance scene under --workload configs (a perfect "
                          "square; its configuration asks 1024)")
