@@ -47,6 +47,23 @@ def test_struct_sizes_match_reference_layout():
         assert [lib.ref_sizeof(i) for i in range(6)] == [116, 144, 32, 16, 16, 16]
 
 
+def _header_fields(struct: str) -> list:
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct " + struct + r" \{(.*?)\} " + struct + ";", text, flags=re.S).group(1)
+    return re.findall(r"(\w+)\s*(?:\[[^\]]*\])?;", body)
+
+
+def test_python_mirrors_match_the_header():
+    """The ctypes mirrors of the tuning and stage-time records and the constants the
+    Python side copies agree with include/lambda_gpu.h."""
+    assert [f[0] for f in N.Tuning._fields_] == _header_fields("lambda_tuning")
+    assert [f[0] for f in N.StageTime._fields_] == _header_fields("lambda_stage_time")
+    text = open(HEADER).read()
+    defines = dict(re.findall(r"#define (LAMBDA_\w+) (\d+)", text))
+    assert int(defines["LAMBDA_NUM_STAGES"]) == N.NUM_STAGES == len(N.STAGE_NAMES)
+    assert int(defines["LAMBDA_PATH_KERNEL_PIXELS"]) == N.PATH_KERNEL_PIXELS
+
+
 def test_null_arguments_are_rejected():
     lib = N.load()
     assert lib.lambda_scene_upload(None, None) == 1
