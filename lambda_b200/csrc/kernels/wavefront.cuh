@@ -66,6 +66,21 @@ __device__ __forceinline__ int job_of(const RenderParams &rp, int p) {
     return lo;
 }
 
+// The job-local pixel taken l-th when warps are to cover 8x4 tiles: the image is cut
+// into bands of 4 rows and each band into blocks of 8 columns (the last ones
+// narrower), row-major inside a block. A bijection of [0, width * height), so it
+// changes which thread or queue slot takes a pixel, never the pixel's arithmetic.
+__device__ __forceinline__ int tile_order(const Job &job, int l) {
+    const int w = job.width;
+    const int band = l / (4 * w);
+    const int hb = min(4, job.height - 4 * band);
+    const int r = l - band * 4 * w;
+    const int cx = r / (8 * hb);
+    const int rr = r - cx * 8 * hb;
+    const int bw = min(8, w - 8 * cx);
+    return (4 * band + rr / bw) * w + 8 * cx + rr % bw;
+}
+
 // Every pixel: seed its stream (job seed, job-local pixel index, as a render of
 // that job alone), record its depth limit, zero film and radiance.
 LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
@@ -170,7 +185,8 @@ LAMBDA_KERNEL void k_raygen(RenderParams rp, DeviceScene sc, PathState ps) {
         return;
     }
     start_sample(ps, p, job, s);
-    ps.queue[0][p] = p;
+    // the first intersect takes the wave's paths tile by tile
+    ps.queue[0][p] = job.base + tile_order(job, p - job.base);
 }
 
 // Material index of object `obj` in instance `inst` (instance.h:38).
@@ -646,10 +662,11 @@ LAMBDA_KERNEL void __launch_bounds__(256) k_path(RenderParams rp, DeviceScene sc
     extern __shared__ int stack_smem[];
     WideStack st_a, st_b;
     wide_stacks(stack_smem, sc, st_a, st_b);
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned n_seg = 0, n_nee = 0, n_film = 0, n_lam = 0, n_spec = 0;
-    if (p < rp.num_pixels) {
-        const Job &job = rp.jobs[job_of(rp, p)];
+    if (v < rp.num_pixels) {
+        const Job &job = rp.jobs[job_of(rp, v)];
+        const int p = job.base + tile_order(job, v - job.base);  // a warp takes an 8x4 tile
         for (int s = 0; s < job.samples; s++) {
             bank_sample(sc, ps, p, job);
             start_sample(ps, p, job, s);
