@@ -427,9 +427,11 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
 
     d = tempfile.mkdtemp()
     c_res, c_spp, m_res, m_spp = 256, 16, 1024, 64
+    i_w, i_h, i_spp = 3840, 2160, args.instanced_spp
     if args.config_size:
         c_res, c_spp = (int(v) for v in args.config_size.split(","))
         m_res, m_spp = c_res, c_spp
+        i_w, i_h, i_spp = c_res, c_res * 9 // 16, c_spp
     cases = [
         ("cornell", f"Cornell box: five 2x2 quad walls, ceiling light 15, dielectric 1.0/1.5 and mirror 0.9 "
                     f"spheres r=0.3; {c_res}x{c_res} depth 8 {c_spp} spp 380-780 nm, seed 1",
@@ -438,9 +440,9 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
                  f"0.8/0.2 scale 10, Perlin sky 0.2-1.0; {m_res}x{m_res} depth 12 {m_spp} spp 360-830 nm",
          lambda: scenes.perlin_sphere(d, m_res, m_res, m_spp, 12, levels=9), lb.RENDER_THINFILM_EXACT),
         ("instanced", f"10,000 instances of a 100,000-triangle Perlin-displaced mesh (seed 5), 40 % thin film / "
-                      f"30 % dielectric / 30 % checker, Perlin sky; 3840x2160 depth 32 at {args.instanced_spp} of "
+                      f"30 % dielectric / 30 % checker, Perlin sky; {i_w}x{i_h} depth 32 at {i_spp} of "
                       f"its 1024 spp, surrogate on",
-         lambda: scenes.instanced_meshes(d, spp=args.instanced_spp), lb.RENDER_THINFILM_SURROGATE),
+         lambda: scenes.instanced_meshes(d, i_w, i_h, i_spp), lb.RENDER_THINFILM_SURROGATE),
     ]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     hbm, tf, _, peak_kind = peaks()
@@ -537,8 +539,9 @@ def main():
     ap.add_argument("--configs", default="cornell,mesh,instanced",
                     help="--workload configs: which configurations, comma-separated")
     ap.add_argument("--config-size", default="", metavar="RES,SPP",
-                    help="--workload configs: render the Cornell and mesh configurations at RES x RES and SPP "
-                         "instead of their own sizes (small cases for profiler captures)")
+                    help="--workload configs: render the Cornell and mesh configurations at RES x RES and SPP, "
+                         "and the instanced one at RES x RES*9/16 and SPP, instead of their own sizes (small cases "
+                         "for profiler captures)")
     ap.add_argument("--instanced-spp", type=int, default=16,
                     help="samples per pixel of the 10,000-instance scene under --workload configs (a perfect "
                          "square; its configuration asks 1024)")
