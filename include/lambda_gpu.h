@@ -285,10 +285,10 @@ lambda_status lambda_render_batch(lambda_ctx *ctx, const lambda_job *jobs, int32
 /* Launch shapes of the wavefront kernels and the choice of the path kernel for small
  * passes. lambda_autotune times a probe render under every candidate (the path kernel
  * among them, unless the probe renders thin films with the surrogate) and keeps the
- * fastest on the context: a winning
- * path kernel covers passes up to the probe's pixels, a winning wavefront sets
- * path_kernel_pixels to 0. lambda_set_tuning installs given values. No counterpart in
- * the reference. */
+ * fastest on the context. A winning path kernel covers passes up to the probe's pixels
+ * (at least LAMBDA_PATH_KERNEL_PIXELS); a winning wavefront leaves the path kernel to
+ * passes smaller than both the probe and LAMBDA_PATH_KERNEL_PIXELS. lambda_set_tuning
+ * installs given values. No counterpart in the reference. */
 typedef struct lambda_tuning {
     int32_t trace_block; /* threads per CTA of the traversal kernels (intersect, shadow): 64, 128 or 256 */
     int32_t shade_block; /* threads per CTA of the shading kernels: 64, 128 or 256 */

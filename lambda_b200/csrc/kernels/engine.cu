@@ -1252,9 +1252,13 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
                     }
                 }
     // the path kernel at every BVH width and block size (not for surrogate renders of
-    // thin films, which it does not run); if one wins, passes up to the probe's pixels
-    // use it
+    // thin films, which it does not run). If one wins, passes up to the probe's pixels
+    // use it; if the wavefront wins, only passes below the probe's size and the default
+    // threshold do.
+    best.path_kernel_pixels = keep.path_kernel_pixels;
     if (!(probes[0].flags & LAMBDA_RENDER_THINFILM_SURROGATE) || !(ctx->dscene.families & (1u << 2))) {
+        const int32_t probe_pixels = int32_t(std::min<size_t>(pixels, INT32_MAX));
+        best.path_kernel_pixels = std::min<int32_t>(LAMBDA_PATH_KERNEL_PIXELS, probe_pixels - 1);
         const lambda_tuning wave_best = best;
         for (int bw : {2, 4, 8})
             for (int tb : {64, 128, 256}) {
@@ -1272,7 +1276,7 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
                 if (ms < best_ms) {
                     best_ms = ms;
                     best = t;
-                    best.path_kernel_pixels = int32_t(std::min<size_t>(pixels, INT32_MAX));
+                    best.path_kernel_pixels = std::max<int32_t>(LAMBDA_PATH_KERNEL_PIXELS, probe_pixels);
                 }
             }
     }

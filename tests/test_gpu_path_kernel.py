@@ -153,3 +153,26 @@ def test_surrogate_flag_without_thin_films_takes_the_path_kernel(scene_dir, ctx)
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        keep.path_kernel_pixels)
     assert np.array_equal(got, want, equal_nan=True)
+
+
+def test_autotune_sets_the_path_kernel_threshold(scene_dir, ctx):
+    """A winning path kernel covers the probe (and at least the default threshold); a
+    winning wavefront keeps the path kernel for passes below both the probe and the
+    default. Either way the probe's frame renders as the tuned form."""
+    sc = CASES["mesh"](scene_dir)
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx.upload(scene)
+    keep = ctx.tuning()
+    try:
+        probe = scene.render_desc(seed=sc.seed)
+        pixels = sc.width * sc.height
+        t = ctx.autotune(probe)
+        assert t.path_kernel_pixels in (max(N.PATH_KERNEL_PIXELS, pixels), min(N.PATH_KERNEL_PIXELS, pixels - 1))
+        ctx.render(probe)
+        path_won = t.path_kernel_pixels >= pixels
+        assert (ctx.stats().kernel_launches == 3) == path_won
+        print(f"autotuned on {pixels} pixels: {'path kernel' if path_won else 'wavefront'}, "
+              f"threshold {t.path_kernel_pixels}")
+    finally:
+        ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
+                       keep.path_kernel_pixels)
