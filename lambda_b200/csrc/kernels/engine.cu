@@ -915,10 +915,11 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     const bool film_surrogate = surrogate && (sc.families & (1u << 2)) != 0;
     if (!film_surrogate && P <= tu.path_kernel_pixels) {
         // A small pass: k_init, one k_path over all samples and bounces, k_finish.
-        const void *f_path =
-            fp64 ? (bw == 2 ? (const void *)k_path<2, true> : bw == 4 ? (const void *)k_path<4, true> : (const void *)k_path<8, true>)
-                 : (bw == 2 ? (const void *)k_path<2, false> : bw == 4 ? (const void *)k_path<4, false> : (const void *)k_path<8, false>);
-        CK(cudaFuncSetAttribute(f_path, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)), "configure kernels");
+        using PathKernel = void (*)(RenderParams, DeviceScene, PathState);
+        const PathKernel f_path = fp64 ? (bw == 2 ? k_path<2, true> : bw == 4 ? k_path<4, true> : k_path<8, true>)
+                                       : (bw == 2 ? k_path<2, false> : bw == 4 ? k_path<4, false> : k_path<8, false>);
+        CK(cudaFuncSetAttribute((const void *)f_path, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)),
+           "configure kernels");
         const int g_path = (P + tb - 1) / tb;
         auto timed = [&](int stage, auto &&launch) {
             if (prof) prof->begin(stage);
@@ -929,17 +930,7 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         CK(clear(), "clear counters");
         CK(cudaEventRecord(ctx->ev_start, stream), "event");
         timed(0, [&] { k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps); });
-        timed(12, [&] {
-            if (fp64) {
-                if (bw == 2) k_path<2, true><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
-                else if (bw == 4) k_path<4, true><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
-                else k_path<8, true><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
-            } else {
-                if (bw == 2) k_path<2, false><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
-                else if (bw == 4) k_path<4, false><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
-                else k_path<8, false><<<g_path, tb, stack_smem, stream>>>(rp, sc, ps);
-            }
-        });
+        timed(12, [&] { f_path<<<g_path, tb, stack_smem, stream>>>(rp, sc, ps); });
         timed(8, [&] { k_finish<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
         CK(cudaGetLastError(), "launch path kernel");
         CK(cudaEventRecord(ctx->ev_stop, stream), "event");
