@@ -261,7 +261,8 @@ typedef struct lambda_render_desc {
  * stream py*width+px seeded with desc->seed, in the reference's order, so results
  * follow the reference sample for sample. completed (may be NULL) is raised
  * monotonically towards width*height while the call runs (pixels x finished
- * sample waves / samples). Blocks until the image is written. */
+ * sample waves / samples; a pass run by the path kernel reports its pixels when it
+ * ends). Blocks until the image is written. */
 lambda_status lambda_render(lambda_ctx *ctx, const lambda_render_desc *desc, float *out_rgb,
                             volatile int32_t *completed);
 
