@@ -527,10 +527,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
     ap.add_argument("--no-compare", action="store_true", help="skip the surrogate/exact comparison")
-    ap.add_argument("--tuning", default="", metavar="TB,SB,GS,WIDTH[,PATH_PIXELS]",
-                    help="fixed launch shapes (trace block, shade block, grid scale, BVH width, and the largest "
-                         "pass the path kernel runs) instead of the autotuner's, e.g. for reproducible profiler "
-                         "captures")
+    ap.add_argument("--tuning", default="", metavar="TB,SB,GS,WIDTH[,PATH_PIXELS[,LANE_FETCH]]",
+                    help="fixed launch shapes (trace block, shade block, grid scale, BVH width, the largest pass "
+                         "the path kernel runs, and 1 for the lane-by-lane intersect) instead of the autotuner's, "
+                         "e.g. for reproducible profiler captures")
     ap.add_argument("--workload", default="thinfilm1080p",
                     choices=["thinfilm1080p", "batch32", "film_queries", "configs"],
                     help="batch32: 32 random-pose views of the 1M-triangle mesh scene in one batched render; "

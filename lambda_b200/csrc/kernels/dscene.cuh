@@ -465,6 +465,29 @@ __device__ __forceinline__ int wide_expand(const DeviceScene &s, int w, const Ra
     return sp;
 }
 
+// The hit record of a finished closest-hit traversal of world ray wr: the winning
+// primitive's attributes in instance space, then in world space. Returns false on a
+// miss (best_obj < 0).
+__device__ __forceinline__ bool closest_hit_finish(const DeviceScene &s, const Ray3 &wr, float best, int best_obj,
+                                                   int best_inst, Hit &h) {
+    if (best_obj < 0) {
+        h.t = kMax;
+        h.instance = -1;
+        h.object = -1;
+        return false;
+    }
+    const InstanceRef ir = instance_ref(s, best_inst);
+    const Ray3 lr = to_local(s.instance_flags[best_inst], ir, wr);
+    const Prim pr = load_prim(s, best_obj);
+    const int inst_material = ir.header().w;
+    const int mat = inst_material >= 0 ? inst_material : prim_material(pr);
+    prim_attributes(s, best_obj, pr, lr.o, lr.d, best, h, s.material_uv[mat] != 0);
+    h.instance = best_inst;
+    h.object = best_obj;
+    to_world(s, best_inst, ir, h);
+    return true;
+}
+
 // Scene::hit in closest-hit mode (scene.h:51-124) over the wide BVH: two-level
 // depth-first traversal that visits the nodes the reference visits in the order it
 // visits them (right child first), culls an entry when its box starts beyond the best
@@ -520,22 +543,7 @@ __device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, 
         }
         if (overflow) break;
     }
-    if (best_obj < 0) {
-        h.t = kMax;
-        h.instance = -1;
-        h.object = -1;
-        return false;
-    }
-    const InstanceRef ir = instance_ref(s, best_inst);
-    const Ray3 lr = to_local(s.instance_flags[best_inst], ir, wr);
-    const Prim pr = load_prim(s, best_obj);
-    const int inst_material = ir.header().w;
-    const int mat = inst_material >= 0 ? inst_material : prim_material(pr);
-    prim_attributes(s, best_obj, pr, lr.o, lr.d, best, h, s.material_uv[mat] != 0);
-    h.instance = best_inst;
-    h.object = best_obj;
-    to_world(s, best_inst, ir, h);
-    return true;
+    return closest_hit_finish(s, wr, best, best_obj, best_inst, h);
 }
 
 // Scene::hit in shadow mode (scene.h:51-124 with occludedInstance/Object) over the

@@ -99,7 +99,10 @@ struct PathState {
 
 // Counters per bounce: paths to trace, then the three material queues, then NEE rays,
 // then the thin-film hits the surrogate left to the exact transfer matrix (a count).
-enum : int { kQActive = 0, kQLambert = 1, kQSpecular = 2, kQFilm = 3, kQShadow = 4, kQFilmFallback = 5, kQueues = 6 };
+// kQFetch: the next unclaimed entry of the bounce's active queue, for intersect
+// kernels whose lanes take rays one by one.
+enum : int { kQActive = 0, kQLambert = 1, kQSpecular = 2, kQFilm = 3, kQShadow = 4, kQFilmFallback = 5, kQFetch = 6,
+             kQueues = 7 };
 __host__ __device__ inline int queue_slot(int bounce, int q) { return bounce * kQueues + q; }
 
 }  // namespace lambda_dev

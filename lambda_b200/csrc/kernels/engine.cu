@@ -793,8 +793,12 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     const int dev = ctx->device, sms = ctx->sm_count;
     const int tb = tu.trace_block, sb = tu.shade_block, gs = tu.grid_scale, bw = tu.bvh_width;
     const size_t stack_smem = wide_stack_bytes(tb, sc.stack_tlas, sc.stack_blas);
-    const void *f_isect = bw == 2 ? (const void *)k_intersect<2> : bw == 4 ? (const void *)k_intersect<4>
-                                                                            : (const void *)k_intersect<8>;
+    // intersect: a warp traces 32 rays to the end, or (lane_fetch) lanes take rays one by one
+    using IntersectKernel = void (*)(int, RenderParams, DeviceScene, PathState);
+    const IntersectKernel k_isect =
+        tu.lane_fetch ? (bw == 2 ? k_intersect_fetch<2> : bw == 4 ? k_intersect_fetch<4> : k_intersect_fetch<8>)
+                      : (bw == 2 ? k_intersect<2> : bw == 4 ? k_intersect<4> : k_intersect<8>);
+    const void *f_isect = (const void *)k_isect;
     const void *f_shadow = bw == 2 ? (const void *)k_shadow<2> : bw == 4 ? (const void *)k_shadow<4>
                                                                          : (const void *)k_shadow<8>;
     int smem_optin = 0;
@@ -808,11 +812,7 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     };
     const int g_isect = grid(f_isect, tb, stack_smem);
     const int g_shadow = grid(f_shadow, tb, stack_smem);
-    auto intersect = [&](int b) {
-        if (bw == 2) k_intersect<2><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
-        else if (bw == 4) k_intersect<4><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
-        else k_intersect<8><<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps);
-    };
+    auto intersect = [&](int b) { k_isect<<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps); };
     auto shadow = [&](int b, cudaStream_t s) {
         if (bw == 2) k_shadow<2><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
         else if (bw == 4) k_shadow<4><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
@@ -1152,7 +1152,8 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
 bool tuning_ok(const lambda_tuning &t) {
     auto block_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
     return block_ok(t.trace_block) && block_ok(t.shade_block) && (t.grid_scale == 1 || t.grid_scale == 2) &&
-           t.max_pixels >= 0 && (t.bvh_width == 2 || t.bvh_width == 4 || t.bvh_width == 8) && t.path_kernel_pixels >= 0;
+           t.max_pixels >= 0 && (t.bvh_width == 2 || t.bvh_width == 4 || t.bvh_width == 8) && t.path_kernel_pixels >= 0 &&
+           (t.lane_fetch == 0 || t.lane_fetch == 1);
 }
 
 }  // namespace
@@ -1231,7 +1232,7 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
             for (int sb : {64, 128, 256})
                 for (int gs : {1, 2}) {
                     double ms = 0;
-                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw, 0}, ms);
+                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw, 0, 0}, ms);
                     if (r == LAMBDA_ERR_UNSUPPORTED) continue;  // stacks too deep for shared memory at this block size
                     if (r != LAMBDA_OK) {
                         ctx->tuning = keep;
@@ -1242,6 +1243,29 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
                         best = ctx->tuning;
                     }
                 }
+    // the intersect kernel with rays taken lane by lane, at every width and traversal
+    // block, with the best wavefront's other shapes
+    {
+        const lambda_tuning grid_best = best;
+        for (int bw : {2, 4, 8})
+            for (int tb : {64, 128, 256}) {
+                lambda_tuning t = grid_best;
+                t.trace_block = tb;
+                t.bvh_width = bw;
+                t.lane_fetch = 1;
+                double ms = 0;
+                const lambda_status r = trial(t, ms);
+                if (r == LAMBDA_ERR_UNSUPPORTED) continue;
+                if (r != LAMBDA_OK) {
+                    ctx->tuning = keep;
+                    return r;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
+            }
+    }
     // the path kernel at every BVH width and block size (not for surrogate renders of
     // thin films, which it does not run). If one wins, passes up to the probe's pixels
     // use it; if the wavefront wins, only passes below the probe's size and the default

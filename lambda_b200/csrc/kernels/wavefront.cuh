@@ -198,6 +198,9 @@ __device__ __forceinline__ int material_of(const DeviceScene &sc, int inst_mater
 // path's emission term and returns -1: the path ends. Any other hit is stored for the
 // shade kernels and its material family returned: 0 Lambertian, 1 mirror or
 // dielectric, 2 thin film.
+__device__ __forceinline__ int trace_finish(const DeviceScene &sc, const PathState &ps, int p, const float4 &o4,
+                                            const float4 &d4, bool hit, const Hit &h);
+
 template <int K>
 __device__ __forceinline__ int trace_path(const DeviceScene &sc, const PathState &ps, int p, const WideStack &st_a,
                                           const WideStack &st_b) {
@@ -207,6 +210,15 @@ __device__ __forceinline__ int trace_path(const DeviceScene &sc, const PathState
     bool overflow = false;
     const bool hit = closest_hit_w<K>(sc, o, d, h, overflow, st_a, st_b);
     if (overflow) atomicOr(ps.error, 1);
+    return trace_finish(sc, ps, p, o4, d4, hit, h);
+}
+
+// What trace_path does with path p's hit record (ray o4, d4): a miss or an emitter
+// hit records the emission term and returns -1; any other hit is stored and its
+// material family returned.
+__device__ __forceinline__ int trace_finish(const DeviceScene &sc, const PathState &ps, int p, const float4 &o4,
+                                            const float4 &d4, bool hit, const Hit &h) {
+    const f3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
     const bool specular = d4.w != 0.0f;
     const float prev_pdf = o4.w;
     const bool lights = sc.total_light_power > 0;
@@ -271,6 +283,106 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_intersect(int bounce, RenderParam
         for (int f = 0; f < 3; f++) {
             const int slot = warp_push(&ps.counts[queue_slot(bounce, kQLambert + f)], family == f);
             if (family == f) ps.mat_queue[f][slot] = p;
+        }
+    }
+}
+
+// Closest hits of the bounce's queue with rays taken lane by lane. Each lane keeps its
+// traversal (stacks, instance-space ray, best hit) across iterations of one loop and
+// advances it by one stack entry per iteration, in the order closest_hit_w visits
+// them, so its hits are closest_hit_w's bit for bit. A lane whose ray is done
+// finishes it as trace_path does, pushes it to its material queue with the lanes that
+// finish at the same step, and takes the next ray from the queue's fetch counter at
+// once. Lanes on different rays then step together instead of waiting for a warp's
+// longest ray. The loop ends when the queue is drained: every iteration pops an
+// entry, finishes a ray or takes one.
+template <int K>
+LAMBDA_KERNEL void __launch_bounds__(256, 2) k_intersect_fetch(int bounce, RenderParams rp, DeviceScene sc,
+                                                               PathState ps) {
+    extern __shared__ int stack_smem[];
+    WideStack st, sub;
+    wide_stacks(stack_smem, sc, st, sub);
+    const int n = ps.counts[queue_slot(bounce, kQActive)];
+    const int *q = ps.queue[bounce & 1];
+    int *next = &ps.counts[queue_slot(bounce, kQFetch)];
+    const int lane = threadIdx.x & 31;
+    int p = -1;
+    Ray3 wr, lr;
+    float best = kMax;
+    int best_obj = -1, best_inst = -1, inst = -1, sp = 0, ssp = 0;
+    bool overflow = false;
+    for (;;) {
+        if (p < 0) {
+            // the lanes that need a ray take consecutive entries, one atomic per group
+            const unsigned need = __activemask();
+            const int leader = __ffs(need) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(next, __popc(need));
+            base = __shfl_sync(need, base, leader);
+            const int idx = base + __popc(need & ((1u << lane) - 1u));
+            if (idx >= n) break;
+            p = q[idx];
+            const float4 o4 = ps.ray_o[p], d4 = ps.ray_d[p];
+            wr = make_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
+            best = kMax;
+            best_obj = best_inst = -1;
+            sp = ssp = 0;
+            overflow = false;
+            float te;
+            if (slab(__ldg(&sc.nodes[0]), __ldg(&sc.nodes[1]), wr, te)) st.put(sp++, __ldg(&sc.wide_code[0]), te);
+        } else if (ssp > 0 && !overflow) {
+            // one BLAS entry
+            --ssp;
+            const int c2 = sub.code[ssp * sub.stride];
+            if (!(sub.te[ssp * sub.stride] > best)) {
+                if (c2 >= 0) {
+                    ssp = wide_expand<K>(sc, c2, lr, best, sub, ssp, overflow);
+                } else {
+                    const int2 lf = __ldg(&sc.wide_leaves[-c2 - 1]);
+                    for (int k = 0; k < lf.y; k++) {
+                        const float t = intersect_t(load_prim(sc, lf.x + k), lr, best);
+                        if (t >= 0) {
+                            best = t;
+                            best_obj = lf.x + k;
+                            best_inst = inst;
+                        }
+                    }
+                }
+            }
+        } else if (sp > 0 && !overflow) {
+            // one TLAS entry; a leaf starts its instance's BLAS (the first instance only)
+            --sp;
+            const int code = st.code[sp * st.stride];
+            float te = st.te[sp * st.stride];
+            if (!(te > best)) {
+                if (code >= 0) {
+                    sp = wide_expand<K>(sc, code, wr, best, st, sp, overflow);
+                } else {
+                    inst = __ldg(&sc.wide_leaves[-code - 1]).x;
+                    const uint32_t flags = sc.instance_flags[inst];
+                    const InstanceRef ir = instance_ref(sc, inst);
+                    const int root = ir.header().z;
+                    lr = to_local(flags, ir, wr);
+                    if ((flags & 2u) ||
+                        (slab(__ldg(&sc.nodes[2 * root]), __ldg(&sc.nodes[2 * root + 1]), lr, te) && !(te > best)))
+                        sub.put(ssp++, __ldg(&sc.wide_code[root]), te);
+                }
+            }
+        } else {
+            // the ray is done (or a stack overflowed): finish it and push it
+            if (overflow) atomicOr(ps.error, 1);
+            Hit h;
+            const bool hit = closest_hit_finish(sc, wr, best, best_obj, best_inst, h);
+            const int family = trace_finish(sc, ps, p, ps.ray_o[p], ps.ray_d[p], hit, h);
+            if (family >= 0) {
+                const unsigned grp = __match_any_sync(__activemask(), family);
+                const int leader = __ffs(grp) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(&ps.counts[queue_slot(bounce, kQLambert + family)], __popc(grp));
+                base = __shfl_sync(grp, base, leader);
+                ps.mat_queue[family][base + __popc(grp & ((1u << lane) - 1u))] = p;
+            }
+            p = -1;
         }
     }
 }
