@@ -319,6 +319,30 @@ lambda_status lambda_autotune_batch(lambda_ctx *ctx, const lambda_render_desc *p
 lambda_status lambda_set_tuning(lambda_ctx *ctx, const lambda_tuning *tuning);
 lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning *tuning);
 
+/* Limits of the device-side guards. Every wait in the kernels is bounded and every
+ * traversal stack push is checked; these settings let a test make a guard fire and
+ * check that the call returns its error and that the next call on the same context
+ * is correct. No reference counterpart (the reference's traversal stack is unchecked,
+ * scene/scene.h:60-118, and its host polls the render forever, main.cpp:129-146).
+ *   mma_polls      polls of each tensor-core MMA-completion wait before it gives up
+ *                  (LAMBDA_DEFAULT_MMA_POLLS); 0 gives up at once. A wait that gives
+ *                  up lets the MMAs already issued finish (bounded by the default)
+ *                  before TMEM is read or freed, and the call returns
+ *                  LAMBDA_ERR_TIMEOUT.
+ *   stack_entries  cap on traversal stack entries per ray and BVH level, 0 for none:
+ *                  the stacks then hold the most entries the uploaded BVH can need.
+ *                  Below that, a ray that would overflow stops, and the call returns
+ *                  LAMBDA_ERR_QUEUE_OVERFLOW.
+ * lambda_set_limits(ctx, NULL) restores the defaults. */
+#define LAMBDA_DEFAULT_MMA_POLLS 4194304u
+typedef struct lambda_limits {
+    uint32_t mma_polls;
+    int32_t stack_entries;
+} lambda_limits;
+
+lambda_status lambda_set_limits(lambda_ctx *ctx, const lambda_limits *limits);
+lambda_status lambda_get_limits(const lambda_ctx *ctx, lambda_limits *limits);
+
 /* Statistics of the last lambda_render or lambda_render_batch on this context. */
 typedef struct lambda_render_stats {
     double render_ms;          /* device time from first raygen to film write */
@@ -399,6 +423,19 @@ lambda_status lambda_thinfilm_fp64(lambda_ctx *ctx, const lambda_film_query *q, 
 #define LAMBDA_MLP_OUT 4
 #define LAMBDA_MLP_PARAMS (5 * 64 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 * 4 + 4) /* 8964 */
 
+/* Where a render trusts the surrogate inside its trained range. The network's
+ * error concentrates at grazing incidence: over 2^18 uniform queries of the
+ * trained box its largest |R error| is 0.19 at cos theta < 0.05, and the next
+ * largest sit at a substrate index near 1 (a film in air) below cos theta 0.2.
+ * A thin-film hit with cos theta < LAMBDA_SURROGATE_GRAZING_COS, or with
+ * n_sub < LAMBDA_SURROGATE_LOW_SUB_INDEX and cos theta < LAMBDA_SURROGATE_LOW_SUB_COS,
+ * therefore takes the exact FP32 transfer matrix, like a hit outside the range
+ * (the render statistics count both as fallbacks). The query entry points
+ * (lambda_surrogate_eval*) evaluate the network everywhere in the range. */
+#define LAMBDA_SURROGATE_GRAZING_COS 0.05f
+#define LAMBDA_SURROGATE_LOW_SUB_INDEX 1.05f
+#define LAMBDA_SURROGATE_LOW_SUB_COS 0.2f
+
 /* Trained range of the surrogate (queries outside it use the exact path). */
 typedef struct lambda_film_range {
     float lambda_nm[2];
@@ -448,13 +485,17 @@ lambda_status lambda_surrogate_eval(lambda_ctx *ctx, const lambda_film_query *q,
  * thread may not call cudaMalloc, which can synchronise the device and fail under
  * the host's memory budget). It has no counterpart in the reference.
  * queries [n] and out [n][4] = (R_s, R_p, T_s, T_p) are caller-owned DEVICE
- * memory (out 16-byte aligned); results equal lambda_surrogate_eval's. The only
- * scratch is a fixed array of LAMBDA_SURROGATE_STATIC_MAX_QUERIES encoded queries
- * (4 MiB) compiled into the library, held by every GPU that loads it until the
- * process exits; n above the limit returns LAMBDA_ERR_INVALID_ARGUMENT. The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress), so
- * make that first call before any stream capture. Every call shares the array:
- * calls that overlap on the GPU race. The call blocks until `out` is written. */
+ * memory of the context's own GPU, or managed memory (out 16-byte aligned); a
+ * host pointer or another GPU's memory returns LAMBDA_ERR_INVALID_ARGUMENT.
+ * Results equal lambda_surrogate_eval's bit for bit. The only scratch is a fixed
+ * array of LAMBDA_SURROGATE_STATIC_MAX_QUERIES encoded queries (4 MiB) compiled
+ * into the library, held by every GPU that loads it until the process exits; n
+ * above the limit returns LAMBDA_ERR_INVALID_ARGUMENT. The first call on a device,
+ * and the first after a device reset, looks up the array's device address
+ * (cudaGetSymbolAddress), which can load the library's GPU module and so
+ * allocate: make that first call as a warm-up, outside the code that must not
+ * allocate and before any stream capture. Every call shares the array: calls that
+ * overlap on the GPU race. The call blocks until `out` is written. */
 #define LAMBDA_SURROGATE_STATIC_MAX_QUERIES 131072
 lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lambda_film_query *queries, int32_t n, float *out);
 

@@ -290,6 +290,19 @@ class Context:
         self._check(self._lib.lambda_get_tuning(self._h, C.byref(t)))
         return t
 
+    def set_limits(self, mma_polls: int = N.DEFAULT_MMA_POLLS, stack_entries: int = 0) -> None:
+        """Device guard limits (lambda_set_limits), for tests that make a guard fire."""
+        lim = N.Limits(mma_polls, stack_entries)
+        self._check(self._lib.lambda_set_limits(self._h, C.byref(lim)))
+
+    def reset_limits(self) -> None:
+        self._check(self._lib.lambda_set_limits(self._h, None))
+
+    def limits(self) -> N.Limits:
+        lim = N.Limits()
+        self._check(self._lib.lambda_get_limits(self._h, C.byref(lim)))
+        return lim
+
     def stats(self) -> RenderStats:
         st = N.RenderStats()
         self._check(self._lib.lambda_get_render_stats(self._h, C.byref(st)))

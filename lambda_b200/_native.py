@@ -39,6 +39,10 @@ RENDER_PROFILE_STAGES = 4
 RENDER_THINFILM_FP64 = 8
 NUM_STAGES = 13
 PATH_KERNEL_PIXELS = 32768  # LAMBDA_PATH_KERNEL_PIXELS
+# the surrogate's grazing region, where renders take the exact transfer matrix
+SURROGATE_GRAZING_COS = 0.05  # LAMBDA_SURROGATE_GRAZING_COS
+SURROGATE_LOW_SUB_INDEX = 1.05  # LAMBDA_SURROGATE_LOW_SUB_INDEX
+SURROGATE_LOW_SUB_COS = 0.2  # LAMBDA_SURROGATE_LOW_SUB_COS
 STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
                "shadow", "finish", "film_encode", "film_mlp", "film_scatter", "path")
 
@@ -143,6 +147,14 @@ class TrainDesc(C.Structure):
                 ("learning_rate", C.c_float), ("seed", C.c_uint64), ("range", FilmRange)]
 
 
+class Limits(C.Structure):
+    """lambda_limits: device guard limits for tests that make a guard fire."""
+    _fields_ = [("mma_polls", C.c_uint32), ("stack_entries", C.c_int32)]
+
+
+DEFAULT_MMA_POLLS = 4194304  # LAMBDA_DEFAULT_MMA_POLLS
+
+
 class TrainReport(C.Structure):
     _fields_ = [("train_ms", C.c_double), ("label_ms", C.c_double), ("final_loss", C.c_float),
                 ("max_abs_error", C.c_float), ("mean_abs_error", C.c_float), ("audit_samples", C.c_int32)]
@@ -166,6 +178,8 @@ _SIGNATURES = {
     "lambda_autotune_batch": (C.c_int, [_P, C.POINTER(RenderDesc), C.c_int32, C.POINTER(Tuning)]),
     "lambda_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "lambda_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "lambda_set_limits": (C.c_int, [_P, C.POINTER(Limits)]),
+    "lambda_get_limits": (C.c_int, [_P, C.POINTER(Limits)]),
     "lambda_get_render_stats": (C.c_int, [_P, C.POINTER(RenderStats)]),
     "lambda_get_stage_times": (C.c_int, [_P, C.POINTER(StageTime)]),
     "lambda_trace_closest": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P]),

@@ -9,7 +9,9 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF_SRC = "/root/reference/src"
+# The reference checkout's src/ tree, read only by the oracle recipe; override with
+# LAMBDA_REF_SRC. Where it is absent the reference harness is simply not built.
+REF_SRC = os.environ.get("LAMBDA_REF_SRC", "/root/reference/src")
 
 
 def _make(args):

@@ -8,13 +8,20 @@
 
 Both are published data and must hold the same values for results to match.
 Output: tables.inc (C++ arrays) and ../../_tables.py (the permutation, for the
-scene generator). Run once: python gen_tables.py /root/reference/src/core/constants.h
+scene generator). Run once: python gen_tables.py <reference>/src/core/constants.h
+(or set LAMBDA_REF_SRC to the reference's src/ directory).
 """
 import os
 import re
 import sys
 
-src = open(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/core/constants.h").read()
+if len(sys.argv) > 1:
+    path = sys.argv[1]
+elif os.environ.get("LAMBDA_REF_SRC"):
+    path = os.path.join(os.environ["LAMBDA_REF_SRC"], "core", "constants.h")
+else:
+    sys.exit("usage: python gen_tables.py <reference>/src/core/constants.h (or set LAMBDA_REF_SRC)")
+src = open(path).read()
 
 perm_txt = re.search(r"h_PERMUTATION\[\]\s*=\s*\{([^}]*)\}", src).group(1)
 perm = [int(x) for x in perm_txt.replace("\n", " ").split(",") if x.strip()]

@@ -321,6 +321,10 @@ DeviceScene lambda_ctx::scene_view(int width) const {
     v.bvh_width = 2 << k;
     v.stack_tlas = wide_stack[k][0];
     v.stack_blas = wide_stack[k][1];
+    if (limits.stack_entries > 0) {  // a test cap (lambda_set_limits): kernels then size and check stacks by it
+        v.stack_tlas = std::min(v.stack_tlas, limits.stack_entries);
+        v.stack_blas = std::min(v.stack_blas, limits.stack_entries);
+    }
     return v;
 }
 
@@ -1181,6 +1185,23 @@ extern "C" lambda_status lambda_set_tuning(lambda_ctx *ctx, const lambda_tuning 
 extern "C" lambda_status lambda_get_tuning(const lambda_ctx *ctx, lambda_tuning *tuning) {
     if (!ctx || !tuning) return LAMBDA_ERR_INVALID_ARGUMENT;
     *tuning = ctx->tuning;
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_set_limits(lambda_ctx *ctx, const lambda_limits *limits) {
+    if (!ctx) return LAMBDA_ERR_INVALID_ARGUMENT;
+    if (!limits) {
+        ctx->limits = lambda_limits{LAMBDA_DEFAULT_MMA_POLLS, 0};
+        return LAMBDA_OK;
+    }
+    if (limits->stack_entries < 0) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "stack_entries must be >= 0");
+    ctx->limits = *limits;
+    return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_get_limits(const lambda_ctx *ctx, lambda_limits *limits) {
+    if (!ctx || !limits) return LAMBDA_ERR_INVALID_ARGUMENT;
+    *limits = ctx->limits;
     return LAMBDA_OK;
 }
 

@@ -28,6 +28,7 @@
 #include <mutex>
 #include <vector>
 
+#include "buffer_policy.h"
 #include "engine.h"
 #include "lambda_gpu.h"
 #define LAMBDA_WAVEFRONT_HELPERS_ONLY
@@ -343,12 +344,13 @@ __device__ __forceinline__ void store_relu32(uint8_t *smem, const TileCtx &t, co
 // loads, 32 ReLU+BF16 conversions and eight 16-byte stores of the next operand row
 // (kLowRegs: one 32-column half at a time, for kernels held to 64 registers). On
 // return y holds this thread's four outputs. Returns false, uniformly across the
-// warpgroup, if an MMA completion wait timed out (the accumulator is then not read
-// as valid).
+// warpgroup, if an MMA completion wait gave up after `polls` polls. A thread whose
+// wait gives up then waits again, bounded by the default limit, for the MMAs already
+// issued, so no TMEM is read or freed under a running MMA; the tile runs to its end
+// in step with the warpgroup's barriers, and its result is discarded.
 template <int G, bool kLowRegs = false>
-__device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
+__device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y, uint32_t polls) {
     const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
-    const uint32_t kPoll = 1u << 22;
     const uint32_t act = t.base + uint32_t(t.act);
     bool done = true;
 #pragma unroll 1
@@ -374,7 +376,10 @@ __device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y) {
             }
             mma_commit(t.bar);
         }
-        done = mbar_wait(t.bar, t.phase, kPoll) && done;
+        if (!mbar_wait(t.bar, t.phase, polls)) {
+            done = false;
+            mbar_wait(t.bar, t.phase, LAMBDA_DEFAULT_MMA_POLLS);  // drain what was issued
+        }
         t.phase ^= 1u;
         fence_after();
         if (layer < 3) {
@@ -422,12 +427,13 @@ __device__ __forceinline__ void put_row(uint8_t *smem, const TileCtx &t, const f
 // out: rows x (R_s, R_p, T_s, T_p). A CTA holds G warpgroups, each working through
 // its own 128-row tiles with its own accumulator, so G dependent layer chains
 // overlap per CTA while the weights are loaded once. Error bit 1 is set if an MMA
-// completion wait timed out.
+// completion wait gave up after `polls` polls (LAMBDA_DEFAULT_MMA_POLLS normally).
 template <bool kQueries, int G>
 __global__ void __launch_bounds__(128 * G, G == 1 ? 1 : 8 / G) k_mlp_tc(const uint4 *__restrict__ packed,
                                                                    const void *__restrict__ in, int n_rows, Range rg,
                                                                    float4 *__restrict__ out, int *error,
-                                                                   const int *count = nullptr, int rows_per_count = 0) {
+                                                                   uint32_t polls, const int *count = nullptr,
+                                                                   int rows_per_count = 0) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int rows = count ? rows_per_count * *count : n_rows;
     const int tiles = (rows + kTileM - 1) / kTileM;
@@ -455,7 +461,7 @@ __global__ void __launch_bounds__(128 * G, G == 1 ? 1 : 8 / G) k_mlp_tc(const ui
         }
         put_row(smem, t, e);
         float y[kOut];
-        ok = mlp_tile<G, (G > 2)>(smem, t, y);
+        ok = mlp_tile<G, (G > 2)>(smem, t, y, polls);
         if (ok && row < rows) out[row] = make_float4(y[0], y[1], y[2], y[3]);
     }
     if (!ok && t.row == 0) atomicOr(error, 2);
@@ -625,6 +631,13 @@ struct FilmSurrogate {
     float lam_lo, lam_hi, cos_lo, cos_hi, d_lo, d_hi, nf_lo, nf_hi, ns_lo, ns_hi;
 };
 
+// Inside the trained range, the grazing region where the render takes the exact
+// transfer matrix because the network's error concentrates there.
+__device__ __forceinline__ bool grazing_exact(float cos_theta, float n_sub) {
+    return cos_theta < LAMBDA_SURROGATE_GRAZING_COS ||
+           (n_sub < LAMBDA_SURROGATE_LOW_SUB_INDEX && cos_theta < LAMBDA_SURROGATE_LOW_SUB_COS);
+}
+
 // Thin-film shade with the surrogate, step 1 of 3 (k_film_encode, k_mlp_tc,
 // k_film_scatter): for thin-film hit i of the bounce, the film thickness and the
 // four hero-wavelength queries (lambda, cos, thickness, n_film, n_sub), encoded as
@@ -632,8 +645,8 @@ struct FilmSurrogate {
 // The domain is a single film with real indices between air (index exactly 1) and
 // a substrate inside the trained box. A back-face hit (light inside the substrate)
 // is mapped to the equivalent incidence from air by Snell's law, since a lossless
-// stack reflects the same from both sides. Hits outside the domain, and back-face
-// hits past the critical angle (where the transfer matrix of material.h:263-309
+// stack reflects the same from both sides. Hits outside the domain or in its
+// grazing region (grazing_exact), and back-face hits past the critical angle (where the transfer matrix of material.h:263-309
 // does not return the physical R = 1), are left to the exact FP32 transfer matrix
 // in step 3; their rows are zeros.
 __global__ void __launch_bounds__(256) k_film_encode(int bounce, RenderParams rp, DeviceScene sc, PathState ps,
@@ -665,7 +678,7 @@ __global__ void __launch_bounds__(256) k_film_encode(int bounce, RenderParams rp
             }
             ok = ok && a.x == 1.0 && a.y == 0.0 && b.y == 0.0 && c.y == 0.0 && nf >= fs.nf_lo && nf <= fs.nf_hi &&
                  ns >= fs.ns_lo && ns <= fs.ns_hi && c0 >= fs.cos_lo && c0 <= fs.cos_hi && lam >= fs.lam_lo &&
-                 lam <= fs.lam_hi;
+                 lam <= fs.lam_hi && !grazing_exact(c0, ns);
             const float v[kIn] = {lam, c0, d, nf, ns};
             encode(v, fs.rg, e[w]);
         }
@@ -837,7 +850,8 @@ lambda_status run_mlp(lambda_ctx *ctx, const void *in, int n_rows, float4 *out_d
     const int tiles = (n_rows + kTileM - 1) / kTileM;
     constexpr int G = kQueryWarpgroups;
     k_mlp_tc<kQueries, G><<<query_grid<kQueries>(ctx, tiles), 128 * G, kSmemOf<G>, ctx->stream>>>(
-        reinterpret_cast<const uint4 *>(w), in, n_rows, to_range(ctx->surrogate_range), out_dev, err);
+        reinterpret_cast<const uint4 *>(w), in, n_rows, to_range(ctx->surrogate_range), out_dev, err,
+        ctx->limits.mma_polls);
     CK(cudaGetLastError(), "launch MLP kernel");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream), "read flags");
@@ -878,7 +892,7 @@ int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const
     k_film_encode<<<grid(film_encode_ctas, 256), 256, 0, s>>>(bounce, rp, sc, ps, fs, rows, in_domain);
     if (prof) prof->end();
     if (prof) prof->begin(10);
-    k_mlp_tc<false, G><<<mlp_grid, 128 * G, kSmemOf<G>, s>>>(w, rows, 0, Range{}, out, ps.error,
+    k_mlp_tc<false, G><<<mlp_grid, 128 * G, kSmemOf<G>, s>>>(w, rows, 0, Range{}, out, ps.error, limits.mma_polls,
                                                              ps.counts + queue_slot(bounce, kQFilm), kHero);
     if (prof) prof->end();
     if (prof) prof->begin(11);
@@ -1120,6 +1134,10 @@ extern "C" lambda_status lambda_surrogate_grad(lambda_ctx *ctx, const float *par
 // every GPU that loads the library until the process exits. The array is shared
 // by all calls and keeps the last call's contents; calls that overlap on the GPU
 // (other streams, other threads, other contexts on the same device) race on it.
+// The first call on a device (and the first after a device reset) looks up the
+// array's device address, which can load this library's GPU module and so
+// allocate: make that call once as a warm-up, outside the region that must not
+// allocate and before any stream capture.
 // ---------------------------------------------------------------------------
 
 namespace {
@@ -1130,32 +1148,78 @@ static_assert(kStaticMaxQueries == 131072, "header and library disagree");
 static __device__ __align__(256) float g_static_rows[kStaticMaxQueries * mlp::kRowStride];
 static __device__ __align__(256) int g_static_error[4];
 
-// Device addresses of the two arrays, looked up once per device. In host code the
-// array names are host-side stand-ins, never device addresses.
+// Device addresses of the two arrays, looked up once per device and CUDA context.
+// In host code the array names are host-side stand-ins, never device addresses.
 struct StaticScratch {
     float *rows = nullptr;
     int *error = nullptr;
+    unsigned long long context_id = 0;  // the context the addresses belong to
     bool ready = false;
 };
 constexpr int kMaxDevices = 64;
 StaticScratch g_static_scratch[kMaxDevices];
 std::mutex g_static_mutex;
 
+// Unique id of the calling thread's current CUDA context (cuCtxGetCurrent and
+// cuCtxGetId, reached through the runtime's driver entry points so the library
+// needs no link to libcuda), or 0 when the driver cannot tell. A device reset
+// destroys the primary context and the next one gets a new id; the module is then
+// loaded again at new addresses.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void **);
+    using GetId = int (*)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    void *c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != 0 || !c || get_id(c, &id) != 0) return 0;
+    return id;
+}
+
 lambda_status static_scratch(lambda_ctx *ctx, StaticScratch &out) {
     if (ctx->device < 0 || ctx->device >= kMaxDevices) return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "device index too large");
     std::lock_guard<std::mutex> lock(g_static_mutex);
     StaticScratch &s = g_static_scratch[ctx->device];
-    if (!s.ready) {
-        CK(cudaSetDevice(ctx->device), "cudaSetDevice");  // the lookup is per device: this device must be current
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");  // the lookup is per device: this device must be current
+    const unsigned long long id = current_context_id();
+    // an unknown id (0) never matches, so the addresses are looked up again on every call
+    if (!s.ready || id == 0 || id != s.context_id) {
         void *rows = nullptr, *err = nullptr;
         CK(cudaGetSymbolAddress(&rows, g_static_rows), "look up the static scratch array");
         CK(cudaGetSymbolAddress(&err, g_static_error), "look up the static error word");
         s.rows = static_cast<float *>(rows);
         s.error = static_cast<int *>(err);
+        s.context_id = id;
         s.ready = true;
     }
     out = s;
     return LAMBDA_OK;
+}
+
+// Whether a caller-owned buffer can be read or written by this context's kernels:
+// device memory of the context's GPU, or managed memory.
+bool buffer_on_context_device(const void *p, int device) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return lambda_host::buffer_usable_on(int(a.type), a.device, device);
 }
 
 __global__ void k_encode_queries(const lambda_film_query *q, int n, mlp::Range rg, float *rows) {
@@ -1180,14 +1244,16 @@ extern "C" lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lam
                          "split larger batches into several calls");
     if (!ctx->has_surrogate) return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "no surrogate installed");
     if (n == 0) return LAMBDA_OK;
-    if (!queries || !out || !is_device_pointer(queries) || !is_device_pointer(out))
-        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "lambda_surrogate_eval_static takes device pointers only");
+    if (!queries || !out || !buffer_on_context_device(queries, ctx->device) ||
+        !buffer_on_context_device(out, ctx->device))
+        return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT,
+                         "lambda_surrogate_eval_static takes device pointers only, on the context's own GPU "
+                         "(or managed memory)");
     if (reinterpret_cast<uintptr_t>(out) % 16 != 0)
         return ctx->fail(LAMBDA_ERR_INVALID_ARGUMENT, "lambda_surrogate_eval_static: out must be 16-byte aligned");
     StaticScratch sc;
-    lambda_status st = static_scratch(ctx, sc);
+    lambda_status st = static_scratch(ctx, sc);  // leaves the context's device current
     if (st != LAMBDA_OK) return st;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     CK(configure_mlp_kernels(), "configure MLP kernels");
     CK(cudaMemsetAsync(sc.error, 0, sizeof(int) * 4, ctx->stream), "clear the static error word");
     k_encode_queries<<<(n + 255) / 256, 256, 0, ctx->stream>>>(queries, n, to_range(ctx->surrogate_range), sc.rows);
@@ -1195,7 +1261,8 @@ extern "C" lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lam
     const int tiles = (n + kTileM - 1) / kTileM;
     constexpr int G = kQueryWarpgroups;
     k_mlp_tc<false, G><<<query_grid<false>(ctx, tiles), 128 * G, kSmemOf<G>, ctx->stream>>>(reinterpret_cast<const uint4 *>(w), sc.rows, n, Range{},
-                                                            reinterpret_cast<float4 *>(out), sc.error);
+                                                            reinterpret_cast<float4 *>(out), sc.error,
+                                                            ctx->limits.mma_polls);
     CK(cudaGetLastError(), "launch MLP kernel");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, sc.error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "read the static error word");

@@ -62,6 +62,10 @@ def test_python_mirrors_match_the_header():
     defines = dict(re.findall(r"#define (LAMBDA_\w+) (\d+)", text))
     assert int(defines["LAMBDA_NUM_STAGES"]) == N.NUM_STAGES == len(N.STAGE_NAMES)
     assert int(defines["LAMBDA_PATH_KERNEL_PIXELS"]) == N.PATH_KERNEL_PIXELS
+    fdefs = {k: float(v) for k, v in re.findall(r"#define (LAMBDA_SURROGATE_\w+) ([0-9.]+)f", text)}
+    assert fdefs == {"LAMBDA_SURROGATE_GRAZING_COS": N.SURROGATE_GRAZING_COS,
+                     "LAMBDA_SURROGATE_LOW_SUB_INDEX": N.SURROGATE_LOW_SUB_INDEX,
+                     "LAMBDA_SURROGATE_LOW_SUB_COS": N.SURROGATE_LOW_SUB_COS}
 
 
 def test_null_arguments_are_rejected():
@@ -122,3 +126,34 @@ def test_write_pfm_round_trip(tmp_path):
     assert np.allclose(read(tmp_path / "b.pfm"), want, rtol=1e-6, atol=1e-6)
     with pytest.raises(lb.LambdaError):
         lb.write_pfm(str(tmp_path / "c.ppm"), img)
+
+
+def test_static_entry_point_buffer_rule(tmp_path):
+    """The rule lambda_surrogate_eval_static applies to caller buffers
+    (host/buffer_policy.h), compiled and run on the CPU: device memory of the
+    context's own GPU or managed memory passes; host, unregistered and another
+    GPU's device memory are refused, so they return an error instead of reaching a
+    kernel."""
+    src = tmp_path / "policy.cpp"
+    src.write_text(r'''
+#include "buffer_policy.h"
+#include <cstdio>
+using namespace lambda_host;
+int main() {
+    int bad = 0;
+    bad += !buffer_usable_on(kMemDevice, 0, 0);
+    bad += !buffer_usable_on(kMemDevice, 3, 3);
+    bad += buffer_usable_on(kMemDevice, 1, 0);   // another GPU's memory
+    bad += buffer_usable_on(kMemDevice, 0, 1);
+    bad += !buffer_usable_on(kMemManaged, 5, 0);  // managed memory migrates
+    bad += buffer_usable_on(kMemHost, 0, 0);
+    bad += buffer_usable_on(kMemUnregistered, 0, 0);
+    std::printf("%d\n", bad);
+    return bad;
+}
+''')
+    exe = tmp_path / "policy"
+    inc = os.path.join(ROOT, "lambda_b200", "csrc", "host")
+    subprocess.run(["g++", "-std=c++20", "-I", inc, str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout

@@ -118,3 +118,27 @@ def test_non_finite_pixels_are_the_references(scene_dir, ctx):
     for py, px in bad:
         rad = r.trace_pixel(sc.seed, int(px), int(py))
         assert not np.isfinite(rad).all(), f"pixel ({px}, {py}) is finite in the reference"
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference harness not built")
+def test_benchmark_frame_at_full_resolution(scene_dir, ctx):
+    """The benchmarked frame at its full 1920x1080 and render seed, at 1 spp (its
+    256 spp would take minutes on the CPU), in the exact and FP64 thin-film forms,
+    against the reference's own renderImage at the same seed and spp: relRMSE on
+    linear XYZ within 1%, and no pixel non-finite that the reference renders finite."""
+    sc = scenes.thinfilm_spheres(scene_dir, 1920, 1080, 256, name="full_thinfilm.lrd")
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx.upload(scene)
+    r = ref_scene(sc.lrd)
+    r.set_samples(1)
+    want = r.render(sc.seed)[0]
+    ref_bad = ~np.isfinite(want).all(axis=2)
+    for name, flags in (("exact", lb.RENDER_THINFILM_EXACT), ("fp64", lb.RENDER_THINFILM_FP64)):
+        img = ctx.render(scene.render_desc(seed=sc.seed, flags=flags, samples=1))
+        bad = ~np.isfinite(img).all(axis=2)
+        assert not (bad & ~ref_bad).any(), f"{name}: a pixel the reference renders finite is non-finite"
+        skip = (bad | ref_bad)[..., None]
+        err = rel_rmse(np.where(skip, 0, img), np.where(skip, 0, want))
+        same = float((img == want).all(axis=2).mean())
+        print(f"1920x1080 x 1 spp, {name}: relRMSE {err:.3e}, identical pixels {same:.4f}")
+        assert err <= TOL_RELRMSE, f"{name}: relRMSE {err}"

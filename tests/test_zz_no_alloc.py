@@ -12,7 +12,6 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from lambda_b200 import _native as N
 from lambda_b200 import surrogate
 
 pytestmark = pytest.mark.gpu
@@ -27,24 +26,38 @@ def _queries(n, seed):
 
 
 def test_static_scratch_matches_allocating_entry_point(ctx):
+    """Bit-equal to lambda_surrogate_eval on consecutive calls, with device memory
+    untouched after the warm-up call."""
     import torch
 
     surrogate.install(ctx)
     fn = ctx._lib.lambda_surrogate_eval_static
-    # two calls in a row: the second must not see the first call's scratch contents
-    for seed, n in ((1, 40000), (2, 1234)):
+    # small, then large, then full: rows a larger earlier call left in the shared
+    # scratch would show up in a later call that read past its own n
+    cases = [(11, 1234), (12, 40000), (13, LIMIT), (14, 777)]
+    prepared = []
+    for seed, n in cases:
         q = _queries(n, seed)
         want = ctx.surrogate_eval(q)  # the allocating entry point
         dq = torch.from_numpy(q).cuda()
-        dout = torch.full((n, 4), float("nan"), dtype=torch.float32, device="cuda")
+        dout = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        prepared.append((n, want, dq, dout))
+    # warm-up: the first call on a device looks up the scratch array's address
+    n, _, dq, dout = prepared[0]
+    assert fn(ctx._h, C.c_void_p(dq.data_ptr()), n, C.c_void_p(dout.data_ptr())) == 0, ctx.last_error
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for n, want, dq, dout in prepared:
+        dout.fill_(float("nan"))
         st = fn(ctx._h, C.c_void_p(dq.data_ptr()), n, C.c_void_p(dout.data_ptr()))
         assert st == 0, ctx.last_error
         got = dout.cpu().numpy()
-        scale = np.abs(want).max()
-        err = np.abs(got - want)
-        # same tolerance as the tensor-core inference test: the two paths differ only in
-        # where the input encoding is computed (host libm vs device sincosf)
-        assert err.max() <= 1e-2 * scale and err.mean() <= 1e-3 * scale, (err.max(), err.mean())
+        # both entry points encode the queries with the same device code and run the
+        # same MLP kernel per 128-row tile, so the results are the same bits
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), \
+            f"n={n}: {int((got != want).sum())} results differ, max {np.abs(got - want).max()}"
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before, "device memory changed across allocation-free calls"
 
 
 def test_static_scratch_rejects_oversized_batches(ctx):
