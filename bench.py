@@ -277,6 +277,36 @@ def _xyz(img):
     return to_xyz(img)
 
 
+def reference_gpu(lrd: str, seed: int, spp: int, ref_cpu_img=None, steps: int = 3) -> dict:
+    """Secondary GPU baseline: the reference's own CUDA renderKernel on this GPU
+    (oracle/_ref/libref_lambda_gpu.so, its headers compiled as its CUDA build
+    compiles them, for sm_100a), driven as its main.cpp drives it, on the same frame
+    and seed at `spp` samples: device time per launch (mean of `steps` after one
+    warm-up launch) and its image against the reference CPU frame of the same seed
+    and spp."""
+    from oracle import ref_gpu
+    from tests.helpers import rel_rmse
+
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libref_lambda_gpu.so not built (needs the reference sources)"}
+    try:
+        g = ref_gpu.RefGpuScene(lrd, W, H)
+        g.set_samples(spp)
+        img, _ = g.render(seed)
+        times = [g.render(seed, image=False)[1] for _ in range(steps)]
+        g.close()
+    except ref_gpu.RefGpuError as e:
+        return {"unavailable": str(e)}
+    ms = float(np.mean(times))
+    res = {"value": W * H * spp / (ms / 1000.0), "unit": UNIT, "ms_per_launch": ms, "spp": spp, "seed": seed,
+           "launches_timed": steps, "kernel": "renderKernel, 16x16 blocks, one thread per pixel (main.cpp)"}
+    if ref_cpu_img is not None:
+        keep = (np.isfinite(img).all(2) & np.isfinite(ref_cpu_img).all(2))[..., None]
+        res["relrmse_xyz_vs_reference_cpu"] = rel_rmse(np.where(keep, img, 0), np.where(keep, ref_cpu_img, 0))
+        res["identical_pixel_frac_vs_reference_cpu"] = float((img == ref_cpu_img).all(2).mean())
+    return res
+
+
 CONVERGED_SPP, CONVERGED_SEED = 4096, 17
 # stated bound on the surrogate's added image error: its relRMSE against the
 # converged frame may exceed the exact form's by at most this much (absolute)
@@ -517,7 +547,7 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
             continue
         sc = make()
         t0 = time.perf_counter()
-        scene = lb.HostScene.parse(sc.lrd)
+        scene = lb.HostScene.parse_gpu(ctx, sc.lrd)
         parse_s = time.perf_counter() - t0
         t0 = time.perf_counter()
         ctx.upload(scene)
@@ -556,7 +586,8 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+bf16" if flags & lb.RENDER_THINFILM_SURROGATE else "f32", "data": "synthetic",
                 "config": {"workload": text, "paths_per_step": paths, "l2": "flushed between timed steps (256 MB write)",
-                           "host_parse_and_bvh_s": parse_s, "upload_s": upload_s,
+                           "parse_and_build_s": parse_s, "build": "lambda_parse_lrd_gpu (instance bounds and "
+                           "large BVH builds on the GPU)", "upload_s": upload_s,
                            "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
                                       "grid_scale": tuning.grid_scale, "bvh_width": tuning.bvh_width,
                                       "source": tuning_source}},
@@ -793,6 +824,9 @@ def main():
                 out["cpu_baseline"] = cb
                 # the metric's quality gate on the benchmarked frame itself
                 out["parity"] = frame_parity(ctx, scene, sc.seed, ref_spp, ref_img, have_surrogate)
+                out["reference_gpu"] = reference_gpu(sc.lrd, sc.seed, ref_spp, ref_img)
+                if "value" in out["reference_gpu"]:
+                    out["reference_gpu"]["ours_over_reference_gpu"] = value / out["reference_gpu"]["value"]
         print(json.dumps(out))
     ctx.close()
     if world > 1:

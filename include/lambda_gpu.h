@@ -198,6 +198,19 @@ typedef struct lambda_host_scene lambda_host_scene;
  * ("file:line: message" or "file: failed to open file (...)") into err. */
 lambda_status lambda_parse_lrd(const char *path, lambda_host_scene **out, char *err, size_t err_len);
 
+/* lambda_parse_lrd with the scene build's heavy steps on the context's GPU, for the
+ * same scene byte for byte: every instance's world bounds and centroid
+ * (Instance::min/max/center, src/scene/instance.h:54-101, which visit every object
+ * of every instance) and the binned-SAH build (src/scene/bvh.h:111-246) of every
+ * object group or instance set of at least gpu_min_items items (0: 65536; smaller
+ * ones build faster on the host). Errors as lambda_parse_lrd's, plus
+ * LAMBDA_ERR_CUDA. Declared with the host functions because it returns a host
+ * scene; it needs a GPU. No reference counterpart: the reference builds on the
+ * host only. */
+typedef struct lambda_ctx lambda_ctx;
+lambda_status lambda_parse_lrd_gpu(lambda_ctx *ctx, const char *path, int32_t gpu_min_items, lambda_host_scene **out,
+                                   char *err, size_t err_len);
+
 /* Views of a parsed scene; pointers stay valid until lambda_host_scene_destroy. */
 lambda_status lambda_host_scene_get(const lambda_host_scene *scene, lambda_scene_desc *desc,
                                     lambda_render_settings *settings);
@@ -220,10 +233,8 @@ lambda_status lambda_write_pfm(const char *path, int32_t width, int32_t height, 
                                char *err, size_t err_len);
 
 /* ---------------------------------------------------------------------------
- * GPU context.
+ * GPU context (lambda_ctx, declared above with lambda_parse_lrd_gpu).
  * ------------------------------------------------------------------------- */
-
-typedef struct lambda_ctx lambda_ctx;
 
 /* Creates a context on one CUDA device (one stream, its own device arena). No
  * reference counterpart: the reference uses the current device and managed memory

@@ -78,6 +78,19 @@ class HostScene:
             raise LambdaError(st, err.value.decode())
         return cls(h, lib)
 
+    @classmethod
+    def parse_gpu(cls, ctx: "Context", path: str, gpu_min_items: int = 0) -> "HostScene":
+        """parse() with the scene build's heavy steps on ctx's GPU (lambda_parse_lrd_gpu):
+        the same scene byte for byte. gpu_min_items: the smallest object group or
+        instance set built on the GPU (0: the library's default)."""
+        lib = N.load()
+        h = C.c_void_p()
+        err = C.create_string_buffer(4096)
+        st = lib.lambda_parse_lrd_gpu(ctx._h, path.encode(), gpu_min_items, C.byref(h), err, len(err))
+        if st != 0:
+            raise LambdaError(st, err.value.decode() or lib.lambda_last_error(ctx._h).decode())
+        return cls(h, lib)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

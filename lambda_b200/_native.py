@@ -164,6 +164,7 @@ class TrainReport(C.Structure):
 _P = C.c_void_p
 _SIGNATURES = {
     "lambda_parse_lrd": (C.c_int, [C.c_char_p, C.POINTER(_P), C.c_char_p, C.c_size_t]),
+    "lambda_parse_lrd_gpu": (C.c_int, [_P, C.c_char_p, C.c_int32, C.POINTER(_P), C.c_char_p, C.c_size_t]),
     "lambda_host_scene_get": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(RenderSettings)]),
     "lambda_host_scene_destroy": (None, [_P]),
     "lambda_write_ppm": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _P, C.c_char_p, C.c_size_t]),

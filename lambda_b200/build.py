@@ -25,7 +25,7 @@ def build(with_oracle: bool = True) -> None:
         if os.path.exists(os.path.join(ROOT, "oracle", "lambda_oracle.c")):
             _make(["-C", os.path.join(ROOT, "oracle")])
         if os.path.isdir(REF_SRC):
-            _make(["-C", os.path.join(ROOT, "oracle"), "ref", f"REF_SRC={REF_SRC}"])
+            _make(["-C", os.path.join(ROOT, "oracle"), "ref", "ref_gpu", f"REF_SRC={REF_SRC}"])
 
 
 if __name__ == "__main__":

@@ -294,26 +294,71 @@ int build_range(const std::vector<ItemBounds> &items, std::vector<int> &order, i
     return self;
 }
 
+// Items as the 9 floats per item (lo, hi, centroid) a BuildAccel step takes.
+std::vector<float> flatten(const std::vector<ItemBounds> &items) {
+    std::vector<float> f(items.size() * 9);
+    for (size_t i = 0; i < items.size(); i++)
+        for (int k = 0; k < 3; k++) {
+            f[9 * i + k] = items[i].lo[k];
+            f[9 * i + 3 + k] = items[i].hi[k];
+            f[9 * i + 6 + k] = items[i].centroid[k];
+        }
+    return f;
+}
+
+// One build over order[start, end): on the GPU when a BuildAccel takes ranges this
+// large, else the host recursion. Both write the same nodes.
+void build_items(const std::vector<ItemBounds> &items, const std::vector<float> *flat, std::vector<int> &order,
+                 int start, int end, std::vector<lambda_bvh_node> &nodes, const BuildAccel *accel) {
+    if (accel && accel->build && flat && end - start >= accel->build_min_items) {
+        accel->build(*flat, order, start, end, nodes);
+        return;
+    }
+    build_range(items, order, start, end, nodes, 1, spawn_levels());
+}
+
 }  // namespace
 
-void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
+void build_bvh(HostScene &s, const std::vector<int> &group_offsets, const BuildAccel *accel,
+               std::vector<float> *instance_boxes) {
     s.nodes.clear();
+    if (instance_boxes) instance_boxes->clear();
     if (s.objects.empty()) return;
     s.nodes.reserve(2 * s.objects.size());
 
     // TLAS over instances
     // An instance's bounds visit all its objects (O(instances x objects)); instances
-    // are independent, so they run on all host threads.
+    // are independent, so they run on all host threads, or on the GPU.
     std::vector<ItemBounds> inst_bounds(s.instances.size());
-    parallel_for(s.instances.size(), [&](size_t i) { inst_bounds[i] = instance_bounds(s, s.instances[i]); });
+    if (accel && accel->instance_bounds) {
+        std::vector<float> f;
+        accel->instance_bounds(s, f);
+        for (size_t i = 0; i < inst_bounds.size(); i++)
+            inst_bounds[i] = ItemBounds{v3(f[9 * i], f[9 * i + 1], f[9 * i + 2]), v3(f[9 * i + 3], f[9 * i + 4], f[9 * i + 5]),
+                                        v3(f[9 * i + 6], f[9 * i + 7], f[9 * i + 8])};
+    } else {
+        parallel_for(s.instances.size(), [&](size_t i) { inst_bounds[i] = instance_bounds(s, s.instances[i]); });
+    }
     std::vector<int> order(s.instances.size());
     std::iota(order.begin(), order.end(), 0);
-    build_range(inst_bounds, order, 0, int(s.instances.size()), s.nodes, 1, spawn_levels());
+    {
+        const bool big = accel && accel->build && int(s.instances.size()) >= accel->build_min_items;
+        const std::vector<float> flat = big ? flatten(inst_bounds) : std::vector<float>{};
+        build_items(inst_bounds, big ? &flat : nullptr, order, 0, int(s.instances.size()), s.nodes, accel);
+    }
     {
         std::vector<lambda_instance> reordered;
         reordered.reserve(s.instances.size());
         for (int i : order) reordered.push_back(s.instances[i]);
         s.instances.swap(reordered);
+    }
+    if (instance_boxes) {
+        instance_boxes->resize(order.size() * 6);
+        for (size_t i = 0; i < order.size(); i++)
+            for (int k = 0; k < 3; k++) {
+                (*instance_boxes)[6 * i + k] = inst_bounds[size_t(order[i])].lo[k];
+                (*instance_boxes)[6 * i + 3 + k] = inst_bounds[size_t(order[i])].hi[k];
+            }
     }
 
     // one BLAS per object group, over a shared object order
@@ -322,9 +367,13 @@ void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
     std::vector<int> obj_order(s.objects.size());
     std::iota(obj_order.begin(), obj_order.end(), 0);
     std::map<int, int> root_of_group;
+    std::vector<float> obj_flat;
     for (size_t g = 0; g + 1 < group_offsets.size(); g++) {
         root_of_group[group_offsets[g]] = int(s.nodes.size());
-        build_range(obj_bounds, obj_order, group_offsets[g], group_offsets[g + 1], s.nodes, 1, spawn_levels());
+        const bool big = accel && accel->build && group_offsets[g + 1] - group_offsets[g] >= accel->build_min_items;
+        if (big && obj_flat.empty()) obj_flat = flatten(obj_bounds);
+        build_items(obj_bounds, big ? &obj_flat : nullptr, obj_order, group_offsets[g], group_offsets[g + 1], s.nodes,
+                    accel);
     }
     for (auto &in : s.instances) in.node = root_of_group.at(in.object);
     {
@@ -335,49 +384,86 @@ void build_bvh(HostScene &s, const std::vector<int> &group_offsets) {
     }
 }
 
-void build_lights(HostScene &s) {
+namespace {
+
+// Whether every object sphere of an instance leaves the scene sphere (C, R) of the
+// light-list merge unchanged, shown from the instance's world box alone: all of its
+// objects' transformed centres lie in the box (up to rounding) and their radii are
+// at most r_max, so if the box's farthest corner from C plus r_max stays below R by
+// a margin far wider than float rounding, the merge's "grow" test fails for each of
+// them, and since R exceeds every object radius its "replace" test fails too. The
+// margins (1e-5 relative, plus an absolute term for the centres' rounding) dwarf
+// the float error of the merge's own arithmetic (about 1e-7 relative).
+bool instance_leaves_sphere(const float *box, double r_max, const V3 &C, float R) {
+    const double c[3] = {C[0], C[1], C[2]};
+    double far = 0, mag = std::fabs(c[0]) + std::fabs(c[1]) + std::fabs(c[2]) + 1.0;
+    for (int k = 0; k < 8; k++) {
+        double d2 = 0;
+        for (int a = 0; a < 3; a++) {
+            const double v = (k >> a) & 1 ? box[3 + a] : box[a];
+            mag = std::max(mag, std::fabs(v));
+            d2 += (v - c[a]) * (v - c[a]);
+        }
+        far = std::max(far, std::sqrt(d2));
+    }
+    const double tol = 1e-5;
+    const double reach = (far + 4.0 * tol * mag) * (1 + tol) + r_max * (1 + tol);
+    return std::isfinite(reach) && reach <= double(R) * (1 - tol) && double(R) > r_max * (1 + tol);
+}
+
+}  // namespace
+
+void build_lights(HostScene &s, const std::vector<float> *instance_boxes) {
     V3 scene_center = v3(0, 0, 0);
     float scene_radius = 0;
     // The merge below is sequential in instance and object order. The transformed
     // centres and radii it consumes are not, so they are computed ahead on all host
-    // threads, a block of instances at a time (at most about 8M objects per block).
+    // threads, an instance at a time. An instance whose box shows that it changes
+    // neither the sphere (instance_leaves_sphere) nor the light list (no emissive
+    // material) is passed over: the merge's state is the same after it either way.
     struct Sphere {
         V3 c;
         float r;
     };
-    std::vector<Sphere> pre;
-    std::vector<size_t> offset;
-    int block_end = 0;
-    size_t block_base = 0;
-    for (int i = 0; i < int(s.instances.size()); i++) {
-        if (i == block_end) {
-            size_t total = 0;
-            offset.clear();
-            block_end = i;
-            while (block_end < int(s.instances.size()) && (total == 0 || total + s.instances[block_end].count <= (size_t(1) << 23))) {
-                offset.push_back(total);
-                total += size_t(s.instances[block_end].count);
-                block_end++;
-            }
-            block_base = size_t(i);
-            pre.resize(total);
-            parallel_for(size_t(block_end - i), [&](size_t k) {
-                const lambda_instance &in = s.instances[block_base + k];
-                const float scale = length(col0(in));
-                for (int j = 0; j < in.count; j++) {
-                    ObjectGeom g{s.objects[in.object + j]};
-                    pre[offset[k] + j] = Sphere{transform(in.transform, g.center(), 1), g.bounding_radius() * scale};
-                }
-            });
+    // per object group (first object, count): the largest bounding radius and
+    // whether any object's own material is emissive
+    std::map<std::pair<int, int>, std::pair<float, bool>> groups;
+    auto group_of = [&](const lambda_instance &in) {
+        auto it = groups.find({in.object, in.count});
+        if (it != groups.end()) return it->second;
+        float r = 0;
+        bool emits = false;
+        for (int j = 0; j < in.count; j++) {
+            ObjectGeom g{s.objects[in.object + j]};
+            r = std::fmax(r, g.bounding_radius());
+            emits = emits || s.materials[s.objects[in.object + j].material].type == LAMBDA_MATERIAL_EMISSIVE;
         }
+        return groups[{in.object, in.count}] = {r, emits};
+    };
+    const bool can_skip = instance_boxes && instance_boxes->size() == s.instances.size() * 6;
+    std::vector<Sphere> pre;
+    for (int i = 0; i < int(s.instances.size()); i++) {
         const lambda_instance &in = s.instances[i];
+        if (can_skip && scene_radius > 0) {
+            const auto [r_max, group_emits] = group_of(in);
+            const bool emits =
+                in.material >= 0 ? s.materials[in.material].type == LAMBDA_MATERIAL_EMISSIVE : group_emits;
+            if (!emits && instance_leaves_sphere(instance_boxes->data() + 6 * size_t(i),
+                                                 double(r_max) * double(length(col0(in))), scene_center, scene_radius))
+                continue;
+        }
+        const float scale = length(col0(in));
+        pre.resize(size_t(in.count));
+        parallel_for(size_t(in.count), [&](size_t j) {
+            ObjectGeom g{s.objects[in.object + int(j)]};
+            pre[j] = Sphere{transform(in.transform, g.center(), 1), g.bounding_radius() * scale};
+        });
         const float scale_sq = length_sq(col0(in));
-        const Sphere *sph = &pre[offset[size_t(i) - block_base]];
         for (int j = 0; j < in.count; j++) {
             const int object_index = in.object + j;
             ObjectGeom g{s.objects[object_index]};
-            const V3 object_center = sph[j].c;
-            const float object_radius = sph[j].r;
+            const V3 object_center = pre[size_t(j)].c;
+            const float object_radius = pre[size_t(j)].r;
             const V3 to_object = object_center - scene_center;
             const float distance = length(to_object);
             if (distance + scene_radius <= object_radius) {

@@ -7,10 +7,6 @@
 #include "lambda_gpu.h"
 #include "scene.h"
 
-struct lambda_host_scene {
-    lambda_host::HostScene scene;
-};
-
 namespace {
 
 void put_error(char *err, size_t len, const std::string &msg) {
@@ -22,7 +18,8 @@ void put_error(char *err, size_t len, const std::string &msg) {
 
 }  // namespace
 
-extern "C" lambda_status lambda_parse_lrd(const char *path, lambda_host_scene **out, char *err, size_t err_len) {
+lambda_status lambda_host::parse_into(const char *path, lambda_host_scene **out, char *err, size_t err_len,
+                                      const BuildAccel *accel) {
     if (!path || !out) {
         put_error(err, err_len, "lambda_parse_lrd: null argument");
         return LAMBDA_ERR_INVALID_ARGUMENT;
@@ -31,7 +28,7 @@ extern "C" lambda_status lambda_parse_lrd(const char *path, lambda_host_scene **
     auto *s = new (std::nothrow) lambda_host_scene();
     if (!s) return LAMBDA_ERR_OUT_OF_MEMORY;
     try {
-        lambda_host::parse_lrd(path, s->scene);
+        lambda_host::parse_lrd(path, s->scene, accel);
     } catch (const lambda_host::SceneError &e) {
         put_error(err, err_len, e.what());
         delete s;
@@ -48,6 +45,10 @@ extern "C" lambda_status lambda_parse_lrd(const char *path, lambda_host_scene **
     put_error(err, err_len, "");
     *out = s;
     return LAMBDA_OK;
+}
+
+extern "C" lambda_status lambda_parse_lrd(const char *path, lambda_host_scene **out, char *err, size_t err_len) {
+    return lambda_host::parse_into(path, out, err, err_len, nullptr);
 }
 
 extern "C" lambda_status lambda_host_scene_get(const lambda_host_scene *s, lambda_scene_desc *desc,

@@ -81,6 +81,8 @@ class LrdReader {
 
     void run();
 
+    const BuildAccel *accel_ = nullptr;  // build steps that run on a GPU (parse_lrd)
+
   private:
     const std::string &file_;
     HostScene &s_;
@@ -635,8 +637,9 @@ void LrdReader::run() {
     if (!have_instance) throw SceneError(LAMBDA_ERR_PARSE, file_ + ": expected \"Instance\"");
 
     group_offsets_.push_back(int(s_.objects.size()));
-    build_bvh(s_, group_offsets_);
-    build_lights(s_);
+    std::vector<float> boxes;
+    build_bvh(s_, group_offsets_, accel_, &boxes);
+    build_lights(s_, &boxes);
 }
 
 // parser.h:639-786. Faces are fan-triangulated; missing vt gives per-triangle
@@ -880,9 +883,10 @@ float spectrum_texture_average(const HostScene &s, int t) {
     }
 }
 
-void parse_lrd(const std::string &path, HostScene &scene) {
+void parse_lrd(const std::string &path, HostScene &scene, const BuildAccel *accel) {
     scene = HostScene{};
     LrdReader reader(path, scene);
+    reader.accel_ = accel;
     reader.run();
 }
 

@@ -914,31 +914,53 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         return int32_t(std::min<int64_t>(completed_base + done, completed_total));
     };
     int launches = 0;
+    bool path_pass = false;
     std::vector<Progress> progress(completed ? size_t(s_max) : 0);
     // the surrogate flag changes nothing on a scene without thin films
     const bool film_surrogate = surrogate && (sc.families & (1u << 2)) != 0;
     if (!film_surrogate && P <= tu.path_kernel_pixels) {
-        // A small pass: k_init, one k_path over all samples and bounces, k_finish.
-        using PathKernel = void (*)(RenderParams, DeviceScene, PathState);
+        // The pass as one persistent k_path launch (it seeds, traces and finishes
+        // every pixel), captured with the counter clears into one graph.
+        using PathKernel = void (*)(RenderParams, DeviceScene, PathState, int *, int *, int *);
         const PathKernel f_path = fp64 ? (bw == 2 ? k_path<2, true> : bw == 4 ? k_path<4, true> : k_path<8, true>)
                                        : (bw == 2 ? k_path<2, false> : bw == 4 ? k_path<4, false> : k_path<8, false>);
         CK(cudaFuncSetAttribute((const void *)f_path, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)),
            "configure kernels");
-        const int g_path = (P + tb - 1) / tb;
-        auto timed = [&](int stage, auto &&launch) {
-            if (prof) prof->begin(stage);
-            launch();
-            if (prof) prof->end();
-        };
+        const int g_path = grid((const void *)f_path, tb, stack_smem);
+        // counts[0]: the work counter (virtual pixels handed out); counts[1]: pixels done
+        auto launch = [&] { f_path<<<g_path, tb, stack_smem, stream>>>(rp, sc, ps, ps.counts, ps.counts + 1, ctx->progress_dev); };
         *ctx->progress_host = 0;
-        CK(clear(), "clear counters");
-        CK(cudaEventRecord(ctx->ev_start, stream), "event");
-        timed(0, [&] { k_init<<<pix_blocks, 256, 0, stream>>>(rp, ps); });
-        timed(12, [&] { f_path<<<g_path, tb, stack_smem, stream>>>(rp, sc, ps); });
-        timed(8, [&] { k_finish<<<pix_blocks, 256, 0, stream>>>(rp, sc, ps); });
-        CK(cudaGetLastError(), "launch path kernel");
-        CK(cudaEventRecord(ctx->ev_stop, stream), "event");
-        launches = 3;
+        if (prof) {
+            CK(clear(), "clear counters");
+            CK(cudaEventRecord(ctx->ev_start, stream), "event");
+            prof->begin(12);
+            launch();
+            prof->end();
+            CK(cudaGetLastError(), "launch path kernel");
+            CK(cudaEventRecord(ctx->ev_stop, stream), "event");
+        } else {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            cudaError_t e = clear();
+            launch();
+            cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            if (e != cudaSuccess || ce != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return ctx->cuda_fail(e != cudaSuccess ? e : ce, "capture path-kernel pass");
+            }
+            if (ctx->graph_exec) {
+                cudaGraphExecDestroy(ctx->graph_exec);
+                ctx->graph_exec = nullptr;
+            }
+            e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return ctx->cuda_fail(e, "instantiate path-kernel pass");
+            CK(cudaEventRecord(ctx->ev_start, stream), "event");
+            CK(cudaGraphLaunch(ctx->graph_exec, stream), "launch path-kernel pass");
+            CK(cudaEventRecord(ctx->ev_stop, stream), "event");
+        }
+        launches = 1;
+        path_pass = true;
     } else if (prof) {
         CK(clear(), "clear counters");
         CK(cudaEventRecord(ctx->ev_start, stream), "event");
@@ -1039,12 +1061,18 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     CK(cudaMemcpyAsync(stats, ps.stats, sizeof(stats), cudaMemcpyDeviceToHost, stream), "read statistics");
     CK(cudaMemcpyAsync(err, ps.error, sizeof(err), cudaMemcpyDeviceToHost, stream), "read flags");
     if (completed && !prof) {
-        // progress from the waves the graph has started (mapped host counter)
+        // progress from the mapped host counter: the waves the graph has started, or
+        // the pixels a path-kernel pass has finished (the largest value seen)
+        int32_t seen = 0;
         for (;;) {
             const cudaError_t q = cudaStreamQuery(stream);
             if (q == cudaSuccess) break;
             if (q != cudaErrorNotReady) return ctx->cuda_fail(q, "render");
-            *completed = pixels_done(std::max(0, *reinterpret_cast<volatile int *>(ctx->progress_host) - 1));
+            const int v = *reinterpret_cast<volatile int *>(ctx->progress_host);
+            const int32_t now = path_pass ? int32_t(std::min<int64_t>(int64_t(completed_base) + std::min(v, P), completed_total))
+                                          : pixels_done(std::max(0, v - 1));
+            seen = std::max(seen, now);
+            *completed = seen;
             std::this_thread::sleep_for(std::chrono::milliseconds(2));
         }
     }

@@ -81,12 +81,9 @@ __device__ __forceinline__ int tile_order(const Job &job, int l) {
     return (4 * band + rr / bw) * w + 8 * cx + rr % bw;
 }
 
-// Every pixel: seed its stream (job seed, job-local pixel index, as a render of
-// that job alone), record its depth limit, zero film and radiance.
-LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= rp.num_pixels) return;
-    const Job &job = rp.jobs[job_of(rp, p)];
+// Pixel p of `job`: seed its stream (job seed, job-local pixel index, as a render
+// of that job alone), record its depth limit, zero film and radiance.
+__device__ __forceinline__ void init_pixel(const PathState &ps, int p, const Job &job) {
     const int local = p - job.base;
     ps.rng[p] = lambda_rng::pcg_seed(job.seed, uint64_t(local));
     ps.path_info[p] = make_int2(local, job.depth);
@@ -94,6 +91,13 @@ LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
     ps.radiance[p] = make_float4(0, 0, 0, 0);
     ps.emit[p] = make_float4(0, 0, 0, 0);
     ps.lam[p] = make_float4(job.lambda_min, job.lambda_min, job.lambda_min, job.lambda_min);
+}
+
+// Every pixel of the pass: init_pixel, and the wave counters.
+LAMBDA_KERNEL void k_init(RenderParams rp, PathState ps) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= rp.num_pixels) return;
+    init_pixel(ps, p, rp.jobs[job_of(rp, p)]);
     if (p == 0) {
         ps.wave[0] = 0;
         ps.wave[1] = 0;
@@ -760,66 +764,9 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams r
     }
 }
 
-// A whole pass in one launch, for passes whose pixels are too few to fill the GPU
-// with one sample wave: thread p runs every sample of its pixel to the end, bounce
-// by bounce, through the same per-path steps as the wavefront kernels and in the
-// same order (bank and start a sample, closest hit, the material's shade, the NEE
-// shadow ray), so the image equals the wavefront's bit for bit with no launch per
-// bounce. k_finish banks the last sample. Thin films are evaluated exactly (FP32,
-// or complex double with kFp64); surrogate renders of thin films need the
-// wavefront, which batches a bounce's thin-film hits for the tensor cores. The
-// statistics are the ones the wave prologue keeps from the queue sizes.
-template <int K, bool kFp64>
-LAMBDA_KERNEL void __launch_bounds__(256) k_path(RenderParams rp, DeviceScene sc, PathState ps) {
-    extern __shared__ int stack_smem[];
-    WideStack st_a, st_b;
-    wide_stacks(stack_smem, sc, st_a, st_b);
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned n_seg = 0, n_nee = 0, n_film = 0, n_lam = 0, n_spec = 0;
-    if (v < rp.num_pixels) {
-        const Job &job = rp.jobs[job_of(rp, v)];
-        const int p = job.base + tile_order(job, v - job.base);  // a warp takes an 8x4 tile
-        for (int s = 0; s < job.samples; s++) {
-            bank_sample(sc, ps, p, job);
-            start_sample(ps, p, job, s);
-            for (int b = 0; b <= rp.depth_max; b++) {
-                n_seg++;
-                const int family = trace_path<K>(sc, ps, p, st_a, st_b);
-                if (family < 0) break;
-                bool alive, nee = false;
-                if (family == 0) {
-                    n_lam++;
-                    alive = lambert_path(sc, ps, p, b, nee);
-                    if (nee) {
-                        n_nee++;
-                        shadow_path<K>(sc, ps, p, st_a, st_b);
-                    }
-                } else if (family == 1) {
-                    n_spec++;
-                    alive = specular_path(sc, ps, p, b);
-                } else {
-                    n_film++;
-                    alive = film_path<kFp64>(sc, ps, p, b);
-                }
-                if (!alive) break;
-            }
-        }
-    }
-    // segments, NEE rays, thin-film hits, (fallback), Lambertian hits, specular hits
-    const unsigned c[6] = {n_seg, n_nee, n_film, 0u, n_lam, n_spec};
-    for (int i = 0; i < 6; i++) {
-        const unsigned sum = __reduce_add_sync(0xffffffffu, c[i]);
-        if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&ps.stats[i], (unsigned long long)sum);
-    }
-}
-
-// Last sample into the film, then the average (renderer.h:84-91), into the
-// job's own image. Jobs that finished before the last wave banked their last
-// sample in k_raygen and hold zero radiance here.
-LAMBDA_KERNEL void k_finish(RenderParams rp, DeviceScene sc, PathState ps) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= rp.num_pixels) return;
-    const Job &job = rp.jobs[job_of(rp, p)];
+// Last sample of pixel p into the film, then the average (renderer.h:84-91), into
+// the job's own image.
+__device__ __forceinline__ void finish_pixel(const DeviceScene &sc, const PathState &ps, int p, const Job &job) {
     const f3 rgb = spectrum_to_rgb(sc, sample_radiance(ps, p), from_f4(ps.lam[p]), job.lambda_range);
     float4 film = ps.film[p];
     film.x += rgb.x;
@@ -830,6 +777,91 @@ LAMBDA_KERNEL void k_finish(RenderParams rp, DeviceScene sc, PathState ps) {
     job.out[3 * local] = film.x / inv;
     job.out[3 * local + 1] = film.y / inv;
     job.out[3 * local + 2] = film.z / inv;
+}
+
+// A whole pass, every job of a batch included, in one persistent launch: each warp
+// takes the next 32 virtual pixels from the work counter `work` (zeroed with the
+// pass's counters) until none are left. Jobs lie end to end in order of decreasing
+// sample count, so the longest pixels are handed out first and the short ones fill
+// in behind them. Lane l runs virtual pixel base + l (a warp covers an 8x4 tile of
+// its job): it seeds the pixel (as k_init), runs every sample to the end, bounce by
+// bounce, through the same per-path steps as the wavefront kernels and in the same
+// order (bank and start a sample, closest hit, the material's shade, the NEE shadow
+// ray), then banks the last sample and writes the job's image (as k_finish). The
+// image therefore equals the wavefront's bit for bit, with no launch per bounce or
+// per wave. After each tile the warp adds its pixels to `done` and publishes the
+// total to `progress` (mapped host memory; the host keeps the largest value it has
+// seen, since warps publish out of order). Thin films are evaluated exactly (FP32,
+// or complex double with kFp64); surrogate renders of thin films need the
+// wavefront, which batches a bounce's thin-film hits for the tensor cores. The
+// statistics are the ones the wave prologue keeps from the queue sizes.
+template <int K, bool kFp64>
+LAMBDA_KERNEL void __launch_bounds__(256) k_path(RenderParams rp, DeviceScene sc, PathState ps, int *work, int *done,
+                                                 int *progress) {
+    extern __shared__ int stack_smem[];
+    WideStack st_a, st_b;
+    wide_stacks(stack_smem, sc, st_a, st_b);
+    const int lane = threadIdx.x & 31;
+    unsigned n_seg = 0, n_nee = 0, n_film = 0, n_lam = 0, n_spec = 0;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(work, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= rp.num_pixels) break;
+        const int v = base + lane;
+        if (v < rp.num_pixels) {
+            const Job &job = rp.jobs[job_of(rp, v)];
+            const int p = job.base + tile_order(job, v - job.base);
+            init_pixel(ps, p, job);
+            for (int s = 0; s < job.samples; s++) {
+                bank_sample(sc, ps, p, job);
+                start_sample(ps, p, job, s);
+                for (int b = 0; b <= rp.depth_max; b++) {
+                    n_seg++;
+                    const int family = trace_path<K>(sc, ps, p, st_a, st_b);
+                    if (family < 0) break;
+                    bool alive, nee = false;
+                    if (family == 0) {
+                        n_lam++;
+                        alive = lambert_path(sc, ps, p, b, nee);
+                        if (nee) {
+                            n_nee++;
+                            shadow_path<K>(sc, ps, p, st_a, st_b);
+                        }
+                    } else if (family == 1) {
+                        n_spec++;
+                        alive = specular_path(sc, ps, p, b);
+                    } else {
+                        n_film++;
+                        alive = film_path<kFp64>(sc, ps, p, b);
+                    }
+                    if (!alive) break;
+                }
+            }
+            finish_pixel(sc, ps, p, job);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int n = min(32, rp.num_pixels - base);
+            const int total = atomicAdd(done, n) + n;
+            if (progress) *reinterpret_cast<volatile int *>(progress) = total;
+        }
+    }
+    // segments, NEE rays, thin-film hits, (fallback), Lambertian hits, specular hits
+    const unsigned c[6] = {n_seg, n_nee, n_film, 0u, n_lam, n_spec};
+    for (int i = 0; i < 6; i++) {
+        const unsigned sum = __reduce_add_sync(0xffffffffu, c[i]);
+        if (lane == 0 && sum) atomicAdd(&ps.stats[i], (unsigned long long)sum);
+    }
+}
+
+// Last sample into the film, then the average, for every pixel of a wavefront pass.
+// Jobs that finished before the last wave banked their last sample in k_raygen and
+// hold zero radiance here.
+LAMBDA_KERNEL void k_finish(RenderParams rp, DeviceScene sc, PathState ps) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= rp.num_pixels) return;
+    finish_pixel(sc, ps, p, rp.jobs[job_of(rp, p)]);
 }
 
 }  // namespace lambda_dev

@@ -37,8 +37,14 @@ int main(int argc, char *argv[]) {
 
     char err[1024] = {0};
     lambda_host_scene *scene = nullptr;
-    if (lambda_parse_lrd(input.c_str(), &scene, err, sizeof(err)) != LAMBDA_OK) {
+    // the scene build runs on the GPU when there is one (the same scene as the host build)
+    lambda_ctx *ctx = nullptr;
+    const bool have_gpu = lambda_ctx_create(0, &ctx) == LAMBDA_OK;
+    const lambda_status parsed = have_gpu ? lambda_parse_lrd_gpu(ctx, input.c_str(), 0, &scene, err, sizeof(err))
+                                          : lambda_parse_lrd(input.c_str(), &scene, err, sizeof(err));
+    if (parsed != LAMBDA_OK) {
         std::cerr << err << std::endl;
+        if (ctx) lambda_ctx_destroy(ctx);
         return 1;
     }
     lambda_scene_desc desc;
@@ -49,8 +55,7 @@ int main(int argc, char *argv[]) {
     const int total = rd.settings.width * rd.settings.height;
     std::vector<float> image(size_t(total) * 3);
 
-    lambda_ctx *ctx = nullptr;
-    if (lambda_ctx_create(0, &ctx) != LAMBDA_OK) {
+    if (!have_gpu) {
         std::cerr << argv[0] << ": " << lambda_last_error(nullptr) << std::endl;
         lambda_host_scene_destroy(scene);
         return 1;

@@ -65,9 +65,9 @@ def test_path_kernel_fp64_thin_film(scene_dir, ctx):
 
 
 def test_path_kernel_runs_and_is_profiled(scene_dir, ctx):
-    """Below the threshold a render is three launches (init, path, finish); the stage
-    profile names the path kernel and counts its segments; above it the wavefront
-    runs."""
+    """Below the threshold a render is one persistent launch of the path kernel (it
+    seeds, traces and finishes every pixel); the stage profile names the path kernel
+    and counts its segments; above it the wavefront runs."""
     sc = CASES["cornell"](scene_dir)
     scene = lb.HostScene.parse(sc.lrd)
     ctx.upload(scene)
@@ -76,7 +76,7 @@ def test_path_kernel_runs_and_is_profiled(scene_dir, ctx):
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        48 * 48)
         ctx.render(scene.render_desc(seed=1))
-        assert ctx.stats().kernel_launches == 3
+        assert ctx.stats().kernel_launches == 1
         ctx.render(scene.render_desc(seed=1, flags=N.RENDER_PROFILE_STAGES))
         st = ctx.stage_times()
         assert st["path"]["launches"] == 1 and st["intersect"]["launches"] == 0
@@ -84,15 +84,16 @@ def test_path_kernel_runs_and_is_profiled(scene_dir, ctx):
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        48 * 48 - 1)
         ctx.render(scene.render_desc(seed=1))
-        assert ctx.stats().kernel_launches > 3
+        assert ctx.stats().kernel_launches > 1
     finally:
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        keep.path_kernel_pixels)
 
 
 def test_path_kernel_batch_equals_single_renders(scene_dir, ctx):
-    """A batch of uneven jobs (sizes, sample counts, depths) in one path-kernel pass:
-    each image equals its job rendered alone by the wavefront."""
+    """A batch of uneven jobs (sizes, sample counts, depths) in one persistent
+    path-kernel launch: each image equals its job rendered alone by the wavefront,
+    and the progress counter ends at the batch's pixel count."""
     sc = CASES["thinfilm"](scene_dir)
     scene = lb.HostScene.parse(sc.lrd)
     ctx.upload(scene)
@@ -104,8 +105,12 @@ def test_path_kernel_batch_equals_single_renders(scene_dir, ctx):
         alone = [ctx.render(d) for d in descs]
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        1 << 30)
-        batch = ctx.render_batch(descs)
-        assert ctx.stats().kernel_launches == 3
+        import ctypes
+
+        done = ctypes.c_int32(0)
+        batch = ctx.render_batch(descs, completed=ctypes.pointer(done))
+        assert ctx.stats().kernel_launches == 1
+        assert done.value == sum(d.settings.width * d.settings.height for d in descs)
     finally:
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        keep.path_kernel_pixels)
@@ -148,7 +153,7 @@ def test_surrogate_flag_without_thin_films_takes_the_path_kernel(scene_dir, ctx)
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        1 << 30)
         got = ctx.render(scene.render_desc(seed=3, flags=lb.RENDER_THINFILM_SURROGATE))
-        assert ctx.stats().kernel_launches == 3
+        assert ctx.stats().kernel_launches == 1
     finally:
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        keep.path_kernel_pixels)
@@ -170,9 +175,54 @@ def test_autotune_sets_the_path_kernel_threshold(scene_dir, ctx):
         assert t.path_kernel_pixels in (max(N.PATH_KERNEL_PIXELS, pixels), min(N.PATH_KERNEL_PIXELS, pixels - 1))
         ctx.render(probe)
         path_won = t.path_kernel_pixels >= pixels
-        assert (ctx.stats().kernel_launches == 3) == path_won
+        assert (ctx.stats().kernel_launches == 1) == path_won
         print(f"autotuned on {pixels} pixels: {'path kernel' if path_won else 'wavefront'}, "
               f"threshold {t.path_kernel_pixels}")
     finally:
         ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
                        keep.path_kernel_pixels)
+
+
+@pytest.mark.parametrize("path_kernel", [False, True])
+def test_progress_rises_while_rendering(scene_dir, ctx, path_kernel):
+    """The caller's `completed` counter (main.cpp's progress poll) rises while a render
+    runs and never falls, for a wavefront pass (waves the graph has started) and for
+    one persistent path-kernel launch (pixels its warps have finished); it ends at
+    the pixel count."""
+    import ctypes
+    import threading
+    import time
+
+    sc = scenes.thinfilm_spheres(scene_dir, 960, 540, 64, name="p_progress.lrd")
+    scene = lb.HostScene.parse(sc.lrd)
+    ctx.upload(scene)
+    keep = ctx.tuning()
+    done = ctypes.c_int32(0)
+    seen = []
+    stop = threading.Event()
+
+    def watch():
+        while not stop.is_set():
+            seen.append(done.value)
+            time.sleep(0.0002)
+
+    try:
+        ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
+                       1 << 30 if path_kernel else 0)
+        t = threading.Thread(target=watch)
+        t.start()
+        try:
+            ctx.render(scene.render_desc(seed=sc.seed), completed=ctypes.pointer(done))
+        finally:
+            stop.set()
+            t.join()
+        assert (ctx.stats().kernel_launches == 1) == path_kernel
+    finally:
+        ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
+                       keep.path_kernel_pixels)
+    seen.append(done.value)
+    assert all(a <= b for a, b in zip(seen, seen[1:])), "progress fell"
+    assert seen[-1] == 960 * 540
+    inner = sorted(set(v for v in seen if 0 < v < 960 * 540))
+    print(f"{'path kernel' if path_kernel else 'wavefront'}: {len(inner)} intermediate progress values")
+    assert len(inner) >= 2

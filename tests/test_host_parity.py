@@ -149,3 +149,21 @@ def test_obj_reader_matches_reference(tmp_path):
                 assert got.shape == want.shape and (got == want).all(), f"case {i}"
     finally:
         os.chdir(cwd)
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference harness not built")
+def test_instanced_light_list_matches_reference(tmp_path):
+    """A scene of many instances: the background light's power comes from the
+    scene-sphere merge, which passes over instances whose world box shows they change
+    nothing. The light list and its powers equal the reference's bit for bit, as do
+    the reordered instances and the nodes."""
+    from lambda_b200 import scenes
+
+    sc = scenes.instanced_meshes(str(tmp_path), 32, 18, 1, instances=300, segments=24, rings=13, box=30.0)
+    s = lb.HostScene.parse(sc.lrd)
+    r = ref.RefScene(sc.lrd)
+    assert (s.light_instances == r.light_instances).all() and (s.light_objects == r.light_objects).all()
+    assert (s.light_powers.view(np.uint32) == r.light_powers.view(np.uint32)).all()
+    assert np.float32(s.total_light_power) == np.float32(r.total_light_power)
+    assert (s.raw("instances") == r.raw("instances")).all()
+    assert (s.raw("nodes") == r.raw("nodes")).all()
