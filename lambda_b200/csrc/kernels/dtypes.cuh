@@ -99,10 +99,10 @@ struct PathState {
 
 // Counters per bounce: paths to trace, then the three material queues, then NEE rays,
 // then the thin-film hits the surrogate left to the exact transfer matrix (a count).
-// kQFetch: the next unclaimed entry of the bounce's active queue, for intersect
-// kernels whose lanes take rays one by one.
+// kQFetch / kQShadowFetch: the next unclaimed entry of the bounce's active / shadow
+// queue, for the lane-by-lane intersect and shadow kernels (lanes take rays one by one).
 enum : int { kQActive = 0, kQLambert = 1, kQSpecular = 2, kQFilm = 3, kQShadow = 4, kQFilmFallback = 5, kQFetch = 6,
-             kQueues = 7 };
+             kQShadowFetch = 7, kQueues = 8 };
 __host__ __device__ inline int queue_slot(int bounce, int q) { return bounce * kQueues + q; }
 
 }  // namespace lambda_dev

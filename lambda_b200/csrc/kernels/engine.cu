@@ -803,8 +803,11 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         tu.lane_fetch ? (bw == 2 ? k_intersect_fetch<2> : bw == 4 ? k_intersect_fetch<4> : k_intersect_fetch<8>)
                       : (bw == 2 ? k_intersect<2> : bw == 4 ? k_intersect<4> : k_intersect<8>);
     const void *f_isect = (const void *)k_isect;
-    const void *f_shadow = bw == 2 ? (const void *)k_shadow<2> : bw == 4 ? (const void *)k_shadow<4>
-                                                                         : (const void *)k_shadow<8>;
+    // shadow rays: a warp's 32 queries to the end, or (lane_fetch) taken lane by lane
+    const IntersectKernel k_shad =
+        tu.lane_fetch ? (bw == 2 ? k_shadow_fetch<2> : bw == 4 ? k_shadow_fetch<4> : k_shadow_fetch<8>)
+                      : (bw == 2 ? k_shadow<2> : bw == 4 ? k_shadow<4> : k_shadow<8>);
+    const void *f_shadow = (const void *)k_shad;
     int smem_optin = 0;
     CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
     if (stack_smem > size_t(smem_optin))
@@ -817,11 +820,7 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     const int g_isect = grid(f_isect, tb, stack_smem);
     const int g_shadow = grid(f_shadow, tb, stack_smem);
     auto intersect = [&](int b) { k_isect<<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps); };
-    auto shadow = [&](int b, cudaStream_t s) {
-        if (bw == 2) k_shadow<2><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
-        else if (bw == 4) k_shadow<4><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
-        else k_shadow<8><<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps);
-    };
+    auto shadow = [&](int b, cudaStream_t s) { k_shad<<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps); };
     const int g_lambert = grid((const void *)k_shade_lambert, sb, 0);
     const int g_spec = grid((const void *)k_shade_specular, sb, 0);
     const int g_film = grid(fp64 ? (const void *)k_shade_film_exact<true> : (const void *)k_shade_film_exact<false>, sb, 0);

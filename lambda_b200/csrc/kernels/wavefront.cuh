@@ -719,17 +719,15 @@ LAMBDA_KERNEL void __launch_bounds__(256, 3) k_shade_film_exact(int bounce, Rend
     }
 }
 
-// The NEE shadow ray of path p (renderer.h:166-173): if nothing occludes the light,
-// its emission times the stored weights is added to the path's NEE radiance.
-template <int K>
-__device__ __forceinline__ void shadow_path(const DeviceScene &sc, const PathState &ps, int p, const WideStack &st_a,
-                                            const WideStack &st_b) {
+// The end of path p's NEE shadow ray (renderer.h:166-173): if nothing occluded the
+// light, its emission (lh: the light's hit record) times the stored weights is added
+// to the path's NEE radiance.
+__device__ __forceinline__ void shadow_finish(const DeviceScene &sc, const PathState &ps, int p, bool occluded,
+                                              const Hit &lh, bool overflow) {
     const float4 o = ps.sh_o[p], dd = ps.sh_d[p];
     const int2 light = ps.sh_light[p];
     const f3 d = mk(dd.x, dd.y, dd.z);
-    Hit lh;
-    bool overflow = false;
-    if (!occluded_w<K>(sc, mk(o.x, o.y, o.z), d, light.x, light.y, lh, overflow, st_a, st_b)) {
+    if (!occluded) {
         const s4 lam = from_f4(ps.lam[p]);
         s4 e;
         if (light.x != -1) {
@@ -751,6 +749,18 @@ __device__ __forceinline__ void shadow_path(const DeviceScene &sc, const PathSta
     if (overflow) atomicOr(ps.error, 1);
 }
 
+// The NEE shadow ray of path p: occlusion, then shadow_finish.
+template <int K>
+__device__ __forceinline__ void shadow_path(const DeviceScene &sc, const PathState &ps, int p, const WideStack &st_a,
+                                            const WideStack &st_b) {
+    const float4 o = ps.sh_o[p], dd = ps.sh_d[p];
+    const int2 light = ps.sh_light[p];
+    Hit lh;
+    bool overflow = false;
+    const bool occ = occluded_w<K>(sc, mk(o.x, o.y, o.z), mk(dd.x, dd.y, dd.z), light.x, light.y, lh, overflow, st_a, st_b);
+    shadow_finish(sc, ps, p, occ, lh, overflow);
+}
+
 template <int K>
 LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
     extern __shared__ int stack_smem[];
@@ -761,6 +771,105 @@ LAMBDA_KERNEL void __launch_bounds__(256, 4) k_shadow(int bounce, RenderParams r
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += stride) {
         const int p = ps.shadow_queue[idx];
         shadow_path<K>(sc, ps, p, st_a, st_b);
+    }
+}
+
+// The bounce's shadow rays taken lane by lane (with lane_fetch), as k_intersect_fetch
+// takes closest hits: each lane keeps its occlusion query (stacks, instance-space ray,
+// light distance) across iterations of one loop and advances it by one stack entry
+// per iteration, in the order occluded_w visits them, so the answer is occluded_w's;
+// a lane whose query is done finishes it (shadow_finish) and takes the next ray from
+// the shadow queue's fetch counter at once.
+template <int K>
+LAMBDA_KERNEL void __launch_bounds__(256, 2) k_shadow_fetch(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    extern __shared__ int stack_smem[];
+    WideStack st, sub;
+    wide_stacks(stack_smem, sc, st, sub);
+    const int n = ps.counts[queue_slot(bounce, kQShadow)];
+    int *next = &ps.counts[queue_slot(bounce, kQShadowFetch)];
+    const int lane = threadIdx.x & 31;
+    int p = -1;
+    Ray3 wr, lr;
+    Hit lh;
+    int2 light = make_int2(-1, -1);
+    float best = kMax;
+    int inst = -1, sp = 0, ssp = 0;
+    bool overflow = false, occ = false;
+    for (;;) {
+        if (p < 0) {
+            const unsigned need = __activemask();
+            const int leader = __ffs(need) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(next, __popc(need));
+            base = __shfl_sync(need, base, leader);
+            const int idx = base + __popc(need & ((1u << lane) - 1u));
+            if (idx >= n) break;
+            p = ps.shadow_queue[idx];
+            const float4 o4 = ps.sh_o[p], d4 = ps.sh_d[p];
+            light = ps.sh_light[p];
+            wr = make_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
+            best = kMax;
+            sp = ssp = 0;
+            overflow = occ = false;
+            // a scene light is first intersected itself; missing it counts as occluded
+            if (light.x != -1) {
+                const InstanceRef ir = instance_ref(sc, light.x);
+                const Ray3 l0 = to_local(sc.instance_flags[light.x], ir, wr);
+                const Prim pr = load_prim(sc, light.y);
+                const float t = intersect_t(pr, l0, kMax);
+                if (t < 0) {
+                    occ = true;
+                } else {
+                    prim_attributes(sc, light.y, pr, l0.o, l0.d, t, lh);
+                    lh.instance = light.x;
+                    lh.object = light.y;
+                    to_world(sc, light.x, ir, lh);
+                    best = t;
+                }
+            }
+            float te;
+            if (!occ && slab(__ldg(&sc.nodes[0]), __ldg(&sc.nodes[1]), wr, te)) st.put(sp++, __ldg(&sc.wide_code[0]), te);
+        } else if (!occ && ssp > 0) {
+            // one BLAS entry; any primitive other than the light closer than it occludes
+            --ssp;
+            const int c2 = sub.code[ssp * sub.stride];
+            if (!(sub.te[ssp * sub.stride] > best)) {
+                if (c2 >= 0) {
+                    ssp = wide_expand<K>(sc, c2, lr, best, sub, ssp, overflow);
+                    occ = overflow;
+                } else {
+                    const int2 lf = __ldg(&sc.wide_leaves[-c2 - 1]);
+                    for (int k = 0; k < lf.y && !occ; k++) {
+                        if (light.x != -1 && inst == light.x && lf.x + k == light.y) continue;
+                        occ = intersect_t(load_prim(sc, lf.x + k), lr, best) >= 0;
+                    }
+                }
+            }
+        } else if (!occ && sp > 0) {
+            // one TLAS entry; a leaf starts its instance's BLAS (the first instance only)
+            --sp;
+            const int code = st.code[sp * st.stride];
+            float te = st.te[sp * st.stride];
+            if (!(te > best)) {
+                if (code >= 0) {
+                    sp = wide_expand<K>(sc, code, wr, best, st, sp, overflow);
+                    occ = overflow;
+                } else {
+                    inst = __ldg(&sc.wide_leaves[-code - 1]).x;
+                    const uint32_t flags = sc.instance_flags[inst];
+                    const InstanceRef ir = instance_ref(sc, inst);
+                    const int root = ir.header().z;
+                    lr = to_local(flags, ir, wr);
+                    if ((flags & 2u) ||
+                        (slab(__ldg(&sc.nodes[2 * root]), __ldg(&sc.nodes[2 * root + 1]), lr, te) && !(te > best)))
+                        sub.put(ssp++, __ldg(&sc.wide_code[root]), te);
+                }
+            }
+        } else {
+            // the query is done: occluded, or both stacks are empty
+            shadow_finish(sc, ps, p, occ, lh, overflow);
+            p = -1;
+        }
     }
 }
 
