@@ -1048,20 +1048,11 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         CK(cudaEventRecord(ctx->ev_stop, stream), "event");
         launches = 1 + s_max * wave_launches + 2;
     }
-    for (size_t k = 0; k < nj; k++) {
-        const lambda_job &j = jobs[order[first + k]];
-        if (!(j.desc.flags & LAMBDA_RENDER_OUTPUT_DEVICE))
-            CK(cudaMemcpyAsync(j.out_rgb, dj[k].out, size_t(dj[k].width) * dj[k].height * 12, cudaMemcpyDeviceToHost,
-                               stream),
-               "copy image to host");
-    }
-    unsigned long long stats[8] = {0};
-    int err[4] = {0};
-    CK(cudaMemcpyAsync(stats, ps.stats, sizeof(stats), cudaMemcpyDeviceToHost, stream), "read statistics");
-    CK(cudaMemcpyAsync(err, ps.error, sizeof(err), cudaMemcpyDeviceToHost, stream), "read flags");
     if (completed && !prof) {
         // progress from the mapped host counter: the waves the graph has started, or
-        // the pixels a path-kernel pass has finished (the largest value seen)
+        // the pixels a path-kernel pass has finished (the largest value seen). This
+        // runs before the copies below: a copy into pageable host memory returns only
+        // once the stream has drained, which would leave nothing to poll.
         int32_t seen = 0;
         for (;;) {
             const cudaError_t q = cudaStreamQuery(stream);
@@ -1075,6 +1066,17 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
             std::this_thread::sleep_for(std::chrono::milliseconds(2));
         }
     }
+    for (size_t k = 0; k < nj; k++) {
+        const lambda_job &j = jobs[order[first + k]];
+        if (!(j.desc.flags & LAMBDA_RENDER_OUTPUT_DEVICE))
+            CK(cudaMemcpyAsync(j.out_rgb, dj[k].out, size_t(dj[k].width) * dj[k].height * 12, cudaMemcpyDeviceToHost,
+                               stream),
+               "copy image to host");
+    }
+    unsigned long long stats[8] = {0};
+    int err[4] = {0};
+    CK(cudaMemcpyAsync(stats, ps.stats, sizeof(stats), cudaMemcpyDeviceToHost, stream), "read statistics");
+    CK(cudaMemcpyAsync(err, ps.error, sizeof(err), cudaMemcpyDeviceToHost, stream), "read flags");
     CK(cudaStreamSynchronize(stream), "render");
     if (prof) CK(prof->collect(), "stage timing");
     float ms = 0;
