@@ -510,6 +510,49 @@ def run_batch(args, ctx, lb, torch, rank, world, local):
     return 0
 
 
+def instanced_cpu_baseline(args, ctx, lb, torch, d, w, h, spp, flags, local) -> dict:
+    """CPU baseline of the 10,000-instance configuration on a reduced scene. The
+    reference's own scene build cannot take the full scene in usable time: its
+    Instance::center averages the transformed centres of all 100,000 triangles of an
+    instance, and makeBVH calls it for every instance three times per level
+    (scene/instance.h:94-100, scene/bvh.h:121, :149, :229). So the reference renders
+    the same configuration with --instanced-cpu instances (same mesh, box, materials,
+    camera, seed) over the full frame at a bounded spp, and the GPU renders that same
+    reduced scene too, for a like-for-like ratio. Fewer instances means fewer boxes
+    entered per ray, so the reference's rate on the reduced scene bounds its rate on
+    the full one from above, and the full-scene ratio derived from it is a lower
+    bound."""
+    from lambda_b200 import scenes
+
+    n_red = args.instanced_cpu
+    red = scenes.instanced_meshes(d, w, h, spp, instances=n_red, name="instanced_reduced.lrd")
+    rscene = lb.HostScene.parse_gpu(ctx, red.lrd)
+    ctx.upload(rscene)
+    rdesc = rscene.render_desc(seed=red.seed, flags=flags | lb.RENDER_OUTPUT_DEVICE)
+    out = torch.empty((h, w, 3), dtype=torch.float32, device=f"cuda:{local}")
+    ctx.render(rdesc, out=out)
+    g_ms = 0.0
+    for _ in range(2):
+        ctx.render(rdesc, out=out)
+        g_ms += ctx.stats().render_ms
+    gpu_value = 2 * w * h * spp / (g_ms / 1000.0)
+    t0 = time.perf_counter()
+    cb = cpu_baseline(red.lrd, red.seed, width=w, height=h, max_spp=spp)
+    wall = time.perf_counter() - t0
+    if cb is None:
+        return {"cpu_baseline": None, "cpu_baseline_note": "reference harness not built"}
+    secs = cb.pop("seconds", None)
+    cb["sample"] = (f"the configuration reduced to {n_red} of its 10,000 instances (same mesh, box, materials, camera "
+                    f"and seed): " + cb["sample"])
+    cb["extrapolation"] = ("the reference's rate on the reduced scene bounds its rate on the full scene from above "
+                           "(fewer instance boxes per ray), so value / cpu_baseline.value understates the full-scene "
+                           "speed-up")
+    return {"cpu_baseline": cb,
+            "reduced_scene": {"instances": n_red, "gpu_value": gpu_value, "cpu_value": cb["value"],
+                              "gpu_over_cpu_same_scene": gpu_value / cb["value"],
+                              "reference_parse_build_and_render_wall_s": wall, "reference_render_s": secs}}
+
+
 def run_configs(args, ctx, lb, torch, rank, world, local):
     """The plain-method configurations, one JSON line each: the Cornell box (256x256,
     depth 8, 16 spp), the 1,048,576-triangle mesh (1024x1024, depth 12, 64 spp) and
@@ -598,11 +641,8 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
                 "stage_shares": {k: round(v["share"], 4) for k, v in stage.items() if v["ms"] > 0},
                 "segments_per_path": st.segments / st.paths,
             }
-            if name == "instanced":
-                line["cpu_baseline"] = None
-                line["cpu_baseline_note"] = ("not timed: the reference's BVH build recomputes each instance's "
-                                             "center over its 100,000 triangles at every split (about 4e10 "
-                                             "point transforms), hours on the host")
+            if name == "instanced" and not args.no_cpu_baseline:
+                line.update(instanced_cpu_baseline(args, ctx, lb, torch, d, w, h, spp, flags, local))
             elif not args.no_cpu_baseline:
                 cb = cpu_baseline(sc.lrd, sc.seed, width=w, height=h, max_spp=spp)
                 if cb is not None:
@@ -639,6 +679,9 @@ def main():
                     help="--workload configs: render the Cornell and mesh configurations at RES x RES and SPP, "
                          "and the instanced one at RES x RES*9/16 and SPP, instead of their own sizes (small cases "
                          "for profiler captures)")
+    ap.add_argument("--instanced-cpu", type=int, default=50,
+                    help="instances of the reduced scene the reference's CPU renderer times for the 10,000-instance "
+                         "configuration (its own scene build is quadratic in instances x triangles)")
     ap.add_argument("--instanced-spp", type=int, default=16,
                     help="samples per pixel of the 10,000-instance scene under --workload configs (a perfect "
                          "square; its configuration asks 1024)")
