@@ -111,7 +111,14 @@ WideBvh build_wide_bvh(const lambda_bvh_node *nodes, int num_nodes, const lambda
     b.emit();
     out.stack_tlas = b.stack_need(0);
     out.stack_blas = 1;
-    for (int i = 0; i < num_instances; i++) out.stack_blas = std::max(out.stack_blas, b.stack_need(instances[i].node));
+    // one walk per distinct BLAS root: instances of one mesh share its tree
+    std::vector<char> seen(size_t(num_nodes), 0);
+    for (int i = 0; i < num_instances; i++) {
+        const int r = instances[i].node;
+        if (seen[size_t(r)]) continue;
+        seen[size_t(r)] = 1;
+        out.stack_blas = std::max(out.stack_blas, b.stack_need(r));
+    }
     return out;
 }
 

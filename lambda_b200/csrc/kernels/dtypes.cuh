@@ -69,6 +69,9 @@ struct RenderParams {
     int num_pixels;     // all jobs' pixels
     int depth_max;      // deepest job: bounces per wave are 0..depth_max
     const int *active;  // [samples_max + 1]: pixels with a sample in wave s (a prefix)
+    // the path kernel's hand-out order: (job, first work index) per job, jobs by
+    // decreasing samples x (depth + 1), so the costliest pixels are taken first
+    const int2 *work;   // [num_jobs]
 };
 
 struct PathState {

@@ -777,12 +777,26 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
             host_off += int64_t(dj[k].width) * dj[k].height;
         }
     }
+    // the path kernel's work order: jobs by decreasing samples x (depth + 1)
+    std::vector<int> by_cost(nj);
+    for (size_t k = 0; k < nj; k++) by_cost[k] = int(k);
+    std::stable_sort(by_cost.begin(), by_cost.end(), [&](int a, int b) {
+        return int64_t(dj[a].samples) * (dj[a].depth + 1) > int64_t(dj[b].samples) * (dj[b].depth + 1);
+    });
+    std::vector<int2> work(nj);
+    int64_t wbase = 0;
+    for (size_t i = 0; i < nj; i++) {
+        work[i] = make_int2(by_cost[i], int(wbase));
+        wbase += int64_t(dj[by_cost[i]].width) * dj[by_cost[i]].height;
+    }
     CK(r.jobs.reserve(nj * sizeof(Job)), "allocate job table");
     CK(r.active.reserve(active.size() * 4), "allocate job table");
+    CK(r.work.reserve(nj * sizeof(int2)), "allocate job table");
     cudaStream_t stream = ctx->stream;
     CK(cudaMemcpyAsync(r.jobs.ptr, dj.data(), nj * sizeof(Job), cudaMemcpyHostToDevice, stream), "upload job table");
     CK(cudaMemcpyAsync(r.active.ptr, active.data(), active.size() * 4, cudaMemcpyHostToDevice, stream),
        "upload job table");
+    CK(cudaMemcpyAsync(r.work.ptr, work.data(), nj * sizeof(int2), cudaMemcpyHostToDevice, stream), "upload job table");
 
     RenderParams rp{};
     rp.jobs = r.jobs.as<Job>();
@@ -790,6 +804,7 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     rp.num_pixels = P;
     rp.depth_max = d_max;
     rp.active = r.active.as<int>();
+    rp.work = r.work.as<int2>();
 
     const PathState ps = ctx->pstate;
     const lambda_tuning &tu = ctx->tuning;

@@ -52,7 +52,7 @@ struct SceneBuffers {
 
 struct RenderBuffers {
     DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, emit, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
-        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out, path_info, jobs, active, film_rows, film_out,
+        q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out, path_info, jobs, active, work, film_rows, film_out,
         film_in_domain;
 };
 
@@ -118,7 +118,7 @@ struct lambda_ctx {
                 &s.wide_code[0], &s.wide_code[1], &s.wide_code[2],
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.emit, &r.hit_p, &r.hit_n,
                 &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
-                &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &r.film_rows, &r.film_out,
+                &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &r.work, &r.film_rows, &r.film_out,
                 &r.film_in_domain, &sbuf.weights_bf16, &sbuf.weights_f32};
     }
 };

@@ -889,11 +889,11 @@ __device__ __forceinline__ void finish_pixel(const DeviceScene &sc, const PathSt
 }
 
 // A whole pass, every job of a batch included, in one persistent launch: each warp
-// takes the next 32 virtual pixels from the work counter `work` (zeroed with the
-// pass's counters) until none are left. Jobs lie end to end in order of decreasing
-// sample count, so the longest pixels are handed out first and the short ones fill
-// in behind them. Lane l runs virtual pixel base + l (a warp covers an 8x4 tile of
-// its job): it seeds the pixel (as k_init), runs every sample to the end, bounce by
+// takes the next 32 work indices from the work counter `work` (zeroed with the
+// pass's counters) until none are left. Work indices run through the jobs in the
+// order of rp.work, by decreasing samples x (depth + 1), so the costliest pixels are
+// handed out first and the cheap ones fill in behind them. Lane l runs work index
+// base + l (a warp covers an 8x4 tile of its job): it seeds the pixel (as k_init), runs every sample to the end, bounce by
 // bounce, through the same per-path steps as the wavefront kernels and in the same
 // order (bank and start a sample, closest hit, the material's shade, the NEE shadow
 // ray), then banks the last sample and writes the job's image (as k_finish). The
@@ -919,8 +919,14 @@ LAMBDA_KERNEL void __launch_bounds__(256) k_path(RenderParams rp, DeviceScene sc
         if (base >= rp.num_pixels) break;
         const int v = base + lane;
         if (v < rp.num_pixels) {
-            const Job &job = rp.jobs[job_of(rp, v)];
-            const int p = job.base + tile_order(job, v - job.base);
+            int lo = 0, hi = rp.num_jobs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (rp.work[mid].y <= v) lo = mid;
+                else hi = mid - 1;
+            }
+            const Job &job = rp.jobs[rp.work[lo].x];
+            const int p = job.base + tile_order(job, v - rp.work[lo].y);
             init_pixel(ps, p, job);
             for (int s = 0; s < job.samples; s++) {
                 bank_sample(sc, ps, p, job);
