@@ -311,9 +311,13 @@ typedef struct lambda_tuning {
                                    every sample of its pixel (same image, no launch per bounce), unless it renders
                                    thin films with the surrogate; 0: always the wavefront. Default
                                    LAMBDA_PATH_KERNEL_PIXELS */
-    int32_t lane_fetch;  /* 1: the wavefront's intersect kernel takes rays lane by lane (a lane whose ray is done takes
-                            the next at once; same hits), for scenes whose rays differ widely in traversal length;
-                            0: each warp traces 32 rays to the end before taking more */
+    int32_t lane_fetch;  /* 1: the wavefront's intersect and shadow kernels take rays lane by lane (a lane whose ray
+                            is done takes the next at once; same hits), for scenes whose rays differ widely in
+                            traversal length; 0: each warp traces 32 rays to the end before taking more */
+    int32_t compressed_nodes; /* 1: traverse the compressed node records (8-bit child boxes against a per-node origin
+                                 and power-of-two scales, checked to contain the exact boxes; a child is tested on
+                                 its exact box when popped, so the hits are the same); 0: the exact 32-byte child
+                                 records */
 } lambda_tuning;
 
 /* Default path_kernel_pixels. Below it a sample wave holds too few paths to hide a

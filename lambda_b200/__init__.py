@@ -294,8 +294,10 @@ class Context:
         return t
 
     def set_tuning(self, trace_block: int, shade_block: int, grid_scale: int = 1, max_pixels: int = 0,
-                   bvh_width: int = 4, path_kernel_pixels: int = N.PATH_KERNEL_PIXELS, lane_fetch: int = 0) -> None:
-        t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels, bvh_width, path_kernel_pixels, lane_fetch)
+                   bvh_width: int = 4, path_kernel_pixels: int = N.PATH_KERNEL_PIXELS, lane_fetch: int = 0,
+                   compressed_nodes: int = 0) -> None:
+        t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels, bvh_width, path_kernel_pixels, lane_fetch,
+                     compressed_nodes)
         self._check(self._lib.lambda_set_tuning(self._h, C.byref(t)))
 
     def tuning(self) -> N.Tuning:

@@ -118,7 +118,7 @@ class Job(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("trace_block", C.c_int32), ("shade_block", C.c_int32), ("grid_scale", C.c_int32),
                 ("max_pixels", C.c_int32), ("bvh_width", C.c_int32), ("path_kernel_pixels", C.c_int32),
-                ("lane_fetch", C.c_int32)]
+                ("lane_fetch", C.c_int32), ("compressed_nodes", C.c_int32)]
 
 
 class RenderStats(C.Structure):

@@ -2,6 +2,7 @@
 #include "wide_bvh.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <limits>
 #include <utility>
@@ -98,6 +99,78 @@ struct Builder {
     }
 };
 
+// One child bound quantized against origin o with scale s: the largest q in
+// [0, 255] whose decoded value o + q * s is <= v (lower bound), or the smallest
+// whose decoded value is >= v (upper bound); -1 when none fits.
+int quant_bound(float v, float o, float s, bool upper) {
+    const double x = (double(v) - double(o)) / double(s);
+    int q = upper ? int(std::ceil(x)) : int(std::floor(x));
+    q = std::clamp(q, 0, 255);
+    auto dec = [&](int k) { return o + float(k) * s; };  // the device's FP32 decode
+    if (upper) {
+        while (q <= 255 && !(dec(q) >= v)) q++;
+        return q <= 255 ? q : -1;
+    }
+    while (q >= 0 && !(dec(q) <= v)) q--;
+    return q;
+}
+
+// The compressed records of every wide node (see WideBvh::quant).
+void quantize(WideBvh &out, const std::vector<std::vector<int>> &children, int width) {
+    const int stride = 1 + (6 * width + 15) / 16;
+    out.quant_stride = stride;
+    const size_t W = children.size();
+    out.quant.assign(W * size_t(stride) * 4, 0u);
+    for (size_t w = 0; w < W; w++) {
+        uint32_t *q = &out.quant[w * size_t(stride) * 4];
+        const int m = int(children[w].size());
+        const float *rec = &out.records[w * size_t(width) * 8];
+        float o[3];
+        bool ok = true;
+        for (int a = 0; a < 3; a++) {
+            o[a] = std::numeric_limits<float>::infinity();
+            for (int k = 0; k < m; k++) o[a] = std::min(o[a], rec[k * 8 + a]);
+            ok = ok && std::isfinite(o[a]);
+        }
+        uint8_t bytes[6 * 8] = {0};
+        uint32_t exps = 0;
+        for (int a = 0; a < 3 && ok; a++) {
+            double span = 0;
+            for (int k = 0; k < m; k++) {
+                const float lo = rec[k * 8 + a], hi = rec[k * 8 + 4 + a];
+                ok = ok && std::isfinite(lo) && std::isfinite(hi);
+                span = std::max(span, double(hi) - double(o[a]));
+            }
+            if (!ok) break;
+            int e = 1;  // biased exponent: s = 2^(e - 127), the smallest normal power of two first
+            while (e < 254 && std::ldexp(1.0, e - 127) * 255.0 < span) e++;
+            bool fit = false;
+            for (; e < 254 && !fit; e++) {
+                const float sc = std::ldexp(1.0f, e - 127);
+                fit = true;
+                for (int k = 0; k < m && fit; k++) {
+                    const int lo = quant_bound(rec[k * 8 + a], o[a], sc, false);
+                    const int hi = quant_bound(rec[k * 8 + 4 + a], o[a], sc, true);
+                    fit = lo >= 0 && hi >= 0;
+                    if (fit) {
+                        bytes[6 * k + a] = uint8_t(lo);
+                        bytes[6 * k + 3 + a] = uint8_t(hi);
+                    }
+                }
+                if (fit) exps |= uint32_t(e) << (8 * a);
+            }
+            ok = fit;
+        }
+        uint32_t packed = exps | (uint32_t(m) << 24);
+        if (!ok) packed = (uint32_t(m) << 24) | 0x80000000u;
+        std::memcpy(&q[0], &o[0], 4);
+        std::memcpy(&q[1], &o[1], 4);
+        std::memcpy(&q[2], &o[2], 4);
+        q[3] = packed;
+        if (ok) std::memcpy(&q[4], bytes, size_t(6 * m));
+    }
+}
+
 }  // namespace
 
 WideBvh build_wide_bvh(const lambda_bvh_node *nodes, int num_nodes, const lambda_instance *instances,
@@ -109,6 +182,7 @@ WideBvh build_wide_bvh(const lambda_bvh_node *nodes, int num_nodes, const lambda
     b.code_of(0);
     for (int i = 0; i < num_instances; i++) b.code_of(instances[i].node);
     b.emit();
+    quantize(out, b.children, width);
     out.stack_tlas = b.stack_need(0);
     out.stack_blas = 1;
     // one walk per distinct BLAS root: instances of one mesh share its tree

@@ -18,6 +18,13 @@
 // distance at least the parent's. The nodes that pass are therefore visited in the
 // reference's order with the reference's culling decisions, and the primitives are
 // tested in the same order against the same best distance.
+//
+// The compressed layout (quant below) adds a conservative 8-bit box per child. A
+// traversal over it tests those boxes when it expands a node, pushes the children
+// that pass with their (lower or equal) entry distances, and at each pop tests the
+// child's exact record before it uses it: a child whose quantized test fails would
+// fail the exact test too, so the nodes expanded, their order and the culling
+// decisions are the exact layout's.
 #pragma once
 
 #include <cstdint>
@@ -38,6 +45,17 @@ struct WideBvh {
                                   // binary nodes collapsed into a wide node (only roots are looked up)
     int stack_tlas = 0;           // entries a TLAS traversal can hold at once (every child passing)
     int stack_blas = 0;           // the same for the deepest BLAS
+    // The compressed layout: per wide node `quant_stride` 16-byte words. Word 0 is
+    // the node's origin o (the least child min per axis, 3 floats) and a packed word:
+    // the biased float exponents e_x, e_y, e_z of the per-axis scales s = 2^(e - 127)
+    // in bits 0-23, the child count in bits 24-27, bit 31 set when the node could not
+    // be quantized (its children are then tested on their exact records). Then 6
+    // bytes per child: lo x y z, hi x y z. A child's quantized box is
+    // [o + lo * s, o + hi * s], computed in FP32 (one multiply, one add, no fused
+    // multiply-add) and checked here to contain the child's exact box, so it passes
+    // a ray's slab test whenever the exact box does, with an entry distance no larger.
+    std::vector<uint32_t> quant;
+    int quant_stride = 0;
 };
 
 // nodes: the binary BVH (TLAS rooted at node 0, BLAS roots given by the instances).

@@ -12,6 +12,8 @@
 // background.h and material.h, in its operand order (see dmath.cuh).
 #pragma once
 
+#include <climits>
+
 #include <cstdint>
 
 #include "dmath.cuh"
@@ -442,27 +444,126 @@ __device__ __forceinline__ void to_world(const DeviceScene &s, int inst, const I
     h.point = xform(m, h.point, 1);
 }
 
-// Expands wide node w: tests its K children (wide_bvh.h) against ray r and pushes
+// BVH layout, the template parameter L of the traversal code: the wide width (2, 4
+// or 8), plus kCompressed for the compressed node records (wide_bvh.h). With the
+// exact records a stack entry is (code, entry distance); with the compressed ones a
+// child's entry is (its record slot w * width + i, its quantized entry distance),
+// tested on its exact record when popped, and a root's entry carries its code
+// (root_entry). Both visit the same nodes in the same order (wide_bvh.h).
+constexpr int kCompressed = 16;
+template <int L>
+constexpr int kWidthOf = L & 15;
+template <int L>
+constexpr bool kQuantOf = (L & kCompressed) != 0;
+template <int L>
+constexpr int kQuantWords = 1 + (6 * kWidthOf<L> + 15) / 16;
+
+// The stack entry of a tree root (or a BLAS root) whose box test was done exactly.
+template <int L>
+__device__ __forceinline__ int root_entry(const DeviceScene &s, int code) {
+    if constexpr (kQuantOf<L>) return -1 - (code + s.num_leaves);
+    else return code;
+}
+
+// The code of a popped entry (v, te) under ray r, or INT_MIN when it is culled: its
+// distance is beyond `best`, or (compressed layout) the child's exact box is missed
+// or entered beyond `best`; te becomes the exact entry distance.
+template <int L>
+__device__ __forceinline__ int pop_code(const DeviceScene &s, int v, float &te, const Ray3 &r, float best) {
+    if (te > best) return INT_MIN;
+    if constexpr (!kQuantOf<L>) {
+        return v;
+    } else {
+        if (v < 0) return -1 - v - s.num_leaves;
+        const float4 lo = __ldg(s.wide + 2 * size_t(v)), hi = __ldg(s.wide + 2 * size_t(v) + 1);
+        if (!slab(lo, hi, r, te) || te > best) return INT_MIN;
+        return __float_as_int(lo.w);
+    }
+}
+
+// One byte of a compressed node's child bytes (words 1.. of its record).
+template <int N>
+__device__ __forceinline__ float qbyte(const uint32_t (&b)[N], int i) {
+    return float((b[i >> 2] >> (8 * (i & 3))) & 0xFFu);
+}
+
+// Expands wide node w: tests its children (wide_bvh.h) against ray r and pushes
 // the ones whose box the ray enters no farther than `best`, last-visited first, with
 // their entry distances. Returns the new stack size; sets `overflow` (and stops)
 // if the stack is full, which the stack sizes computed for the scene rule out.
-template <int K>
+// Compressed layout: the children's quantized boxes decode as o + q * s in FP32
+// (one multiply, one add, as the encoder checked them), and each child that passes
+// is pushed as its record slot.
+template <int L>
 __device__ __forceinline__ int wide_expand(const DeviceScene &s, int w, const Ray3 &r, float best, const WideStack &st,
                                            int sp, bool &overflow) {
+    constexpr int K = kWidthOf<L>;
     const float4 *c = s.wide + size_t(w) * (2 * K);
+    if constexpr (kQuantOf<L>) {
+        constexpr int QW = kQuantWords<L>;
+        const uint4 *q = s.wide_q + size_t(w) * QW;
+        const uint4 h = __ldg(q);
+        const int m = int((h.w >> 24) & 15u);
+        if (h.w & 0x80000000u) {  // not quantized: the exact records
 #pragma unroll
-    for (int i = K - 1; i >= 0; i--) {
-        const float4 lo = __ldg(c + 2 * i), hi = __ldg(c + 2 * i + 1);
-        float te;
-        if (slab(lo, hi, r, te) && !(te > best)) {
-            if (sp >= st.cap) {
-                overflow = true;
-                return sp;
+            for (int i = K - 1; i >= 0; i--) {
+                if (i >= m) continue;
+                const float4 lo = __ldg(c + 2 * i), hi = __ldg(c + 2 * i + 1);
+                float te;
+                if (slab(lo, hi, r, te) && !(te > best)) {
+                    if (sp >= st.cap) {
+                        overflow = true;
+                        return sp;
+                    }
+                    st.put(sp++, w * K + i, te);
+                }
             }
-            st.put(sp++, __float_as_int(lo.w), te);
+            return sp;
         }
+        uint32_t b[4 * (QW - 1)];
+#pragma unroll
+        for (int k = 1; k < QW; k++) {
+            const uint4 x = __ldg(q + k);
+            b[4 * (k - 1)] = x.x;
+            b[4 * (k - 1) + 1] = x.y;
+            b[4 * (k - 1) + 2] = x.z;
+            b[4 * (k - 1) + 3] = x.w;
+        }
+        const float ox = __uint_as_float(h.x), oy = __uint_as_float(h.y), oz = __uint_as_float(h.z);
+        const float sx = __uint_as_float((h.w & 0xFFu) << 23), sy = __uint_as_float(((h.w >> 8) & 0xFFu) << 23),
+                    sz = __uint_as_float(((h.w >> 16) & 0xFFu) << 23);
+#pragma unroll
+        for (int i = K - 1; i >= 0; i--) {
+            if (i >= m) continue;
+            const float4 lo = make_float4(ox + qbyte(b, 6 * i) * sx, oy + qbyte(b, 6 * i + 1) * sy,
+                                          oz + qbyte(b, 6 * i + 2) * sz, 0.0f);
+            const float4 hi = make_float4(ox + qbyte(b, 6 * i + 3) * sx, oy + qbyte(b, 6 * i + 4) * sy,
+                                          oz + qbyte(b, 6 * i + 5) * sz, 0.0f);
+            float te;
+            if (slab(lo, hi, r, te) && !(te > best)) {
+                if (sp >= st.cap) {
+                    overflow = true;
+                    return sp;
+                }
+                st.put(sp++, w * K + i, te);
+            }
+        }
+        return sp;
+    } else {
+#pragma unroll
+        for (int i = K - 1; i >= 0; i--) {
+            const float4 lo = __ldg(c + 2 * i), hi = __ldg(c + 2 * i + 1);
+            float te;
+            if (slab(lo, hi, r, te) && !(te > best)) {
+                if (sp >= st.cap) {
+                    overflow = true;
+                    return sp;
+                }
+                st.put(sp++, __float_as_int(lo.w), te);
+            }
+        }
+        return sp;
     }
-    return sp;
 }
 
 // The hit record of a finished closest-hit traversal of world ray wr: the winning
@@ -501,12 +602,12 @@ __device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, 
     int best_obj = -1, best_inst = -1;
     int sp = 0;
     float te;
-    if (slab(__ldg(&s.nodes[0]), __ldg(&s.nodes[1]), wr, te)) st.put(sp++, __ldg(&s.wide_code[0]), te);
+    if (slab(__ldg(&s.nodes[0]), __ldg(&s.nodes[1]), wr, te)) st.put(sp++, root_entry<K>(s, __ldg(&s.wide_code[0])), te);
     while (sp > 0) {
         --sp;
-        const int code = st.code[sp * st.stride];
         te = st.te[sp * st.stride];
-        if (te > best) continue;
+        const int code = pop_code<K>(s, st.code[sp * st.stride], te, wr, best);
+        if (code == INT_MIN) continue;
         if (code >= 0) {
             sp = wide_expand<K>(s, code, wr, best, st, sp, overflow);
             if (overflow) break;
@@ -521,11 +622,12 @@ __device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, 
         if (!(flags & 2u) && (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best))
             continue;
         int ssp = 0;
-        sub.put(ssp++, __ldg(&s.wide_code[root]), te);
+        sub.put(ssp++, root_entry<K>(s, __ldg(&s.wide_code[root])), te);
         while (ssp > 0) {
             --ssp;
-            const int c2 = sub.code[ssp * sub.stride];
-            if (sub.te[ssp * sub.stride] > best) continue;
+            float te2 = sub.te[ssp * sub.stride];
+            const int c2 = pop_code<K>(s, sub.code[ssp * sub.stride], te2, lr, best);
+            if (c2 == INT_MIN) continue;
             if (c2 >= 0) {
                 ssp = wide_expand<K>(s, c2, lr, best, sub, ssp, overflow);
                 if (overflow) break;
@@ -570,12 +672,12 @@ __device__ __forceinline__ bool occluded_w(const DeviceScene &s, f3 o, f3 d, int
     }
     int sp = 0;
     float te;
-    if (slab(__ldg(&s.nodes[0]), __ldg(&s.nodes[1]), wr, te)) st.put(sp++, __ldg(&s.wide_code[0]), te);
+    if (slab(__ldg(&s.nodes[0]), __ldg(&s.nodes[1]), wr, te)) st.put(sp++, root_entry<K>(s, __ldg(&s.wide_code[0])), te);
     while (sp > 0) {
         --sp;
-        const int code = st.code[sp * st.stride];
         te = st.te[sp * st.stride];
-        if (te > best) continue;
+        const int code = pop_code<K>(s, st.code[sp * st.stride], te, wr, best);
+        if (code == INT_MIN) continue;
         if (code >= 0) {
             sp = wide_expand<K>(s, code, wr, best, st, sp, overflow);
             if (overflow) return true;
@@ -589,11 +691,12 @@ __device__ __forceinline__ bool occluded_w(const DeviceScene &s, f3 o, f3 d, int
         if (!(flags & 2u) && (!slab(__ldg(&s.nodes[2 * root]), __ldg(&s.nodes[2 * root + 1]), lr, te) || te > best))
             continue;
         int ssp = 0;
-        sub.put(ssp++, __ldg(&s.wide_code[root]), te);
+        sub.put(ssp++, root_entry<K>(s, __ldg(&s.wide_code[root])), te);
         while (ssp > 0) {
             --ssp;
-            const int c2 = sub.code[ssp * sub.stride];
-            if (sub.te[ssp * sub.stride] > best) continue;
+            float te2 = sub.te[ssp * sub.stride];
+            const int c2 = pop_code<K>(s, sub.code[ssp * sub.stride], te2, lr, best);
+            if (c2 == INT_MIN) continue;
             if (c2 >= 0) {
                 ssp = wide_expand<K>(s, c2, lr, best, sub, ssp, overflow);
                 if (overflow) return true;

@@ -15,6 +15,8 @@ struct DeviceScene {
     const float4 *wide;          // wide BVH child records, `width` per node (wide_bvh.h)
     const int2 *wide_leaves;     // (index, count) of every binary leaf
     const int *wide_code;        // per binary node: wide code of the tree roots
+    const uint4 *wide_q;         // compressed node records (wide_bvh.h), kQuantWords per node
+    int num_leaves;              // binary leaves (the compressed layout's root entries encode codes with it)
     int bvh_width;               // children per wide node (2, 4 or 8)
     int stack_tlas, stack_blas;  // traversal stack entries a ray can need
     const float4 *prims;

@@ -312,12 +312,18 @@ lambda_status validate_scene(lambda_ctx *ctx, const lambda_scene_desc &d) {
 
 }  // namespace
 
+int layout_index(const lambda_tuning &t) {
+    return (t.bvh_width == 2 ? 0 : (t.bvh_width == 4 ? 1 : 2)) + (t.compressed_nodes ? 3 : 0);
+}
+
 DeviceScene lambda_ctx::scene_view(int width) const {
     const int k = width == 2 ? 0 : (width == 4 ? 1 : 2);
     DeviceScene v = dscene;
     v.wide = scene.wide[k].as<float4>();
     v.wide_leaves = scene.wide_leaves[k].as<int2>();
     v.wide_code = scene.wide_code[k].as<int>();
+    v.wide_q = scene.wide_q[k].as<uint4>();
+    v.num_leaves = wide_leaves_n[k];
     v.bvh_width = 2 << k;
     v.stack_tlas = wide_stack[k][0];
     v.stack_blas = wide_stack[k][1];
@@ -471,6 +477,8 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
         CK(b.wide[k].upload(w.records.data(), w.records.size() * sizeof(float), s), "upload wide BVH");
         CK(b.wide_leaves[k].upload(w.leaves.data(), w.leaves.size() * sizeof(int32_t), s), "upload wide BVH");
         CK(b.wide_code[k].upload(w.code.data(), w.code.size() * sizeof(int32_t), s), "upload wide BVH");
+        CK(b.wide_q[k].upload(w.quant.data(), w.quant.size() * sizeof(uint32_t), s), "upload wide BVH");
+        ctx->wide_leaves_n[k] = int(w.leaves.size() / 2);
         CK(cudaStreamSynchronize(s), "upload wide BVH");  // the host vectors go out of scope
         ctx->wide_stack[k][0] = w.stack_tlas;
         ctx->wide_stack[k][1] = w.stack_blas;
@@ -812,16 +820,16 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     const int dev = ctx->device, sms = ctx->sm_count;
     const int tb = tu.trace_block, sb = tu.shade_block, gs = tu.grid_scale, bw = tu.bvh_width;
     const size_t stack_smem = wide_stack_bytes(tb, sc.stack_tlas, sc.stack_blas);
-    // intersect: a warp traces 32 rays to the end, or (lane_fetch) lanes take rays one by one
+    // intersect: a warp traces 32 rays to the end, or (lane_fetch) lanes take rays one
+    // by one; over the tuned BVH layout (width, exact or compressed node records)
     using IntersectKernel = void (*)(int, RenderParams, DeviceScene, PathState);
-    const IntersectKernel k_isect =
-        tu.lane_fetch ? (bw == 2 ? k_intersect_fetch<2> : bw == 4 ? k_intersect_fetch<4> : k_intersect_fetch<8>)
-                      : (bw == 2 ? k_intersect<2> : bw == 4 ? k_intersect<4> : k_intersect<8>);
+    const int li = layout_index(tu);
+    static const IntersectKernel isect_fetch[6] = {k_intersect_fetch<2>, k_intersect_fetch<4>, k_intersect_fetch<8>, k_intersect_fetch<2 | kCompressed>, k_intersect_fetch<4 | kCompressed>, k_intersect_fetch<8 | kCompressed>}, isect_warp[6] = {k_intersect<2>, k_intersect<4>, k_intersect<8>, k_intersect<2 | kCompressed>, k_intersect<4 | kCompressed>, k_intersect<8 | kCompressed>};
+    const IntersectKernel k_isect = tu.lane_fetch ? isect_fetch[li] : isect_warp[li];
     const void *f_isect = (const void *)k_isect;
     // shadow rays: a warp's 32 queries to the end, or (lane_fetch) taken lane by lane
-    const IntersectKernel k_shad =
-        tu.lane_fetch ? (bw == 2 ? k_shadow_fetch<2> : bw == 4 ? k_shadow_fetch<4> : k_shadow_fetch<8>)
-                      : (bw == 2 ? k_shadow<2> : bw == 4 ? k_shadow<4> : k_shadow<8>);
+    static const IntersectKernel shad_fetch[6] = {k_shadow_fetch<2>, k_shadow_fetch<4>, k_shadow_fetch<8>, k_shadow_fetch<2 | kCompressed>, k_shadow_fetch<4 | kCompressed>, k_shadow_fetch<8 | kCompressed>}, shad_warp[6] = {k_shadow<2>, k_shadow<4>, k_shadow<8>, k_shadow<2 | kCompressed>, k_shadow<4 | kCompressed>, k_shadow<8 | kCompressed>};
+    const IntersectKernel k_shad = tu.lane_fetch ? shad_fetch[li] : shad_warp[li];
     const void *f_shadow = (const void *)k_shad;
     int smem_optin = 0;
     CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
@@ -936,8 +944,8 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         // The pass as one persistent k_path launch (it seeds, traces and finishes
         // every pixel), captured with the counter clears into one graph.
         using PathKernel = void (*)(RenderParams, DeviceScene, PathState, int *, int *, int *);
-        const PathKernel f_path = fp64 ? (bw == 2 ? k_path<2, true> : bw == 4 ? k_path<4, true> : k_path<8, true>)
-                                       : (bw == 2 ? k_path<2, false> : bw == 4 ? k_path<4, false> : k_path<8, false>);
+        static const PathKernel path64[6] = {k_path<2, true>, k_path<4, true>, k_path<8, true>, k_path<2 | kCompressed, true>, k_path<4 | kCompressed, true>, k_path<8 | kCompressed, true>}, path32[6] = {k_path<2, false>, k_path<4, false>, k_path<8, false>, k_path<2 | kCompressed, false>, k_path<4 | kCompressed, false>, k_path<8 | kCompressed, false>};
+        const PathKernel f_path = fp64 ? path64[li] : path32[li];
         CK(cudaFuncSetAttribute((const void *)f_path, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)),
            "configure kernels");
         const int g_path = grid((const void *)f_path, tb, stack_smem);
@@ -1201,7 +1209,7 @@ bool tuning_ok(const lambda_tuning &t) {
     auto block_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
     return block_ok(t.trace_block) && block_ok(t.shade_block) && (t.grid_scale == 1 || t.grid_scale == 2) &&
            t.max_pixels >= 0 && (t.bvh_width == 2 || t.bvh_width == 4 || t.bvh_width == 8) && t.path_kernel_pixels >= 0 &&
-           (t.lane_fetch == 0 || t.lane_fetch == 1);
+           (t.lane_fetch == 0 || t.lane_fetch == 1) && (t.compressed_nodes == 0 || t.compressed_nodes == 1);
 }
 
 }  // namespace
@@ -1297,7 +1305,7 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
             for (int sb : {64, 128, 256})
                 for (int gs : {1, 2}) {
                     double ms = 0;
-                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw, 0, 0}, ms);
+                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw, 0, 0, 0}, ms);
                     if (r == LAMBDA_ERR_UNSUPPORTED) continue;  // stacks too deep for shared memory at this block size
                     if (r != LAMBDA_OK) {
                         ctx->tuning = keep;
@@ -1331,7 +1339,28 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
                 }
             }
     }
-    // the path kernel at every BVH width and block size (not for surrogate renders of
+    // the compressed node records at every width, with the best shapes so far (warp
+    // or lane-by-lane traversal)
+    {
+        const lambda_tuning exact_best = best;
+        for (int bw : {2, 4, 8}) {
+            lambda_tuning t = exact_best;
+            t.bvh_width = bw;
+            t.compressed_nodes = 1;
+            double ms = 0;
+            const lambda_status r = trial(t, ms);
+            if (r == LAMBDA_ERR_UNSUPPORTED) continue;
+            if (r != LAMBDA_OK) {
+                ctx->tuning = keep;
+                return r;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
+    }
+    // the path kernel at every BVH width, node layout and block size (not for surrogate renders of
     // thin films, which it does not run). If one wins, passes up to the probe's pixels
     // use it; if the wavefront wins, only passes below the probe's size and the default
     // threshold do.
@@ -1341,10 +1370,12 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
         best.path_kernel_pixels = std::min<int32_t>(LAMBDA_PATH_KERNEL_PIXELS, probe_pixels - 1);
         const lambda_tuning wave_best = best;
         for (int bw : {2, 4, 8})
+            for (int cn : {0, 1})
             for (int tb : {64, 128, 256}) {
                 lambda_tuning t = wave_best;
                 t.trace_block = tb;
                 t.bvh_width = bw;
+                t.compressed_nodes = cn;
                 t.path_kernel_pixels = INT32_MAX;
                 double ms = 0;
                 const lambda_status r = trial(t, ms);
@@ -1432,19 +1463,17 @@ __global__ void k_trace_shadow(DeviceScene sc, const float *rays, const int *li,
     if (overflow) atomicOr(error, 1);
 }
 
-// Launches a ray-query kernel of the tuned BVH width with its stacks in shared memory.
-template <class F2, class F4, class F8, class... A>
-cudaError_t launch_query(lambda_ctx *ctx, F2 f2, F4 f4, F8 f8, int n, A... args) {
+// Launches a ray-query kernel (fns: one per BVH layout, in layout_index order) of the
+// tuned layout with its stacks in shared memory.
+template <class... A>
+cudaError_t launch_query(lambda_ctx *ctx, void (*const *fns)(DeviceScene, A...), int n, A... args) {
     const DeviceScene sc = ctx->scene_view(ctx->tuning.bvh_width);
     const size_t smem = wide_stack_bytes(128, sc.stack_tlas, sc.stack_blas);
-    const int w = sc.bvh_width;
-    const void *fn = w == 2 ? (const void *)f2 : w == 4 ? (const void *)f4 : (const void *)f8;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    void (*fn)(DeviceScene, A...) = fns[layout_index(ctx->tuning)];
+    cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     const int blocks = (n + 127) / 128;
-    if (w == 2) f2<<<blocks, 128, smem, ctx->stream>>>(sc, args...);
-    else if (w == 4) f4<<<blocks, 128, smem, ctx->stream>>>(sc, args...);
-    else f8<<<blocks, 128, smem, ctx->stream>>>(sc, args...);
+    fn<<<blocks, 128, smem, ctx->stream>>>(sc, args...);
     return cudaGetLastError();
 }
 
@@ -1475,8 +1504,8 @@ extern "C" lambda_status lambda_trace_closest(lambda_ctx *ctx, const float *rays
     CK(ctx->rbuf.error.reserve(16), "allocate flags");
     int *err = ctx->rbuf.error.as<int>();
     CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
-    CK(launch_query(ctx, k_trace_closest<2>, k_trace_closest<4>, k_trace_closest<8>, n, static_cast<const float *>(dr), n,
-                    di, dobj, dt, err),
+    static void (*const closest[6])(DeviceScene, const float *, int, int *, int *, float *, int *) = {k_trace_closest<2>, k_trace_closest<4>, k_trace_closest<8>, k_trace_closest<2 | kCompressed>, k_trace_closest<4 | kCompressed>, k_trace_closest<8 | kCompressed>};
+    CK(launch_query(ctx, closest, n, static_cast<const float *>(dr), n, di, dobj, dt, err),
        "launch closest-hit queries");
     CK(cudaGetLastError(), "launch trace");
     int herr = 0;
@@ -1517,8 +1546,10 @@ extern "C" lambda_status lambda_trace_shadow(lambda_ctx *ctx, const float *rays,
     CK(ctx->rbuf.error.reserve(16), "allocate flags");
     int *err = ctx->rbuf.error.as<int>();
     CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
-    CK(launch_query(ctx, k_trace_shadow<2>, k_trace_shadow<4>, k_trace_shadow<8>, n, static_cast<const float *>(dr),
-                    static_cast<const int *>(dli), static_cast<const int *>(dlo), n, docc, err),
+    static void (*const shadow[6])(DeviceScene, const float *, const int *, const int *, int, int *, int *) =
+        {k_trace_shadow<2>, k_trace_shadow<4>, k_trace_shadow<8>, k_trace_shadow<2 | kCompressed>, k_trace_shadow<4 | kCompressed>, k_trace_shadow<8 | kCompressed>};
+    CK(launch_query(ctx, shadow, n, static_cast<const float *>(dr), static_cast<const int *>(dli),
+                    static_cast<const int *>(dlo), n, docc, err),
        "launch shadow queries");
     CK(cudaGetLastError(), "launch trace");
     int herr = 0;

@@ -21,6 +21,10 @@ struct DeviceBuffer {
 
 bool is_device_pointer(const void *p);
 
+// Index of the tuned BVH layout: widths 2, 4, 8 (0-2), then the same widths with
+// compressed node records (3-5); the order of the kernel tables that dispatch on it.
+int layout_index(const lambda_tuning &t);
+
 // CTAs of `block` threads with `dyn_smem` bytes of dynamic shared memory that one SM
 // holds at once, from the kernel's registers and static shared memory and the SM's
 // limits (at least 1).
@@ -48,6 +52,7 @@ struct SceneBuffers {
         material_uv,
         cie, perm, worley, instance_flags;
     DeviceBuffer wide[3], wide_leaves[3], wide_code[3];  // wide BVH of width 2, 4, 8
+    DeviceBuffer wide_q[3];                               // its compressed node records
 };
 
 struct RenderBuffers {
@@ -78,13 +83,14 @@ struct lambda_ctx {
     SceneBuffers scene;
     lambda_dev::DeviceScene dscene{};
     int wide_stack[3][2] = {};  // traversal stack entries (TLAS, BLAS) of the width 2, 4, 8 trees
+    int wide_leaves_n[3] = {};  // binary leaves of each (codes of the compressed layout's root entries)
 
     RenderBuffers rbuf;
     lambda_dev::PathState pstate{};
     cudaGraphExec_t graph_exec = nullptr;
     lambda_render_stats stats{};
     lambda_stage_time stage_times[LAMBDA_NUM_STAGES]{};
-    lambda_tuning tuning{256, 256, 1, 0, 4, LAMBDA_PATH_KERNEL_PIXELS, 0};  // launch shapes (max_pixels 0: no limit)
+    lambda_tuning tuning{256, 256, 1, 0, 4, LAMBDA_PATH_KERNEL_PIXELS, 0, 0};  // launch shapes (max_pixels 0: no limit)
     lambda_limits limits{LAMBDA_DEFAULT_MMA_POLLS, 0};  // device guard limits (lambda_set_limits)
     int *progress_host = nullptr;           // waves started by the running pass graph (mapped host memory)
     int *progress_dev = nullptr;            // its device address
@@ -115,7 +121,7 @@ struct lambda_ctx {
                 &s.cspectrum_flat, &s.materials, &s.material_props, &s.scalar_tex, &s.spectrum_tex, &s.light_inst,
                 &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.material_uv, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &s.wide[0], &s.wide[1], &s.wide[2], &s.wide_leaves[0], &s.wide_leaves[1], &s.wide_leaves[2],
-                &s.wide_code[0], &s.wide_code[1], &s.wide_code[2],
+                &s.wide_code[0], &s.wide_code[1], &s.wide_code[2], &s.wide_q[0], &s.wide_q[1], &s.wide_q[2],
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.emit, &r.hit_p, &r.hit_n,
                 &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
                 &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &r.work, &r.film_rows, &r.film_out,

@@ -333,12 +333,14 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_intersect_fetch(int bounce, Rende
             sp = ssp = 0;
             overflow = false;
             float te;
-            if (slab(__ldg(&sc.nodes[0]), __ldg(&sc.nodes[1]), wr, te)) st.put(sp++, __ldg(&sc.wide_code[0]), te);
+            if (slab(__ldg(&sc.nodes[0]), __ldg(&sc.nodes[1]), wr, te))
+                st.put(sp++, root_entry<K>(sc, __ldg(&sc.wide_code[0])), te);
         } else if (ssp > 0 && !overflow) {
             // one BLAS entry
             --ssp;
-            const int c2 = sub.code[ssp * sub.stride];
-            if (!(sub.te[ssp * sub.stride] > best)) {
+            float te2 = sub.te[ssp * sub.stride];
+            const int c2 = pop_code<K>(sc, sub.code[ssp * sub.stride], te2, lr, best);
+            if (c2 != INT_MIN) {
                 if (c2 >= 0) {
                     ssp = wide_expand<K>(sc, c2, lr, best, sub, ssp, overflow);
                 } else {
@@ -356,9 +358,9 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_intersect_fetch(int bounce, Rende
         } else if (sp > 0 && !overflow) {
             // one TLAS entry; a leaf starts its instance's BLAS (the first instance only)
             --sp;
-            const int code = st.code[sp * st.stride];
             float te = st.te[sp * st.stride];
-            if (!(te > best)) {
+            const int code = pop_code<K>(sc, st.code[sp * st.stride], te, wr, best);
+            if (code != INT_MIN) {
                 if (code >= 0) {
                     sp = wide_expand<K>(sc, code, wr, best, st, sp, overflow);
                 } else {
@@ -369,7 +371,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_intersect_fetch(int bounce, Rende
                     lr = to_local(flags, ir, wr);
                     if ((flags & 2u) ||
                         (slab(__ldg(&sc.nodes[2 * root]), __ldg(&sc.nodes[2 * root + 1]), lr, te) && !(te > best)))
-                        sub.put(ssp++, __ldg(&sc.wide_code[root]), te);
+                        sub.put(ssp++, root_entry<K>(sc, __ldg(&sc.wide_code[root])), te);
                 }
             }
         } else {
@@ -828,12 +830,14 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_shadow_fetch(int bounce, RenderPa
                 }
             }
             float te;
-            if (!occ && slab(__ldg(&sc.nodes[0]), __ldg(&sc.nodes[1]), wr, te)) st.put(sp++, __ldg(&sc.wide_code[0]), te);
+            if (!occ && slab(__ldg(&sc.nodes[0]), __ldg(&sc.nodes[1]), wr, te))
+                st.put(sp++, root_entry<K>(sc, __ldg(&sc.wide_code[0])), te);
         } else if (!occ && ssp > 0) {
             // one BLAS entry; any primitive other than the light closer than it occludes
             --ssp;
-            const int c2 = sub.code[ssp * sub.stride];
-            if (!(sub.te[ssp * sub.stride] > best)) {
+            float te2 = sub.te[ssp * sub.stride];
+            const int c2 = pop_code<K>(sc, sub.code[ssp * sub.stride], te2, lr, best);
+            if (c2 != INT_MIN) {
                 if (c2 >= 0) {
                     ssp = wide_expand<K>(sc, c2, lr, best, sub, ssp, overflow);
                     occ = overflow;
@@ -848,9 +852,9 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_shadow_fetch(int bounce, RenderPa
         } else if (!occ && sp > 0) {
             // one TLAS entry; a leaf starts its instance's BLAS (the first instance only)
             --sp;
-            const int code = st.code[sp * st.stride];
             float te = st.te[sp * st.stride];
-            if (!(te > best)) {
+            const int code = pop_code<K>(sc, st.code[sp * st.stride], te, wr, best);
+            if (code != INT_MIN) {
                 if (code >= 0) {
                     sp = wide_expand<K>(sc, code, wr, best, st, sp, overflow);
                     occ = overflow;
@@ -862,7 +866,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_shadow_fetch(int bounce, RenderPa
                     lr = to_local(flags, ir, wr);
                     if ((flags & 2u) ||
                         (slab(__ldg(&sc.nodes[2 * root]), __ldg(&sc.nodes[2 * root + 1]), lr, te) && !(te > best)))
-                        sub.put(ssp++, __ldg(&sc.wide_code[root]), te);
+                        sub.put(ssp++, root_entry<K>(sc, __ldg(&sc.wide_code[root])), te);
                 }
             }
         } else {

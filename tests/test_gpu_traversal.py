@@ -66,12 +66,16 @@ def _oracle_hit(sc, scene, rays):
     return port.hit(scene, rays)
 
 
-@pytest.fixture(params=[2, 4, 8])
+@pytest.fixture(params=["2", "4", "8", "2c", "4c", "8c"])
 def width(request, ctx):
+    """BVH width, and "c" for the compressed node records."""
     keep = ctx.tuning()
-    ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, request.param)
+    w, compressed = int(request.param[0]), int(request.param.endswith("c"))
+    ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, w,
+                   keep.path_kernel_pixels, keep.lane_fetch, compressed)
     yield request.param
-    ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width)
+    ctx.set_tuning(keep.trace_block, keep.shade_block, keep.grid_scale, keep.max_pixels, keep.bvh_width,
+                   keep.path_kernel_pixels, keep.lane_fetch, keep.compressed_nodes)
 
 
 def test_closest_hit_ids_bit_exact(loaded, width, ctx):
