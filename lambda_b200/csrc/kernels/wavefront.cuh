@@ -909,7 +909,7 @@ __device__ __forceinline__ void finish_pixel(const DeviceScene &sc, const PathSt
 // wavefront, which batches a bounce's thin-film hits for the tensor cores. The
 // statistics are the ones the wave prologue keeps from the queue sizes.
 template <int K, bool kFp64>
-LAMBDA_KERNEL void __launch_bounds__(256) k_path(RenderParams rp, DeviceScene sc, PathState ps, int *work, int *done,
+LAMBDA_KERNEL void __launch_bounds__(256, 3) k_path(RenderParams rp, DeviceScene sc, PathState ps, int *work, int *done,
                                                  int *progress) {
     extern __shared__ int stack_smem[];
     WideStack st_a, st_b;
