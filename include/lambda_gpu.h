@@ -320,6 +320,9 @@ typedef struct lambda_tuning {
                                  and power-of-two scales, checked to contain the exact boxes; a child is tested on
                                  its exact box when popped, so the hits are the same); 0: the exact 32-byte child
                                  records */
+    int32_t fused_bounce; /* 1: a wavefront bounce runs as one kernel (closest hit, the material's shade and the NEE
+                             shadow ray of each path; same image), for frames whose bounces are too short to repay
+                             a chain of launches; not for surrogate renders of thin films. 0: separate kernels */
 } lambda_tuning;
 
 /* Default path_kernel_pixels. Below it a sample wave holds too few paths to hide a
@@ -382,10 +385,11 @@ lambda_status lambda_get_render_stats(const lambda_ctx *ctx, lambda_render_stats
  * 9-11 thin-film shade with the surrogate: 9 the hits' queries encoded as MLP rows,
  * 10 the tensor-core MLP, 11 the scatter (with the exact transfer matrix for hits
  * outside the surrogate's domain), 12 the path kernel of small passes (every sample
- * and bounce of a pixel in one thread; items = segments). items = paths, rays or hits
- * the stage processed over the whole render. No reference counterpart (the
- * reference's single kernel has no stages). */
-#define LAMBDA_NUM_STAGES 13
+ * and bounce of a pixel in one thread; items = segments), 13 the fused bounce kernel
+ * (tuning.fused_bounce: a bounce's intersect, shade and shadow rays in one launch;
+ * items = segments). items = paths, rays or hits the stage processed over the whole
+ * render. No reference counterpart (the reference's single kernel has no stages). */
+#define LAMBDA_NUM_STAGES 14
 typedef struct lambda_stage_time {
     double ms;
     int64_t launches;

@@ -295,9 +295,9 @@ class Context:
 
     def set_tuning(self, trace_block: int, shade_block: int, grid_scale: int = 1, max_pixels: int = 0,
                    bvh_width: int = 4, path_kernel_pixels: int = N.PATH_KERNEL_PIXELS, lane_fetch: int = 0,
-                   compressed_nodes: int = 0) -> None:
+                   compressed_nodes: int = 0, fused_bounce: int = 0) -> None:
         t = N.Tuning(trace_block, shade_block, grid_scale, max_pixels, bvh_width, path_kernel_pixels, lane_fetch,
-                     compressed_nodes)
+                     compressed_nodes, fused_bounce)
         self._check(self._lib.lambda_set_tuning(self._h, C.byref(t)))
 
     def tuning(self) -> N.Tuning:
@@ -444,6 +444,8 @@ STAGE_BYTES = {
     # per segment: the ray and hit state of intersect plus a scatter's reads and writes
     # (the path kernel keeps a pixel's state in one thread, mostly in L1/L2)
     "path": 4 + 32 + 48 + 4 + 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
+    # the fused bounce kernel: the same per-segment reads and writes as the path kernel
+    "bounce": 4 + 32 + 48 + 4 + 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
 }
 
 

@@ -37,14 +37,14 @@ RENDER_THINFILM_SURROGATE = 1
 RENDER_OUTPUT_DEVICE = 2
 RENDER_PROFILE_STAGES = 4
 RENDER_THINFILM_FP64 = 8
-NUM_STAGES = 13
+NUM_STAGES = 14
 PATH_KERNEL_PIXELS = 32768  # LAMBDA_PATH_KERNEL_PIXELS
 # the surrogate's grazing region, where renders take the exact transfer matrix
 SURROGATE_GRAZING_COS = 0.05  # LAMBDA_SURROGATE_GRAZING_COS
 SURROGATE_LOW_SUB_INDEX = 1.05  # LAMBDA_SURROGATE_LOW_SUB_INDEX
 SURROGATE_LOW_SUB_COS = 0.2  # LAMBDA_SURROGATE_LOW_SUB_COS
 STAGE_NAMES = ("init", "wave_prologue", "raygen", "intersect", "shade_lambert", "shade_specular", "shade_film",
-               "shadow", "finish", "film_encode", "film_mlp", "film_scatter", "path")
+               "shadow", "finish", "film_encode", "film_mlp", "film_scatter", "path", "bounce")
 
 
 class LambdaError(RuntimeError):
@@ -118,7 +118,7 @@ class Job(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("trace_block", C.c_int32), ("shade_block", C.c_int32), ("grid_scale", C.c_int32),
                 ("max_pixels", C.c_int32), ("bvh_width", C.c_int32), ("path_kernel_pixels", C.c_int32),
-                ("lane_fetch", C.c_int32), ("compressed_nodes", C.c_int32)]
+                ("lane_fetch", C.c_int32), ("compressed_nodes", C.c_int32), ("fused_bounce", C.c_int32)]
 
 
 class RenderStats(C.Structure):

@@ -831,17 +831,25 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     static const IntersectKernel shad_fetch[6] = {k_shadow_fetch<2>, k_shadow_fetch<4>, k_shadow_fetch<8>, k_shadow_fetch<2 | kCompressed>, k_shadow_fetch<4 | kCompressed>, k_shadow_fetch<8 | kCompressed>}, shad_warp[6] = {k_shadow<2>, k_shadow<4>, k_shadow<8>, k_shadow<2 | kCompressed>, k_shadow<4 | kCompressed>, k_shadow<8 | kCompressed>};
     const IntersectKernel k_shad = tu.lane_fetch ? shad_fetch[li] : shad_warp[li];
     const void *f_shadow = (const void *)k_shad;
+    // fused_bounce: one kernel per bounce (closest hit, shade, shadow ray)
+    static const IntersectKernel bounce64[6] = {k_bounce<2, true>, k_bounce<4, true>, k_bounce<8, true>, k_bounce<2 | kCompressed, true>, k_bounce<4 | kCompressed, true>, k_bounce<8 | kCompressed, true>}, bounce32[6] = {k_bounce<2, false>, k_bounce<4, false>, k_bounce<8, false>, k_bounce<2 | kCompressed, false>, k_bounce<4 | kCompressed, false>, k_bounce<8 | kCompressed, false>};
+    const bool fused = tu.fused_bounce != 0 && !surrogate;
+    const IntersectKernel k_bnc = fp64 ? bounce64[li] : bounce32[li];
     int smem_optin = 0;
     CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
     if (stack_smem > size_t(smem_optin))
         return ctx->fail(LAMBDA_ERR_UNSUPPORTED, "the scene's traversal stacks exceed shared memory at this block size");
     CK(cudaFuncSetAttribute(f_isect, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)), "configure kernels");
     CK(cudaFuncSetAttribute(f_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)), "configure kernels");
+    if (fused)
+        CK(cudaFuncSetAttribute((const void *)k_bnc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stack_smem)),
+           "configure kernels");
     auto grid = [&](const void *fn, int block, size_t smem) {
         return std::max(1, std::min((P + block - 1) / block, resident_ctas(fn, dev, block, smem) * sms * gs));
     };
     const int g_isect = grid(f_isect, tb, stack_smem);
     const int g_shadow = grid(f_shadow, tb, stack_smem);
+    const int g_bounce = fused ? grid((const void *)k_bnc, tb, stack_smem) : 1;
     auto intersect = [&](int b) { k_isect<<<g_isect, tb, stack_smem, stream>>>(b, rp, sc, ps); };
     auto shadow = [&](int b, cudaStream_t s) { k_shad<<<g_shadow, tb, stack_smem, s>>>(b, rp, sc, ps); };
     const int g_lambert = grid((const void *)k_shade_lambert, sb, 0);
@@ -889,6 +897,10 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
         auto keep = [&](cudaError_t e) {
             if (fork_err == cudaSuccess) fork_err = e;
         };
+        if (fused) {
+            for (int b = 0; b <= d_max; b++) timed(13, [&] { k_bnc<<<g_bounce, tb, stack_smem, stream>>>(b, rp, sc, ps); });
+            return n;
+        }
         cudaStream_t shadow_stream = ctx->side[2];
         bool shadow_pending = false;
         for (int b = 0; b <= d_max; b++) {
@@ -1193,6 +1205,7 @@ lambda_status render_jobs(lambda_ctx *ctx, const lambda_job *jobs, int n, volati
         ctx->stage_times[2].items = tot.paths;
         ctx->stage_times[3].items = prof.counts[3] ? ctx->stats.segments : 0;
         ctx->stage_times[12].items = prof.counts[12] ? ctx->stats.segments : 0;
+        ctx->stage_times[13].items = prof.counts[13] ? ctx->stats.segments : 0;
         ctx->stage_times[4].items = int64_t(tot.stats[4]);
         ctx->stage_times[5].items = int64_t(tot.stats[5]);
         ctx->stage_times[6].items = surrogate ? 0 : ctx->stats.thinfilm_hits;
@@ -1209,7 +1222,8 @@ bool tuning_ok(const lambda_tuning &t) {
     auto block_ok = [](int b) { return b == 64 || b == 128 || b == 256; };
     return block_ok(t.trace_block) && block_ok(t.shade_block) && (t.grid_scale == 1 || t.grid_scale == 2) &&
            t.max_pixels >= 0 && (t.bvh_width == 2 || t.bvh_width == 4 || t.bvh_width == 8) && t.path_kernel_pixels >= 0 &&
-           (t.lane_fetch == 0 || t.lane_fetch == 1) && (t.compressed_nodes == 0 || t.compressed_nodes == 1);
+           (t.lane_fetch == 0 || t.lane_fetch == 1) && (t.compressed_nodes == 0 || t.compressed_nodes == 1) &&
+           (t.fused_bounce == 0 || t.fused_bounce == 1);
 }
 
 }  // namespace
@@ -1305,7 +1319,7 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
             for (int sb : {64, 128, 256})
                 for (int gs : {1, 2}) {
                     double ms = 0;
-                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw, 0, 0, 0}, ms);
+                    const lambda_status r = trial(lambda_tuning{tb, sb, gs, keep.max_pixels, bw, 0, 0, 0, 0}, ms);
                     if (r == LAMBDA_ERR_UNSUPPORTED) continue;  // stacks too deep for shared memory at this block size
                     if (r != LAMBDA_OK) {
                         ctx->tuning = keep;
@@ -1359,6 +1373,30 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
                 best = t;
             }
         }
+    }
+    // one kernel per bounce at every width and traversal block, with the best shapes so
+    // far (not for surrogate renders of thin films, which keep the batched MLP stage)
+    if (!(probes[0].flags & LAMBDA_RENDER_THINFILM_SURROGATE) || !(ctx->dscene.families & (1u << 2))) {
+        const lambda_tuning sep_best = best;
+        for (int bw : {2, 4, 8})
+            for (int tb : {64, 128, 256}) {
+                lambda_tuning t = sep_best;
+                t.trace_block = tb;
+                t.bvh_width = bw;
+                t.lane_fetch = 0;
+                t.fused_bounce = 1;
+                double ms = 0;
+                const lambda_status r = trial(t, ms);
+                if (r == LAMBDA_ERR_UNSUPPORTED) continue;
+                if (r != LAMBDA_OK) {
+                    ctx->tuning = keep;
+                    return r;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
+            }
     }
     // the path kernel at every BVH width, node layout and block size (not for surrogate renders of
     // thin films, which it does not run). If one wins, passes up to the probe's pixels

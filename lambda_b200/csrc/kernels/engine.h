@@ -90,7 +90,7 @@ struct lambda_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     lambda_render_stats stats{};
     lambda_stage_time stage_times[LAMBDA_NUM_STAGES]{};
-    lambda_tuning tuning{256, 256, 1, 0, 4, LAMBDA_PATH_KERNEL_PIXELS, 0, 0};  // launch shapes (max_pixels 0: no limit)
+    lambda_tuning tuning{256, 256, 1, 0, 4, LAMBDA_PATH_KERNEL_PIXELS, 0, 0, 0};  // launch shapes (max_pixels 0: no limit)
     lambda_limits limits{LAMBDA_DEFAULT_MMA_POLLS, 0};  // device guard limits (lambda_set_limits)
     int *progress_host = nullptr;           // waves started by the running pass graph (mapped host memory)
     int *progress_dev = nullptr;            // its device address

@@ -877,6 +877,46 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_shadow_fetch(int bounce, RenderPa
     }
 }
 
+// One bounce of every active path in one kernel (tuning.fused_bounce): its closest
+// hit, its material's shade and, for a Lambertian hit, its NEE shadow ray, through
+// the same per-path steps as the path kernel and in the same order, so the image is
+// the wavefront's. A wave is then raygen and one launch per bounce instead of four
+// or more, which pays where a bounce's kernels are short and their chain of
+// launches is the cost (small frames). The material and shadow counters are raised
+// as the separate kernels' pushes raise them, for the statistics; those queues
+// themselves stay empty.
+template <int K, bool kFp64>
+LAMBDA_KERNEL void __launch_bounds__(256, 3) k_bounce(int bounce, RenderParams rp, DeviceScene sc, PathState ps) {
+    extern __shared__ int stack_smem[];
+    WideStack st_a, st_b;
+    wide_stacks(stack_smem, sc, st_a, st_b);
+    const int n = ps.counts[queue_slot(bounce, kQActive)];
+    const int *q = ps.queue[bounce & 1];
+    int *q_next = ps.queue[(bounce + 1) & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int idx = base + threadIdx.x;
+        int p = 0, family = -1;
+        bool alive = false, nee = false;
+        if (idx < n) {
+            p = q[idx];
+            family = trace_path<K>(sc, ps, p, st_a, st_b);
+            if (family == 0) {
+                alive = lambert_path(sc, ps, p, bounce, nee);
+                if (nee) shadow_path<K>(sc, ps, p, st_a, st_b);
+            } else if (family == 1) {
+                alive = specular_path(sc, ps, p, bounce);
+            } else if (family == 2) {
+                alive = film_path<kFp64>(sc, ps, p, bounce);
+            }
+        }
+        const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);
+        if (alive) q_next[slot] = p;
+        for (int f = 0; f < 3; f++) warp_push(&ps.counts[queue_slot(bounce, kQLambert + f)], family == f);
+        warp_push(&ps.counts[queue_slot(bounce, kQShadow)], nee);
+    }
+}
+
 // Last sample of pixel p into the film, then the average (renderer.h:84-91), into
 // the job's own image.
 __device__ __forceinline__ void finish_pixel(const DeviceScene &sc, const PathState &ps, int p, const Job &job) {
