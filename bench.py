@@ -499,7 +499,8 @@ def run_batch(args, ctx, lb, torch, rank, world, local):
                        "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
                                   "grid_scale": tuning.grid_scale, "max_pixels": tuning.max_pixels,
                                   "bvh_width": tuning.bvh_width, "lane_fetch": tuning.lane_fetch,
-                                  "compressed_nodes": tuning.compressed_nodes, "path_kernel_pixels": tuning.path_kernel_pixels, "source": tuning_source}},
+                                  "compressed_nodes": tuning.compressed_nodes, "fused_bounce": tuning.fused_bounce,
+                                  "path_kernel_pixels": tuning.path_kernel_pixels, "source": tuning_source}},
             "e2e": {"value": world * paths * args.steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": len(hdescs) * C.sizeof(N.Job), "scene": "resident",
                     "d2h_bytes_per_step": sum(d.settings.width * d.settings.height * 12 for d in descs)},
@@ -634,7 +635,8 @@ def run_configs(args, ctx, lb, torch, rank, world, local):
                            "large BVH builds on the GPU)", "upload_s": upload_s,
                            "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
                                       "grid_scale": tuning.grid_scale, "bvh_width": tuning.bvh_width, "lane_fetch": tuning.lane_fetch,
-                                  "compressed_nodes": tuning.compressed_nodes, "path_kernel_pixels": tuning.path_kernel_pixels,
+                                  "compressed_nodes": tuning.compressed_nodes, "fused_bounce": tuning.fused_bounce,
+                                  "path_kernel_pixels": tuning.path_kernel_pixels,
                                       "source": tuning_source}},
                 "e2e": {"value": world * paths * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": w * h * 12, "scene": "resident"},
@@ -666,11 +668,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=SPP)
     ap.add_argument("--no-compare", action="store_true", help="skip the surrogate/exact comparison")
-    ap.add_argument("--tuning", default="", metavar="TB,SB,GS,WIDTH[,PATH_PIXELS[,LANE_FETCH[,COMPRESSED]]]",
+    ap.add_argument("--tuning", default="",
+                    metavar="TB,SB,GS,WIDTH[,PATH_PIXELS[,LANE_FETCH[,COMPRESSED[,FUSED_BOUNCE]]]]",
                     help="fixed launch shapes (trace block, shade block, grid scale, BVH width, the largest pass "
                          "the path kernel runs, 1 for the lane-by-lane intersect and shadow rays, 1 for the "
-                         "compressed BVH node records) instead of the autotuner's, e.g. for reproducible profiler "
-                         "captures")
+                         "compressed BVH node records, 1 for one kernel per bounce) instead of the autotuner's, "
+                         "e.g. for reproducible profiler captures")
     ap.add_argument("--workload", default="thinfilm1080p",
                     choices=["thinfilm1080p", "batch32", "film_queries", "configs"],
                     help="batch32: 32 random-pose views of the 1M-triangle mesh scene in one batched render; "
@@ -849,7 +852,8 @@ def main():
                        "paths_per_step": paths_per_step,
                        "tuning": {"trace_block": tuning.trace_block, "shade_block": tuning.shade_block,
                                   "grid_scale": tuning.grid_scale, "bvh_width": tuning.bvh_width, "lane_fetch": tuning.lane_fetch,
-                                  "compressed_nodes": tuning.compressed_nodes, "path_kernel_pixels": tuning.path_kernel_pixels,
+                                  "compressed_nodes": tuning.compressed_nodes, "fused_bounce": tuning.fused_bounce,
+                                  "path_kernel_pixels": tuning.path_kernel_pixels,
                                   "source": tuning_source}},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 12},
