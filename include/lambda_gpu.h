@@ -204,9 +204,9 @@ lambda_status lambda_parse_lrd(const char *path, lambda_host_scene **out, char *
  * of every instance) and the binned-SAH build (src/scene/bvh.h:111-246) of every
  * object group or instance set of at least gpu_min_items items (0: 65536; smaller
  * ones build faster on the host). Errors as lambda_parse_lrd's, plus
- * LAMBDA_ERR_CUDA. The build takes temporary device memory of about 2.6 KB per
- * item of the largest range it builds (its per-node bins; 2.7 GB for the
- * 1,048,576-triangle mesh) and frees it before returning. Declared with the host functions because it returns a host
+ * LAMBDA_ERR_CUDA. The build takes temporary device memory of about 260 bytes per
+ * item of the largest range it builds plus about 175 MB (the per-node bins of up
+ * to 65,536 nodes at a time), and frees it before returning. Declared with the host functions because it returns a host
  * scene; it needs a GPU. No reference counterpart: the reference builds on the
  * host only. */
 typedef struct lambda_ctx lambda_ctx;

@@ -682,17 +682,19 @@ void gpu_build(lambda_ctx *ctx, const std::vector<float> &items9, std::vector<in
     int *prefix = sc.get<int>(size_t(n) + 1);
     int *fail_pos = sc.get<int>(size_t(n));
     int *pass_pos = sc.get<int>(size_t(n));
-    // per task of a level: at most n tasks
+    // a level's tasks (at most n), processed in chunks of at most `cap` tasks: the
+    // per-task keys, boxes and bins (about 2.6 KB a task) are sized for one chunk
     const size_t max_tasks = size_t(n);
+    const size_t cap = std::min<size_t>(max_tasks, size_t(1) << 16);
     Task *tasks = sc.get<Task>(max_tasks);
     Task *next = sc.get<Task>(max_tasks);
-    auto *keys = sc.get<unsigned long long>(max_tasks * kTaskKeys);
-    TaskBox *boxes = sc.get<TaskBox>(max_tasks);
-    auto *bin_keys = sc.get<unsigned long long>(max_tasks * 3 * kBinN * kBinKeys);
-    int *bin_n = sc.get<int>(max_tasks * 3 * kBinN);
-    Split *splits = sc.get<Split>(max_tasks);
-    int *is_split = sc.get<int>(max_tasks + 1);
-    int *child_base = sc.get<int>(max_tasks + 1);
+    auto *keys = sc.get<unsigned long long>(cap * kTaskKeys);
+    TaskBox *boxes = sc.get<TaskBox>(cap);
+    auto *bin_keys = sc.get<unsigned long long>(cap * 3 * kBinN * kBinKeys);
+    int *bin_n = sc.get<int>(cap * 3 * kBinN);
+    Split *splits = sc.get<Split>(cap);
+    int *is_split = sc.get<int>(cap + 1);
+    int *child_base = sc.get<int>(cap + 1);
     // records: at most 2n - 1 nodes
     const size_t max_recs = 2 * size_t(n);
     Rec *recs = sc.get<Rec>(max_recs);
@@ -702,7 +704,7 @@ void gpu_build(lambda_ctx *ctx, const std::vector<float> &items9, std::vector<in
     // CUB scan scratch, sized for the larger of the two scans
     size_t scan_bytes = 0, b2 = 0;
     ck(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, flags, prefix, n + 1, st), "size scan");
-    ck(cub::DeviceScan::ExclusiveSum(nullptr, b2, is_split, child_base, int(max_tasks) + 1, st), "size scan");
+    ck(cub::DeviceScan::ExclusiveSum(nullptr, b2, is_split, child_base, int(cap) + 1, st), "size scan");
     void *scan_tmp = sc.get<uint8_t>(std::max(scan_bytes, b2));
     const size_t scan_cap = std::max(scan_bytes, b2);
 
@@ -710,31 +712,47 @@ void gpu_build(lambda_ctx *ctx, const std::vector<float> &items9, std::vector<in
     ck(cudaMemcpyAsync(tasks, &root, sizeof(Task), cudaMemcpyHostToDevice, st), "upload root");
     int n_tasks = 1, n_recs = 1;
     std::vector<int> level_lo{0}, level_hi{1};  // record ranges per level
-    const int B = 256, PB = blocks(n, B);
+    std::vector<Task> htasks;
+    const int B = 256;
     for (int level = 0; n_tasks > 0; level++) {
-        k_assign<<<PB, B, 0, st>>>(tasks, n_tasks, start, end, pos_task);
-        k_init_keys<<<blocks(int64_t(n_tasks) * kTaskKeys, B), B, 0, st>>>(keys, n_tasks);
-        k_task_bounds<<<PB, B, 0, st>>>(items, d_order, pos_task, start, end, keys);
-        k_task_decode<<<blocks(n_tasks, 128), 128, 0, st>>>(items, d_order, keys, n_tasks, boxes, bin_keys, bin_n);
-        k_task_bins<<<PB, B, 0, st>>>(items, d_order, pos_task, start, end, boxes, bin_keys, bin_n);
-        k_task_split<<<blocks(n_tasks, 64), 64, 0, st>>>(items, d_order, tasks, n_tasks, boxes, bin_keys, bin_n, splits);
-        k_flags<<<blocks(n + 1, B), B, 0, st>>>(items, d_order, pos_task, start, end, splits, flags);
-        size_t tb = scan_cap;
-        ck(cub::DeviceScan::ExclusiveSum(scan_tmp, tb, flags, prefix, n + 1, st), "scan flags");
-        k_fail_list<<<PB, B, 0, st>>>(pos_task, start, end, tasks, splits, flags, prefix, fail_pos);
-        k_pass_list<<<PB, B, 0, st>>>(pos_task, start, end, tasks, splits, flags, prefix, pass_pos);
-        k_swap<<<PB, B, 0, st>>>(pos_task, start, end, tasks, splits, prefix, fail_pos, pass_pos, d_order);
-        k_is_split<<<blocks(n_tasks + 1, B), B, 0, st>>>(splits, n_tasks, is_split);
-        tb = scan_cap;
-        ck(cub::DeviceScan::ExclusiveSum(scan_tmp, tb, is_split, child_base, n_tasks + 1, st), "scan splits");
-        k_children<<<blocks(n_tasks, B), B, 0, st>>>(tasks, n_tasks, boxes, splits, prefix, start, child_base, level,
-                                                     n_recs, recs, next);
-        ck(cudaGetLastError(), "launch build level");
-        int splits_n = 0;
-        ck(cudaMemcpyAsync(&splits_n, child_base + n_tasks, sizeof(int), cudaMemcpyDeviceToHost, st), "read level");
-        ck(cudaStreamSynchronize(st), "build level");
+        // the level's task ranges, which give each chunk its positions
+        htasks.resize(size_t(n_tasks));
+        ck(cudaMemcpyAsync(htasks.data(), tasks, size_t(n_tasks) * sizeof(Task), cudaMemcpyDeviceToHost, st),
+           "read level");
+        ck(cudaStreamSynchronize(st), "read level");
+        int next_count = 0;
+        for (int c0 = 0; c0 < n_tasks; c0 += int(cap)) {
+            const int c1 = std::min(n_tasks, c0 + int(cap)), nt = c1 - c0;
+            const int P0 = htasks[size_t(c0)].start, P1 = htasks[size_t(c1 - 1)].end, np = P1 - P0;
+            const size_t off = size_t(P0 - start);
+            int *pt = pos_task + off, *fl = flags + off, *pf = prefix + off, *fp = fail_pos + off, *pp = pass_pos + off;
+            const Task *tk = tasks + c0;
+            const int PB = blocks(np, B);
+            k_assign<<<PB, B, 0, st>>>(tk, nt, P0, P1, pt);
+            k_init_keys<<<blocks(int64_t(nt) * kTaskKeys, B), B, 0, st>>>(keys, nt);
+            k_task_bounds<<<PB, B, 0, st>>>(items, d_order, pt, P0, P1, keys);
+            k_task_decode<<<blocks(nt, 128), 128, 0, st>>>(items, d_order, keys, nt, boxes, bin_keys, bin_n);
+            k_task_bins<<<PB, B, 0, st>>>(items, d_order, pt, P0, P1, boxes, bin_keys, bin_n);
+            k_task_split<<<blocks(nt, 64), 64, 0, st>>>(items, d_order, tk, nt, boxes, bin_keys, bin_n, splits);
+            k_flags<<<blocks(np + 1, B), B, 0, st>>>(items, d_order, pt, P0, P1, splits, fl);
+            size_t tb = scan_cap;
+            ck(cub::DeviceScan::ExclusiveSum(scan_tmp, tb, fl, pf, np + 1, st), "scan flags");
+            k_fail_list<<<PB, B, 0, st>>>(pt, P0, P1, tk, splits, fl, pf, fp);
+            k_pass_list<<<PB, B, 0, st>>>(pt, P0, P1, tk, splits, fl, pf, pp);
+            k_swap<<<PB, B, 0, st>>>(pt, P0, P1, tk, splits, pf, fp, pp, d_order);
+            k_is_split<<<blocks(nt + 1, B), B, 0, st>>>(splits, nt, is_split);
+            tb = scan_cap;
+            ck(cub::DeviceScan::ExclusiveSum(scan_tmp, tb, is_split, child_base, nt + 1, st), "scan splits");
+            k_children<<<blocks(nt, B), B, 0, st>>>(tk, nt, boxes, splits, pf, P0, child_base, level,
+                                                    n_recs + next_count, recs, next + next_count);
+            ck(cudaGetLastError(), "launch build level");
+            int splits_n = 0;
+            ck(cudaMemcpyAsync(&splits_n, child_base + nt, sizeof(int), cudaMemcpyDeviceToHost, st), "read level");
+            ck(cudaStreamSynchronize(st), "build level");
+            next_count += 2 * splits_n;
+        }
         std::swap(tasks, next);
-        n_tasks = 2 * splits_n;
+        n_tasks = next_count;
         if (n_tasks > 0) {
             if (size_t(n_recs + n_tasks) > max_recs) throw BuildError{cudaErrorUnknown, "build exceeded its node bound"};
             level_lo.push_back(n_recs);
