@@ -36,6 +36,8 @@ struct DeviceScene {
     const float *light_cdf;      // running sums of light_power in list order
     const float *material_emission;  // per material: average emission (0 if not emissive)
     const uint8_t *material_uv;      // per material: 1 if a texture it evaluates reads the hit's (u, v)
+    const float4 *film_flat;         // per material: (n_outer, n_film, n_sub, 1) of a one-layer thin film whose
+                                     // indices are real and non-dispersive, else zeros
     const uint32_t *instance_flags;  // bit 0: transform and inverse are exactly the identity; bit 1: also
                                      // alone in its TLAS leaf, whose box is its BLAS root's box
     const float *cie;            // [471][3] as float

@@ -447,6 +447,24 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     int3 wlo, wdim;
     build_worley_table(d, worley, wlo, wdim);
     const std::vector<int> props(d.material_properties, d.material_properties + d.num_material_properties);
+    // Per material: the three indices (outer medium, film, substrate) of a one-layer
+    // thin film whose complex spectra are all non-dispersive (every bin equal) and
+    // real, with w = 1; else zeros. Those are exactly the values a spectrum lookup
+    // returns at any wavelength, so the film kernels take them from here instead.
+    std::vector<float4> film_flat(size_t(std::max(d.num_materials, 1)), make_float4(0, 0, 0, 0));
+    for (int i = 0; i < d.num_materials; i++) {
+        const lambda_material &m = d.materials[i];
+        if (m.type != LAMBDA_MATERIAL_THINFILM || m.p[0] != 1) continue;
+        float v[3];
+        bool ok = true;
+        for (int k = 0; k < 3 && ok; k++) {
+            const int cs = d.material_properties[m.p[1] + k];
+            const double im = d.complex_spectra[size_t(cs) * LAMBDA_CIE_BINS * 2 + 1];
+            ok = cflat[size_t(cs)] != 0 && im == 0.0 && !std::signbit(im);  // +0: the fast path uses +0 imaginary parts
+            if (ok) v[k] = float(d.complex_spectra[size_t(cs) * LAMBDA_CIE_BINS * 2]);
+        }
+        if (ok) film_flat[size_t(i)] = make_float4(v[0], v[1], v[2], 1.0f);
+    }
 
     CK(b.nodes.upload(nodes.data(), nodes.size() * sizeof(float4), s), "upload nodes");
     CK(b.prims.upload(prims.data(), prims.size() * sizeof(float4), s), "upload objects");
@@ -467,6 +485,7 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     CK(b.light_cdf.upload(cdf.data(), cdf.size() * sizeof(float), s), "upload lights");
     CK(b.material_emission.upload(emission.data(), emission.size() * sizeof(float), s), "upload materials");
     CK(b.material_uv.upload(muv.data(), muv.size(), s), "upload materials");
+    CK(b.film_flat.upload(film_flat.data(), film_flat.size() * sizeof(float4), s), "upload materials");
     CK(b.cie.upload(cie.data(), cie.size() * sizeof(float), s), "upload CIE table");
     CK(b.perm.upload(kPerlinPermutation, sizeof(kPerlinPermutation), s), "upload permutation");
     CK(b.worley.upload(worley.data(), worley.size() * sizeof(float4), s), "upload Worley lattice");
@@ -542,6 +561,7 @@ extern "C" lambda_status lambda_scene_upload(lambda_ctx *ctx, const lambda_scene
     ds.light_cdf = b.light_cdf.as<float>();
     ds.material_emission = b.material_emission.as<float>();
     ds.material_uv = b.material_uv.as<uint8_t>();
+    ds.film_flat = b.film_flat.as<float4>();
     ds.instance_flags = b.instance_flags.as<uint32_t>();
     ds.families = families;
     ds.cie = b.cie.as<float>();

@@ -49,7 +49,7 @@ struct StageProfiler {
 struct SceneBuffers {
     DeviceBuffer nodes, prims, tri, instances, spectra, spectrum_flat, cspectra, cspectrum_flat, materials,
         material_props, scalar_tex, spectrum_tex, light_inst, light_obj, light_power, light_cdf, material_emission,
-        material_uv,
+        material_uv, film_flat,
         cie, perm, worley, instance_flags;
     DeviceBuffer wide[3], wide_leaves[3], wide_code[3];  // wide BVH of width 2, 4, 8
     DeviceBuffer wide_q[3];                               // its compressed node records
@@ -119,7 +119,7 @@ struct lambda_ctx {
         RenderBuffers &r = rbuf;
         return {&s.nodes, &s.prims, &s.tri, &s.instances, &s.spectra, &s.spectrum_flat, &s.cspectra,
                 &s.cspectrum_flat, &s.materials, &s.material_props, &s.scalar_tex, &s.spectrum_tex, &s.light_inst,
-                &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.material_uv, &s.cie, &s.perm, &s.worley, &s.instance_flags,
+                &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.material_uv, &s.film_flat, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &s.wide[0], &s.wide[1], &s.wide[2], &s.wide_leaves[0], &s.wide_leaves[1], &s.wide_leaves[2],
                 &s.wide_code[0], &s.wide_code[1], &s.wide_code[2], &s.wide_q[0], &s.wide_q[1], &s.wide_q[2],
                 &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.emit, &r.hit_p, &r.hit_n,

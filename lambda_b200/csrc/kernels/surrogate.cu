@@ -710,6 +710,7 @@ __global__ void __launch_bounds__(256, 3) k_film_scatter(int bounce, RenderParam
         if (valid) {
             p = q[idx];
             const ShadeIn s = load_shade(ps, sc, p);
+            const float4 ff = __ldg(&sc.film_flat[s.mat]);
             ok = in_domain[idx] != 0;
             s4 R;
             if (ok) {
@@ -721,12 +722,12 @@ __global__ void __launch_bounds__(256, 3) k_film_scatter(int bounce, RenderParam
             } else {
                 float thick[kMaxFilmLayers];
                 thin_film_thickness(sc, s, thick);
-                R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+                R = thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick, ff);
             }
             Rng rng = path_rng(ps, p);
             s4 att;
             f3 nd;
-            thin_film_scatter(sc, s, R, rng, att, nd);
+            thin_film_scatter(sc, s, R, rng, att, nd, ff);
             alive = finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
         }
         const int slot = warp_push(&ps.counts[queue_slot(bounce + 1, kQActive)], alive);

@@ -401,6 +401,7 @@ struct ShadeIn {
     f3 nrm;
     bool front;
     int4 m;
+    int mat;  // the material's index
     s4 T, lam;
 };
 
@@ -420,6 +421,7 @@ __device__ __forceinline__ ShadeIn load_shade(const PathState &ps, const DeviceS
     s.nrm = mk(hn.x, hn.y, hn.z);
     s.front = id.z != 0;
     s.m = __ldg(&sc.materials[id.x]);
+    s.mat = id.x;
     s.T = from_f4(ps.throughput[p]);
     s.lam = from_f4(ps.lam[p]);
     return s;
@@ -593,8 +595,22 @@ LAMBDA_KERNEL void __launch_bounds__(256) k_shade_specular(int bounce, RenderPar
 // reverse on back-face hits. With non-dispersive indices the interfaces are
 // formed once for all four wavelengths.
 __device__ inline s4 thin_film_r4(const DeviceScene &sc, const int4 &m, bool front, float cos0, const s4 &lam,
-                                  const float *thickness) {
+                                  const float *thickness, float4 ff = make_float4(0, 0, 0, 0)) {
     const int L = m.y < kMaxFilmLayers ? m.y : kMaxFilmLayers;
+    if (ff.w != 0.0f) {
+        // one film with real, non-dispersive indices (film_flat): the values every
+        // spectrum lookup below would return
+        cx<float> n[3] = {{front ? ff.x : ff.z, 0.0f}, {ff.y, 0.0f}, {front ? ff.z : ff.x, 0.0f}};
+        FilmPrep<float, 1> f;
+        film_prepare<float, 1>(1, n, cos0, f);
+        s4 R;
+#pragma unroll 1
+        for (int w = 0; w < kHero; w++) {
+            const FilmResult<float> r = film_apply<float, 1>(f, thickness, (2 * kPi) / lam.v[w], false);
+            R.v[w] = (r.rs + r.rp) * 0.5f;
+        }
+        return R;
+    }
     bool flat = true;
     for (int k = 0; k < L + 2; k++) flat = flat && sc.cspectrum_flat[sc.material_props[m.z + k]];
     s4 R;
@@ -659,7 +675,17 @@ __device__ inline s4 thin_film_r4_fp64(const DeviceScene &sc, const int4 &m, boo
 // Hero-wavelength reflect/refract choice and secondary-wavelength weights of the
 // thin film (material.h:228-261), given the four reflectances.
 __device__ __forceinline__ void thin_film_scatter(const DeviceScene &sc, const ShadeIn &s, const s4 &R, Rng &rng,
-                                                  s4 &att, f3 &nd) {
+                                                  s4 &att, f3 &nd, float4 ff = make_float4(0, 0, 0, 0)) {
+    if (ff.w != 0.0f) {
+        // non-dispersive real indices (film_flat): no secondary wavelength terminates
+        const float ratio = s.front ? ff.x / ff.z : ff.z / ff.x;
+        const float rh = R.v[0];
+        const bool refl = rng.next() < rh;
+        nd = refl ? reflected(s.d, s.nrm) : refracted(s.d, s.nrm, ratio);
+        att.v[0] = 1;
+        for (int k = 1; k < kHero; k++) att.v[k] = refl ? R.v[k] / rh : (1 - R.v[k]) / (1 - rh);
+        return;
+    }
     const int outer = sc.material_props[s.m.z], sub = sc.material_props[s.m.z + s.m.y + 1];
     const float n0h = float(cspectrum_at(sc, outer, s.lam.v[0]).x);
     const float n1h = float(cspectrum_at(sc, sub, s.lam.v[0]).x);
@@ -691,12 +717,13 @@ __device__ __forceinline__ bool film_path(const DeviceScene &sc, const PathState
     const ShadeIn s = load_shade(ps, sc, p);
     float thick[kMaxFilmLayers];
     thin_film_thickness(sc, s, thick);
+    const float4 ff = __ldg(&sc.film_flat[s.mat]);
     const s4 R = kFp64 ? thin_film_r4_fp64(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick)
-                       : thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick);
+                       : thin_film_r4(sc, s.m, s.front, dot(s.nrm, -s.d), s.lam, thick, ff);
     Rng rng = path_rng(ps, p);
     s4 att;
     f3 nd;
-    thin_film_scatter(sc, s, R, rng, att, nd);
+    thin_film_scatter(sc, s, R, rng, att, nd, ff);
     return finish_scatter(ps, s, rng, bounce, att, nd, 0, true);
 }
 
