@@ -431,21 +431,22 @@ def default_film_range() -> N.FilmRange:
 # not counting scene data, which is read-only and cache resident for small scenes.
 STAGE_BYTES = {
     "raygen": 16 * 2 + 16 * 2 + 16 + 8 * 2 + 16 * 4 + 4,   # film rw, radiance rw, lam w, rng rw, ray/T w, queue
-    "intersect": 4 + 32 + 48 + 4,                          # queue id, ray read, hit write, material push
-    "shade_lambert": 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 64 + 8,  # queue, dir, hit, T/lam, rng rw, ray w, T w, NEE w, pushes
-    "shade_specular": 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
-    "shade_film": 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
+    "intersect": 4 + 32 + 16 + 4,                          # queue id, ray read, hit id write, material push
+    # the shade kernels rebuild the hit record from the ray and the hit id
+    "shade_lambert": 4 + 32 + 16 + 16 * 2 + 8 * 2 + 32 + 16 + 64 + 8,  # queue, ray, hit id, T/lam, rng rw, ray w, T w, NEE w, pushes
+    "shade_specular": 4 + 32 + 16 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
+    "shade_film": 4 + 32 + 16 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
     "shadow": 4 + 16 * 3 + 8 + 16 * 2,                     # queue, NEE ray + weights, light ids, radiance rw
     "finish": 16 * 3 + 12,
-    # surrogate thin film: queue, dir, hit, T/lam, then 4 rows of 32 B and a domain flag
-    "film_encode": 4 + 16 + 48 + 16 * 2 + 4 * 32 + 1,
-    # queue, dir, hit, T/lam, 4 outputs of 16 B, domain flag, rng rw, ray w, T w, push
-    "film_scatter": 4 + 16 + 48 + 16 * 2 + 4 * 16 + 1 + 8 * 2 + 32 + 16 + 4,
+    # surrogate thin film: queue, ray, hit id, T/lam, then 4 rows of 32 B and a domain flag
+    "film_encode": 4 + 32 + 16 + 16 * 2 + 4 * 32 + 1,
+    # queue, ray, hit id, T/lam, 4 outputs of 16 B, domain flag, rng rw, ray w, T w, push
+    "film_scatter": 4 + 32 + 16 + 16 * 2 + 4 * 16 + 1 + 8 * 2 + 32 + 16 + 4,
     # per segment: the ray and hit state of intersect plus a scatter's reads and writes
     # (the path kernel keeps a pixel's state in one thread, mostly in L1/L2)
-    "path": 4 + 32 + 48 + 4 + 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
+    "path": 4 + 32 + 16 + 4 + 4 + 32 + 16 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
     # the fused bounce kernel: the same per-segment reads and writes as the path kernel
-    "bounce": 4 + 32 + 48 + 4 + 4 + 16 + 48 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
+    "bounce": 4 + 32 + 16 + 4 + 4 + 32 + 16 + 16 * 2 + 8 * 2 + 32 + 16 + 4,
 }
 
 

@@ -593,13 +593,16 @@ __device__ __forceinline__ bool closest_hit_finish(const DeviceScene &s, const R
 // depth-first traversal that visits the nodes the reference visits in the order it
 // visits them (right child first), culls an entry when its box starts beyond the best
 // hit, lets a TLAS leaf test only its first instance (scene.h:80), and accepts
-// candidates when t < best. Returns false on a miss.
+// candidates when t < best. This is the traversal alone: best, best_obj and
+// best_inst come back (best_obj < 0 on a miss); closest_hit_finish makes the hit
+// record from them.
 template <int K>
-__device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow,
-                                              const WideStack &st, const WideStack &sub) {
-    const Ray3 wr = make_ray(o, d);
-    float best = kMax;
-    int best_obj = -1, best_inst = -1;
+__device__ __forceinline__ void closest_hit_ids_w(const DeviceScene &s, const Ray3 &wr, float &best, int &best_obj,
+                                                  int &best_inst, bool &overflow, const WideStack &st,
+                                                  const WideStack &sub) {
+    best = kMax;
+    best_obj = -1;
+    best_inst = -1;
     int sp = 0;
     float te;
     if (slab(__ldg(&s.nodes[0]), __ldg(&s.nodes[1]), wr, te)) st.put(sp++, root_entry<K>(s, __ldg(&s.wide_code[0])), te);
@@ -645,6 +648,16 @@ __device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, 
         }
         if (overflow) break;
     }
+}
+
+// Scene::hit in closest-hit mode with the hit record. Returns false on a miss.
+template <int K>
+__device__ __forceinline__ bool closest_hit_w(const DeviceScene &s, f3 o, f3 d, Hit &h, bool &overflow,
+                                              const WideStack &st, const WideStack &sub) {
+    const Ray3 wr = make_ray(o, d);
+    float best;
+    int best_obj, best_inst;
+    closest_hit_ids_w<K>(s, wr, best, best_obj, best_inst, overflow, st, sub);
     return closest_hit_finish(s, wr, best, best_obj, best_inst, h);
 }
 

@@ -87,9 +87,7 @@ struct PathState {
     float4 *throughput;
     float4 *radiance;     // NEE terms of the running sample
     float4 *emit;         // emission term of a sample that ended at a miss or an emitter
-    float4 *hit_p;        // world point xyz, w = u
-    float4 *hit_n;        // shading normal xyz, w = v
-    int4 *hit_id;         // instance (-1 = miss), object, front facing, 0
+    int4 *hit_id;         // material, object, distance (float bits), instance of a stored hit
     float4 *sh_o;         // NEE ray origin xyz, w = MIS weight
     float4 *sh_d;         // NEE ray direction xyz, w = light pdf
     float4 *sh_a;         // throughput * BSDF * cos

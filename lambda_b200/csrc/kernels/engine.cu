@@ -652,8 +652,6 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     CK(r.throughput.reserve(P * 16), "allocate path state");
     CK(r.radiance.reserve(P * 16), "allocate path state");
     CK(r.emit.reserve(P * 16), "allocate path state");
-    CK(r.hit_p.reserve(P * 16), "allocate path state");
-    CK(r.hit_n.reserve(P * 16), "allocate path state");
     CK(r.hit_id.reserve(P * 16), "allocate path state");
     CK(r.sh_o.reserve(P * 16), "allocate path state");
     CK(r.sh_d.reserve(P * 16), "allocate path state");
@@ -679,8 +677,6 @@ lambda_status lambda_ctx::ensure_state(int pixels, int depth) {
     ps.throughput = r.throughput.as<float4>();
     ps.radiance = r.radiance.as<float4>();
     ps.emit = r.emit.as<float4>();
-    ps.hit_p = r.hit_p.as<float4>();
-    ps.hit_n = r.hit_n.as<float4>();
     ps.hit_id = r.hit_id.as<int4>();
     ps.sh_o = r.sh_o.as<float4>();
     ps.sh_d = r.sh_d.as<float4>();

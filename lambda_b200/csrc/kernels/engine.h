@@ -56,7 +56,7 @@ struct SceneBuffers {
 };
 
 struct RenderBuffers {
-    DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, emit, hit_p, hit_n, hit_id, sh_o, sh_d, sh_a, sh_light,
+    DeviceBuffer rng, film, lam, ray_o, ray_d, throughput, radiance, emit, hit_id, sh_o, sh_d, sh_a, sh_light,
         q0, q1, qs, qm0, qm1, qm2, counts, wave, stats, error, out, path_info, jobs, active, work, film_rows, film_out,
         film_in_domain;
 };
@@ -122,8 +122,8 @@ struct lambda_ctx {
                 &s.light_obj, &s.light_power, &s.light_cdf, &s.material_emission, &s.material_uv, &s.film_flat, &s.cie, &s.perm, &s.worley, &s.instance_flags,
                 &s.wide[0], &s.wide[1], &s.wide[2], &s.wide_leaves[0], &s.wide_leaves[1], &s.wide_leaves[2],
                 &s.wide_code[0], &s.wide_code[1], &s.wide_code[2], &s.wide_q[0], &s.wide_q[1], &s.wide_q[2],
-                &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.emit, &r.hit_p, &r.hit_n,
-                &r.hit_id, &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
+                &r.rng, &r.film, &r.lam, &r.ray_o, &r.ray_d, &r.throughput, &r.radiance, &r.emit, &r.hit_id,
+                &r.sh_o, &r.sh_d, &r.sh_a, &r.sh_light, &r.q0, &r.q1, &r.qs, &r.qm0, &r.qm1, &r.qm2, &r.counts, &r.wave,
                 &r.stats, &r.error, &r.out, &r.path_info, &r.jobs, &r.active, &r.work, &r.film_rows, &r.film_out,
                 &r.film_in_domain, &sbuf.weights_bf16, &sbuf.weights_f32};
     }

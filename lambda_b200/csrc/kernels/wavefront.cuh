@@ -201,70 +201,74 @@ __device__ __forceinline__ int material_of(const DeviceScene &sc, int inst_mater
 // Closest hit of path p (renderer.h:94-131). A miss or an emitter hit records the
 // path's emission term and returns -1: the path ends. Any other hit is stored for the
 // shade kernels and its material family returned: 0 Lambertian, 1 mirror or
-// dielectric, 2 thin film.
+// dielectric, 2 thin film. The stored hit is (material, object, distance, instance)
+// alone: load_shade rebuilds the hit point, normal, (u, v) and facing from it with
+// the same functions, so the traversal kernels leave that work, and its bytes, to
+// the hits' shading kernels.
 __device__ __forceinline__ int trace_finish(const DeviceScene &sc, const PathState &ps, int p, const float4 &o4,
-                                            const float4 &d4, bool hit, const Hit &h);
+                                            const float4 &d4, const Ray3 &wr, float best, int obj, int inst);
 
 template <int K>
 __device__ __forceinline__ int trace_path(const DeviceScene &sc, const PathState &ps, int p, const WideStack &st_a,
                                           const WideStack &st_b) {
     const float4 o4 = ps.ray_o[p], d4 = ps.ray_d[p];
-    const f3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
-    Hit h;
+    const Ray3 wr = make_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
+    float best;
+    int obj, inst;
     bool overflow = false;
-    const bool hit = closest_hit_w<K>(sc, o, d, h, overflow, st_a, st_b);
+    closest_hit_ids_w<K>(sc, wr, best, obj, inst, overflow, st_a, st_b);
     if (overflow) atomicOr(ps.error, 1);
-    return trace_finish(sc, ps, p, o4, d4, hit, h);
+    return trace_finish(sc, ps, p, o4, d4, wr, best, obj, inst);
 }
 
-// What trace_path does with path p's hit record (ray o4, d4): a miss or an emitter
-// hit records the emission term and returns -1; any other hit is stored and its
-// material family returned.
+// What trace_path does with path p's closest hit (ray o4, d4 = wr; best, obj, inst
+// from the traversal, obj < 0 on a miss): a miss or an emitter hit records the
+// emission term and returns -1; any other hit is stored and its material family
+// returned.
 __device__ __forceinline__ int trace_finish(const DeviceScene &sc, const PathState &ps, int p, const float4 &o4,
-                                            const float4 &d4, bool hit, const Hit &h) {
+                                            const float4 &d4, const Ray3 &wr, float best, int obj, int inst) {
     const f3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
     const bool specular = d4.w != 0.0f;
     const float prev_pdf = o4.w;
     const bool lights = sc.total_light_power > 0;
-    if (!hit) {
+    if (obj < 0) {
         const s4 lam = from_f4(ps.lam[p]);
         float w = 1;
         if (!specular && lights)
             w = power_heuristic(prev_pdf, (1 / (4 * kPi)) * sc.light_power[sc.num_lights - 1] / sc.total_light_power);
         const s4 T = from_f4(ps.throughput[p]);
         ps.emit[p] = to_f4(T * background_eval(sc, d, lam) * w);
-    } else {
-        const InstanceRef ir = instance_ref(sc, h.instance);
-        const int4 ih = ir.header();
-        const int mat = material_of(sc, ih.w, h.object);
-        const int4 m = __ldg(&sc.materials[mat]);
-        if (m.x == kEmissive) {
-            float w = 1;
-            if (!specular && lights) {
-                float M[16], Mi[16];
-                ir.load_m(M, 0);
-                ir.load_m(Mi, 1);
-                const Prim pr = load_prim(sc, h.object);
-                const f3 c0 = mk(M[0], M[4], M[8]);
-                const float light_power = prim_area(pr) * length_sq(c0) * sc.material_emission[mat];
-                const float pdf = prim_pdf(pr, xform(Mi, o, 1), normalize(xform(Mi, d, 0)));
-                w = power_heuristic(prev_pdf, pdf * light_power / sc.total_light_power);
-            }
-            ShadePoint sp;
-            sp.point = h.point;
-            sp.u = h.u;
-            sp.v = h.v;
-            const s4 lam = from_f4(ps.lam[p]);
-            const s4 T = from_f4(ps.throughput[p]);
-            ps.emit[p] = to_f4(T * spectrum_texture4(sc, m.y, sp, lam) * w);
-        } else {
-            ps.hit_p[p] = make_float4(h.point.x, h.point.y, h.point.z, h.u);
-            ps.hit_n[p] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.v);
-            ps.hit_id[p] = make_int4(mat, h.object, h.front ? 1 : 0, h.instance);
-            return m.x == kLambertian ? 0 : (m.x == kThinFilm ? 2 : 1);
-        }
+        return -1;
     }
-    return -1;
+    const InstanceRef ir = instance_ref(sc, inst);
+    const int4 ih = ir.header();
+    const int mat = material_of(sc, ih.w, obj);
+    const int4 m = __ldg(&sc.materials[mat]);
+    if (m.x == kEmissive) {
+        Hit h;
+        closest_hit_finish(sc, wr, best, obj, inst, h);
+        float w = 1;
+        if (!specular && lights) {
+            float M[16], Mi[16];
+            ir.load_m(M, 0);
+            ir.load_m(Mi, 1);
+            const Prim pr = load_prim(sc, obj);
+            const f3 c0 = mk(M[0], M[4], M[8]);
+            const float light_power = prim_area(pr) * length_sq(c0) * sc.material_emission[mat];
+            const float pdf = prim_pdf(pr, xform(Mi, o, 1), normalize(xform(Mi, d, 0)));
+            w = power_heuristic(prev_pdf, pdf * light_power / sc.total_light_power);
+        }
+        ShadePoint sp;
+        sp.point = h.point;
+        sp.u = h.u;
+        sp.v = h.v;
+        const s4 lam = from_f4(ps.lam[p]);
+        const s4 T = from_f4(ps.throughput[p]);
+        ps.emit[p] = to_f4(T * spectrum_texture4(sc, m.y, sp, lam) * w);
+        return -1;
+    }
+    ps.hit_id[p] = make_int4(mat, obj, __float_as_int(best), inst);
+    return m.x == kLambertian ? 0 : (m.x == kThinFilm ? 2 : 1);
 }
 
 // Closest hit; misses and emitter hits record their emission term and end the
@@ -377,9 +381,7 @@ LAMBDA_KERNEL void __launch_bounds__(256, 2) k_intersect_fetch(int bounce, Rende
         } else {
             // the ray is done (or a stack overflowed): finish it and push it
             if (overflow) atomicOr(ps.error, 1);
-            Hit h;
-            const bool hit = closest_hit_finish(sc, wr, best, best_obj, best_inst, h);
-            const int family = trace_finish(sc, ps, p, ps.ray_o[p], ps.ray_d[p], hit, h);
+            const int family = trace_finish(sc, ps, p, ps.ray_o[p], ps.ray_d[p], wr, best, best_obj, best_inst);
             if (family >= 0) {
                 const unsigned grp = __match_any_sync(__activemask(), family);
                 const int leader = __ffs(grp) - 1;
@@ -411,15 +413,17 @@ __device__ __forceinline__ Rng path_rng(const PathState &ps, int p) { return pix
 __device__ __forceinline__ ShadeIn load_shade(const PathState &ps, const DeviceScene &sc, int p) {
     ShadeIn s;
     s.p = p;
-    const float4 d4 = ps.ray_d[p];
+    const float4 o4 = ps.ray_o[p], d4 = ps.ray_d[p];
     s.d = mk(d4.x, d4.y, d4.z);
-    const float4 hp = ps.hit_p[p], hn = ps.hit_n[p];
+    // the hit record from (object, distance, instance), as closest_hit_w makes it
     const int4 id = ps.hit_id[p];
-    s.sp.point = mk(hp.x, hp.y, hp.z);
-    s.sp.u = hp.w;
-    s.sp.v = hn.w;
-    s.nrm = mk(hn.x, hn.y, hn.z);
-    s.front = id.z != 0;
+    Hit h;
+    closest_hit_finish(sc, make_ray(mk(o4.x, o4.y, o4.z), s.d), __int_as_float(id.z), id.y, id.w, h);
+    s.sp.point = h.point;
+    s.sp.u = h.u;
+    s.sp.v = h.v;
+    s.nrm = h.normal;
+    s.front = h.front;
     s.m = __ldg(&sc.materials[id.x]);
     s.mat = id.x;
     s.T = from_f4(ps.throughput[p]);
