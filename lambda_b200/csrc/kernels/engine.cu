@@ -1448,7 +1448,7 @@ lambda_status autotune_views(lambda_ctx *ctx, const lambda_render_desc *probes, 
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         // path state, queues, staged image, the surrogate's MLP rows, outputs and domain flags
-        constexpr size_t kBytesPerPixel = 8 + 16 * 14 + 8 + 8 + 4 * 6 + 12 + 4 * 32 + 4 * 16 + 1;
+        constexpr size_t kBytesPerPixel = 8 + 16 * 12 + 8 + 8 + 4 * 6 + 12 + 4 * 32 + 4 * 16 + 1;
         best.max_pixels = int32_t(std::min<size_t>((free_b / 2) / kBytesPerPixel, size_t(1) << 30));
     }
     ctx->tuning = best;
