@@ -145,8 +145,29 @@ __device__ inline float worley_noise(const DeviceScene &s, f3 p) {
     const int ix = xi - 1 - s.worley_lo.x, iy = yi - 1 - s.worley_lo.y, iz = zi - 1 - s.worley_lo.z;
     const bool inside = ix >= 0 && iy >= 0 && iz >= 0 && ix + 2 < s.worley_dim.x && iy + 2 < s.worley_dim.y &&
                         iz + 2 < s.worley_dim.z;
-    const float4 *block = inside ? s.worley_cells + (size_t(iz) * dxy + size_t(iy) * dx + ix) : nullptr;
     float d2 = 0;
+    if (inside) {
+        // The walk unrolled: each cell's offsets, and so its gaps, are constants. The
+        // squared gaps per axis and side are formed once; the test, the load and the
+        // distance are the rolled loop's below.
+        constexpr unsigned char kOrder[27] = {0x15, 0x14, 0x16, 0x11, 0x19, 0x05, 0x25, 0x10, 0x18,
+                                              0x12, 0x1a, 0x04, 0x24, 0x06, 0x26, 0x01, 0x21, 0x09,
+                                              0x29, 0x00, 0x20, 0x08, 0x28, 0x02, 0x22, 0x0a, 0x2a};
+        const float4 *block = s.worley_cells + (size_t(iz) * dxy + size_t(iy) * dx + ix);
+        const float gxx[3] = {fx * fx, 0.0f, (1 - fx) * (1 - fx)};
+        const float gyy[3] = {fy * fy, 0.0f, (1 - fy) * (1 - fy)};
+        const float gzz[3] = {fz * fz, 0.0f, (1 - fz) * (1 - fz)};
+#pragma unroll
+        for (int c = 0; c < 27; c++) {
+            const int ox = kOrder[c] & 3, oy = (kOrder[c] >> 2) & 3, oz = (kOrder[c] >> 4) & 3;
+            if (c > 0 && gxx[ox] + gyy[oy] + gzz[oz] > d2 * 1.0001f + 1e-6f) continue;
+            const float4 h = __ldg(block + (oz * dxy + oy * dx + ox));
+            const f3 feature = mk(h.x, h.y, h.z) + mk(float(xi + ox - 1), float(yi + oy - 1), float(zi + oz - 1));
+            const float e2 = length_sq(p - feature);
+            d2 = c == 0 ? e2 : fminf(d2, e2);
+        }
+        return fminf(9999.0f, sqrtf(d2));
+    }
 #pragma unroll 1
     for (int c = 0; c < 27; c++) {
         const int code = kWorleyOrder[c];
@@ -158,13 +179,7 @@ __device__ inline float worley_noise(const DeviceScene &s, f3 p) {
             const float lb2 = gx * gx + gy * gy + gz * gz;
             if (lb2 > d2 * 1.0001f + 1e-6f) continue;
         }
-        f3 off;
-        if (inside) {
-            const float4 h = __ldg(block + ((zo + 1) * dxy + (yo + 1) * dx + (xo + 1)));
-            off = mk(h.x, h.y, h.z);
-        } else {
-            off = worley_feature(s, xi + xo, yi + yo, zi + zo);
-        }
+        const f3 off = worley_feature(s, xi + xo, yi + yo, zi + zo);
         const f3 feature = off + mk(float(xi + xo), float(yi + yo), float(zi + zo));
         const float e2 = length_sq(p - feature);
         d2 = c == 0 ? e2 : fminf(d2, e2);
