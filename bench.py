@@ -48,7 +48,7 @@ W, H, SPP, DEPTH = 1920, 1080, 256, 16
 # dram__bytes_write.sum over its 2,073,600 camera rays); the JSON line scales the
 # bytes to the average launch as `traffic`.
 PROFILED = {
-    "intersect": {"dram_bytes_per_item": (89.619968e6 + 50.342656e6) / 2073600, "issue_slot_utilisation": 0.6455},
+    "intersect": {"dram_bytes_per_item": (89.285632e6 + 16.259072e6) / 2073600, "issue_slot_utilisation": 0.6141},
 }
 
 
