@@ -147,9 +147,14 @@ __device__ inline float worley_noise(const DeviceScene &s, f3 p) {
                         iz + 2 < s.worley_dim.z;
     float d2 = 0;
     if (inside) {
-        // The walk unrolled: each cell's offsets, and so its gaps, are constants. The
-        // squared gaps per axis and side are formed once; the test, the load and the
-        // distance are the rolled loop's below.
+        // The walk unrolled, in rounds of independent loads instead of a chain: the
+        // centre and its six face neighbours unconditionally, then the 20 edge and
+        // corner cells four at a time, each group's cells tested against the minimum
+        // before the group and loaded together. Each cell's offsets, and so its gaps,
+        // are constants; the squared gaps per axis and side are formed once. A cell is
+        // skipped only when its box is farther (with the margin) than a distance
+        // already found, which never skips the nearest feature, so the minimum is the
+        // one the sequential walk below finds.
         constexpr unsigned char kOrder[27] = {0x15, 0x14, 0x16, 0x11, 0x19, 0x05, 0x25, 0x10, 0x18,
                                               0x12, 0x1a, 0x04, 0x24, 0x06, 0x26, 0x01, 0x21, 0x09,
                                               0x29, 0x00, 0x20, 0x08, 0x28, 0x02, 0x22, 0x0a, 0x2a};
@@ -157,14 +162,35 @@ __device__ inline float worley_noise(const DeviceScene &s, f3 p) {
         const float gxx[3] = {fx * fx, 0.0f, (1 - fx) * (1 - fx)};
         const float gyy[3] = {fy * fy, 0.0f, (1 - fy) * (1 - fy)};
         const float gzz[3] = {fz * fz, 0.0f, (1 - fz) * (1 - fz)};
-#pragma unroll
-        for (int c = 0; c < 27; c++) {
+        auto cell_d2 = [&](int c, const float4 &h) {
             const int ox = kOrder[c] & 3, oy = (kOrder[c] >> 2) & 3, oz = (kOrder[c] >> 4) & 3;
-            if (c > 0 && gxx[ox] + gyy[oy] + gzz[oz] > d2 * 1.0001f + 1e-6f) continue;
-            const float4 h = __ldg(block + (oz * dxy + oy * dx + ox));
             const f3 feature = mk(h.x, h.y, h.z) + mk(float(xi + ox - 1), float(yi + oy - 1), float(zi + oz - 1));
-            const float e2 = length_sq(p - feature);
-            d2 = c == 0 ? e2 : fminf(d2, e2);
+            return length_sq(p - feature);
+        };
+        auto cell_at = [&](int c) {
+            const int ox = kOrder[c] & 3, oy = (kOrder[c] >> 2) & 3, oz = (kOrder[c] >> 4) & 3;
+            return block + (oz * dxy + oy * dx + ox);
+        };
+        float4 h1[7];
+#pragma unroll
+        for (int c = 0; c < 7; c++) h1[c] = __ldg(cell_at(c));
+        d2 = cell_d2(0, h1[0]);
+#pragma unroll
+        for (int c = 1; c < 7; c++) d2 = fminf(d2, cell_d2(c, h1[c]));
+#pragma unroll
+        for (int c0 = 7; c0 < 27; c0 += 4) {
+            const float reach = d2 * 1.0001f + 1e-6f;
+            float4 h[4];
+            bool near[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int c = c0 + k;
+                near[k] = !(gxx[kOrder[c] & 3] + gyy[(kOrder[c] >> 2) & 3] + gzz[(kOrder[c] >> 4) & 3] > reach);
+                h[k] = near[k] ? __ldg(cell_at(c)) : make_float4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (near[k]) d2 = fminf(d2, cell_d2(c0 + k, h[k]));
         }
         return fminf(9999.0f, sqrtf(d2));
     }
