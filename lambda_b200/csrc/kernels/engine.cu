@@ -834,7 +834,7 @@ lambda_status render_pass(lambda_ctx *ctx, const lambda_job *jobs, const std::ve
     const lambda_tuning &tu = ctx->tuning;
     const DeviceScene sc = ctx->scene_view(tu.bvh_width);
     const int dev = ctx->device, sms = ctx->sm_count;
-    const int tb = tu.trace_block, sb = tu.shade_block, gs = tu.grid_scale, bw = tu.bvh_width;
+    const int tb = tu.trace_block, sb = tu.shade_block, gs = tu.grid_scale;
     const size_t stack_smem = wide_stack_bytes(tb, sc.stack_tlas, sc.stack_blas);
     // intersect: a warp traces 32 rays to the end, or (lane_fetch) lanes take rays one
     // by one; over the tuned BVH layout (width, exact or compressed node records)

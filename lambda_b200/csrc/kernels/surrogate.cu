@@ -80,7 +80,6 @@ constexpr int kActBytes = kTileM * kH * 2;       //   [128][16] overlays the sta
 template <int G> constexpr int kBarOf = sAct + G * kActBytes;
 template <int G> constexpr int kTmemSlotOf = kBarOf<G> + 8 * G;
 template <int G> constexpr int kSmemOf = kTmemSlotOf<G> + 8;
-constexpr int kSmemBytes = kSmemOf<1>;
 constexpr int kTmemCols = 64;  // per warpgroup
 constexpr int kQueryWarpgroups = 4;  // warpgroups per CTA of the batched query kernel
 
