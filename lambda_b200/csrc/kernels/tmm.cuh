@@ -189,9 +189,22 @@ __device__ __forceinline__ void film_prepare(int L, const cx<R> *n, R cos0, Film
 // round-trip phase (Airy summation, the closed form of the 2x2 product). The
 // denominator is at least (1 - |r01 r12|)^2, far from zero for real indices, so FP32
 // keeps it within a few 1e-7 of FP64.
+// The quotient takes the fast division (2 ulp), well inside the FP32 form's 1e-5.
 __device__ __forceinline__ float airy_r(float r01, float r12, float cos2phi) {
     const float ab = r01 * r12, t = 2 * ab * cos2phi;
-    return (r01 * r01 + r12 * r12 + t) / (1 + ab * ab + t);
+    return __fdividef(r01 * r01 + r12 * r12 + t, 1 + ab * ab + t);
+}
+
+// cos x of a film's round-trip phase (|x| up to about 1e5), for the FP32 form only.
+// Cody and Waite's reduction: x less n 2 pi, n the integer nearest x / (2 pi), with
+// 2 pi split into two floats (c1, 2 pi rounded to float; c2, the float nearest
+// 2 pi - c1; the remainder, 6.9e-15, times n stays below 1e-9) and fused
+// multiply-adds, then the hardware cosine on [-pi, pi] (absolute error below 4e-7).
+__device__ __forceinline__ float cos_phase(float x) {
+    const float n = rintf(x * 0.159154937f);
+    float r = fmaf(-n, 6.28318548f, x);
+    r = fmaf(-n, -1.74845553e-7f, r);
+    return __cosf(r);
 }
 
 // Layer phases at one wavelength; k = 2 pi / lambda, d[j] in nm.
@@ -201,7 +214,7 @@ __device__ __forceinline__ FilmResult<R> film_apply(const FilmPrep<R, MAXL> &f, 
         if (f.airy) {
             // the same phase as below: ((n k) d) cos, real here; round trip 2 phi
             const R phi = ((f.n_layer[0].re * k) * d[0]) * f.cos_layer[0].re;
-            const R c2 = cosf(2 * phi);
+            const R c2 = cos_phase(2 * phi);
             FilmResult<R> out;
             out.rs = airy_r(f.rs01, f.rs12, c2);
             out.rp = airy_r(f.rp01, f.rp12, c2);
