@@ -9,11 +9,11 @@
 //                    to BF16 exactly as inference rounds it; per-CTA gradients are
 //                    summed with atomics
 //   k_adam           Adam update of the FP32 master weights
-//   k_mlp_tc         inference on the 5th-generation tensor cores: persistent CTAs of
-//                    4 warps, BF16 weights resident in shared memory (canonical K-major
-//                    layout, no swizzle), tcgen05.mma with FP32 accumulators in tensor
-//                    memory, tcgen05.ld epilogues (bias, ReLU, BF16) writing the next
-//                    layer's operand back to shared memory
+//   k_mlp_tc         inference on the 5th-generation tensor cores: one persistent CTA
+//                    per SM of 5 warpgroups, BF16 weights resident in shared memory
+//                    (canonical K-major layout, no swizzle), each layer's input rows
+//                    and FP32 accumulators in tensor memory (tcgen05.mma with A from
+//                    TMEM), tcgen05.ld / tcgen05.st epilogues (ReLU, BF16)
 //   k_film_encode    the render's thin-film shade, in three kernels per bounce: the
 //   k_mlp_tc         hits' four hero-wavelength queries encoded as MLP rows, the
 //   k_film_scatter   tensor-core MLP over them, then the scatter; hits outside the
@@ -71,17 +71,21 @@ constexpr int sB2 = sW4 + kOutPad * kH * 2;      // [64][8]: (b2 hi, b2 lo, 0, .
 constexpr int sB3 = sB2 + kH * 16;               // [64][8]
 constexpr int sB4 = sB3 + kH * 16;               // [16][8]
 constexpr int kPackedWeightBytes = sB4 + kOutPad * 16;  // the weight image, copied as is
-constexpr int sOnes = kPackedWeightBytes;        // [128][8]: (1, 1, 0, ...), shared by the warpgroups
-constexpr int sZero = sOnes + kTileM * 16;       // [128][8] zeros
-constexpr int sAct = sZero + kTileM * 16;        // G activation tiles [128][64]; each layer-1 operand
-constexpr int kActBytes = kTileM * kH * 2;       //   [128][16] overlays the start of its tile
-// A CTA of G warpgroups: each runs its own stream of 128-row tiles with its own
-// activation tile, mbarrier and kTmemCols TMEM columns; the weights are shared.
-template <int G> constexpr int kBarOf = sAct + G * kActBytes;
-template <int G> constexpr int kTmemSlotOf = kBarOf<G> + 8 * G;
-template <int G> constexpr int kSmemOf = kTmemSlotOf<G> + 8;
-constexpr int kTmemCols = 64;  // per warpgroup
-constexpr int kQueryWarpgroups = 4;  // warpgroups per CTA of the batched query kernel
+constexpr int sZero = kPackedWeightBytes;        // [128][8] zeros
+// A CTA runs kChains warpgroups, each with its own stream of 128-row tiles, its own
+// MMA-completion mbarrier and 96 TMEM columns: a 64-column FP32 accumulator and a
+// 32-column BF16 operand (the layer's input rows, two values per column). The
+// weights are the only operands in shared memory.
+constexpr int kChains = 5;                       // 5 x 96 + 8 columns fit the SM's 512
+constexpr int sBar = sZero + kTileM * 16;        // kChains mbarriers
+constexpr int sTmemSlot = sBar + 8 * kChains;
+constexpr int kMlpSmem = sTmemSlot + 8;
+constexpr int kMlpThreads = 128 * kChains;
+constexpr int kTmemAlloc = 512;                  // the CTA's TMEM allocation (a power of two)
+constexpr int tAcc = 0;                          // chain c's accumulator: columns 64c .. 64c + 63
+constexpr int tOperand = 64 * kChains;           // chain c's operand: columns 320 + 32c .. + 31
+constexpr int tOnes = tOperand + 32 * kChains;   // (1, 1, 0 ...) rows, 8 columns, shared by the chains
+static_assert(tOnes + 8 <= kTmemAlloc, "TMEM columns");
 
 // Input normalisation to [-1, 1] over the trained box.
 struct Range {
@@ -129,15 +133,6 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 // Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M = 128.
 __host__ __device__ constexpr uint32_t instr_desc(int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(kTileM >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-        :
-        : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -224,83 +219,115 @@ __device__ __forceinline__ uint32_t relu_bf16x2(uint32_t lo, uint32_t hi) {
 // Tensor-core inference
 // ---------------------------------------------------------------------------
 
-// Writes 8 consecutive bf16 values (k = c*8 .. c*8+7 of row r) of a K-major operand.
-__device__ __forceinline__ void put8(uint8_t *smem, int base, int r, int c, int K, const float *v) {
-    __nv_bfloat162 p[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) p[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-    *reinterpret_cast<uint4 *>(smem + base + core_offset(r, c * 8, K)) = *reinterpret_cast<uint4 *>(p);
+// D (TMEM) = A (TMEM, BF16, K-major rows: row i in lane i, two K values per 32-bit
+// column) x B (shared memory descriptor).
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
-// Barrier of warpgroup wg of a CTA of G: the CTA barrier when it is the only one,
-// else named barrier 1 + wg. A barrier id in a register makes ptxas reserve all 16
-// of the CTA's barriers, which limits how many CTAs an SM holds; that is paid only
-// by the multi-warpgroup query kernel (two CTAs per SM), never by the render's
-// single-warpgroup kernel, which runs several CTAs per SM.
-template <int G>
-__device__ __forceinline__ void wg_sync(int wg) {
-    if constexpr (G == 1) __syncthreads();
-    else asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
+// 16 / 8 consecutive 32-bit columns of this warp's 32 TMEM lanes (one per thread).
+__device__ __forceinline__ void tmem_st16(uint32_t addr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(addr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
 }
+
+__device__ __forceinline__ void tmem_st8(uint32_t addr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(addr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+
+// Waits for this thread's outstanding tcgen05.st.
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// One lane of a converged warp (elect.sync); the MMAs are issued from a
+// warp-uniform branch, so their operands stay warp-uniform.
+__device__ __forceinline__ bool elect_one() {
+    uint32_t leader;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "elect.sync _|p, 0xffffffff;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(leader));
+    return leader != 0;
+}
+
+// Round-to-nearest BF16 of two FP32 values; lo in the low half (element k).
+__device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
+    uint32_t d;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
+// Barrier of warpgroup wg (named barrier 1 + wg, 128 threads).
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory"); }
 
 // AND of a predicate over warpgroup wg, as its barrier.
-template <int G>
 __device__ __forceinline__ bool wg_sync_and(int wg, bool v) {
-    if constexpr (G == 1) {
-        return __syncthreads_and(v) != 0;
-    } else {
-        uint32_t r;
-        asm volatile(
-            "{\n\t.reg .pred p, q;\n\t"
-            "setp.ne.b32 q, %1, 0;\n\t"
-            "barrier.cta.red.and.pred p, %2, 128, q;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(r)
-            : "r"(uint32_t(v)), "r"(1 + wg)
-            : "memory");
-        return r != 0;
-    }
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 q, %1, 0;\n\t"
+        "barrier.cta.red.and.pred p, %2, 128, q;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r)
+        : "r"(uint32_t(v)), "r"(1 + wg)
+        : "memory");
+    return r != 0;
 }
 
-// One warpgroup's slot in a CTA of the tensor-core MLP kernels.
-struct TileCtx {
-    uint32_t base;       // shared-memory address of smem[0]
-    int act;             // byte offset of this warpgroup's activation tile
-    uint32_t bar;        // its MMA completion mbarrier
-    uint32_t tmem;       // its TMEM accumulator (lane 0, first of its kTmemCols columns)
-    uint32_t lane_base;  // this warp's 32 TMEM lanes of it
-    uint32_t phase;
-    int wg;              // its index in the CTA (its barrier, see wg_sync)
-    int row;             // this thread's row in the warpgroup's tiles (0..127)
-};
-
-// Sets up one CTA of G warpgroups: the weight image and the constant (1, 1) and zero
-// blocks into shared memory, one completion mbarrier per warpgroup, and G *
-// kTmemCols TMEM columns (warp 0 allocates).
-template <int G>
-__device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__restrict__ packed) {
-    const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7;
-    for (int i = tid; i < kPackedWeightBytes / 16; i += blockDim.x) reinterpret_cast<uint4 *>(smem)[i] = packed[i];
-    constexpr uint32_t kOneOne = 0x3F803F80u;  // bf16 (1, 1)
-    for (int r = tid; r < kTileM; r += blockDim.x) {
-        *reinterpret_cast<uint4 *>(smem + sOnes + r * 16) = make_uint4(kOneOne, 0, 0, 0);
-        *reinterpret_cast<uint4 *>(smem + sZero + r * 16) = make_uint4(0, 0, 0, 0);
-    }
-    TileCtx t;
-    t.base = smem_u32(smem);
-    t.act = sAct + wg * kActBytes;
-    t.bar = smem_u32(smem + kBarOf<G> + 8 * wg);
-    t.phase = 0;
-    t.wg = wg;
-    t.row = tid & 127;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kTmemSlotOf<G>);
-    if (tid < G) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(smem + kBarOf<G> + 8 * tid)) : "memory");
+// Inference over n_rows rows, or rows_per_count * *count rows when count is given
+// (a count the GPU produced, such as a bounce's thin-film hits): row i's input is
+// kRowStride floats already encoded (kQueries = false) or the i-th
+// lambda_film_query, encoded here (kQueries = true); out: rows x (R_s, R_p, T_s, T_p).
+//
+// One CTA per SM, persistent, of kChains warpgroups. Each warpgroup works through its
+// own 128-row tiles, one thread per row, with every layer's input rows kept in tensor
+// memory: the thread writes its row's layer-1 operand (5 features, the two
+// constant-1 bias columns, zeros to K = 16) with tcgen05.st, and each hidden layer's
+// epilogue reads the accumulator (tcgen05.ld), applies ReLU and BF16 rounding in one
+// cvt per pair and stores the next layer's operand back with tcgen05.st. The MMAs
+// (M = 128, N = 64 or 16, K = 16 each) take A from those columns and only the
+// weights from shared memory, so shared-memory bandwidth, which bounds the
+// operand-in-shared-memory form at N = 64, carries 24.5 KB per tile instead of about
+// 140 KB. Biases ride in the MMAs as before: layer 1 through its two constant-1
+// columns; layers 2-4 through one extra K step, (1, 1, 0 ...) rows in tensor memory
+// against (b_hi, b_lo, 0 ...) rows whose second core matrix is the zero block.
+// One elected lane of the warpgroup's first warp issues a layer's MMAs and commits
+// them to the warpgroup's mbarrier; the next tile's input is loaded (and encoded)
+// while the output layer's MMAs run. Error bit 1 is set if an MMA completion wait
+// gave up after `polls` polls (LAMBDA_DEFAULT_MMA_POLLS normally); the thread then
+// waits again, bounded by the default limit, for the MMAs already issued, so no TMEM
+// is read or freed under a running MMA, and the warpgroup stops after the tile.
+template <bool kQueries>
+__global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_tc(const uint4 *__restrict__ packed,
+                                                          const void *__restrict__ in, int n_rows, Range rg,
+                                                          float4 *__restrict__ out, int *error, uint32_t polls,
+                                                          const int *count = nullptr, int rows_per_count = 0) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int rows = count ? rows_per_count * *count : n_rows;
+    const int tiles = (rows + kTileM - 1) / kTileM;
+    if (int(blockIdx.x) * kChains >= tiles) return;  // uniform per block, before any TMEM allocation
+    const int tid = threadIdx.x, wg = tid >> 7, r = tid & 127, wi = (tid >> 5) & 3;
+    for (int i = tid; i < kPackedWeightBytes / 16; i += kMlpThreads) reinterpret_cast<uint4 *>(smem)[i] = packed[i];
+    for (int i = tid; i < kTileM; i += kMlpThreads) *reinterpret_cast<uint4 *>(smem + sZero + i * 16) = make_uint4(0, 0, 0, 0);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + sTmemSlot);
+    if (tid < kChains) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(smem + sBar + 8 * tid)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (tid < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(G * kTmemCols)
+                     "r"(kTmemAlloc)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -308,142 +335,25 @@ __device__ __forceinline__ TileCtx tile_setup(uint8_t *smem, const uint4 *__rest
     fence_before();
     __syncthreads();
     fence_after();
-    t.tmem = *tmem_slot + uint32_t(wg * kTmemCols);
-    t.lane_base = t.tmem + (uint32_t((warp & 3) * 32) << 16);
-    return t;
-}
-
-template <int G>
-__device__ __forceinline__ void tile_teardown(const TileCtx &t) {
-    // every TMEM read has completed (tcgen05.ld waits) before the columns are released
+    const uint32_t base = smem_u32(smem), tmem0 = *tmem_slot;
+    const uint32_t lanes = uint32_t(wi * 32) << 16;  // this warp's 32 TMEM lanes
+    if (wg == 0) {
+        const uint32_t ones[8] = {0x3F803F80u, 0, 0, 0, 0, 0, 0, 0};  // bf16 (1, 1), zeros
+        tmem_st8(tmem0 + tOnes + lanes, ones);
+        tmem_wait_st();
+    }
     fence_before();
     __syncthreads();
     fence_after();
-    if ((threadIdx.x >> 5) == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem - uint32_t((threadIdx.x >> 7) * kTmemCols)),
-                     "r"(G * kTmemCols)
-                     : "memory");
-}
-
-// ReLU + BF16 of 32 accumulator columns of this thread's row, stored as columns
-// col0 .. col0 + 31 of the next layer's operand.
-__device__ __forceinline__ void store_relu32(uint8_t *smem, const TileCtx &t, const uint32_t (&a)[32], int col0) {
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const uint4 v = make_uint4(relu_bf16x2(a[8 * c], a[8 * c + 1]), relu_bf16x2(a[8 * c + 2], a[8 * c + 3]),
-                                   relu_bf16x2(a[8 * c + 4], a[8 * c + 5]), relu_bf16x2(a[8 * c + 6], a[8 * c + 7]));
-        *reinterpret_cast<uint4 *>(smem + t.act + core_offset(t.row, col0 + 8 * c, kH)) = v;
-    }
-}
-
-// Four layers over the 128-row operand put_row stored for this warpgroup. One
-// warpgroup barrier per layer: the operand rows are in shared memory, then the
-// warpgroup's first thread issues the layer's MMAs and commits them to the mbarrier
-// every thread of the warpgroup waits on. The hidden epilogue is two 32-column TMEM
-// loads, 32 ReLU+BF16 conversions and eight 16-byte stores of the next operand row
-// (kLowRegs: one 32-column half at a time, for kernels held to 64 registers). On
-// return y holds this thread's four outputs. Returns false, uniformly across the
-// warpgroup, if an MMA completion wait gave up after `polls` polls. A thread whose
-// wait gives up then waits again, bounded by the default limit, for the MMAs already
-// issued, so no TMEM is read or freed under a running MMA; the tile runs to its end
-// in step with the warpgroup's barriers, and its result is discarded.
-template <int G, bool kLowRegs = false>
-__device__ __forceinline__ bool mlp_tile(uint8_t *smem, TileCtx &t, float *y, uint32_t polls) {
+    const uint32_t acc = tmem0 + tAcc + uint32_t(64 * wg), opnd = tmem0 + tOperand + uint32_t(32 * wg);
+    const uint32_t ones = tmem0 + tOnes, bar = base + sBar + 8 * wg;
     const uint32_t id64 = instr_desc(kH), id16 = instr_desc(kOutPad);
-    const uint32_t act = t.base + uint32_t(t.act);
-    bool done = true;
-#pragma unroll 1
-    for (int layer = 0; layer < 4; layer++) {
-        fence_proxy_async();
-        fence_before();
-        wg_sync<G>(t.wg);
-        if (t.row == 0) {
-            fence_after();
-            if (layer == 0) {
-                mma_bf16(t.tmem, smem_desc(act, 128, 256), smem_desc(t.base + sW1, 128, 256), id64, 0);
-            } else {
-                const int wofs = layer == 1 ? sW2 : (layer == 2 ? sW3 : sW4);
-                const int bofs = layer == 1 ? sB2 : (layer == 2 ? sB3 : sB4);
-                const uint32_t idesc = layer == 3 ? id16 : id64;
-                // bias: (1, 1, 0 ...) rows against (b_hi, b_lo, 0 ...) rows; second K core from the zero block
-                mma_bf16(t.tmem, smem_desc(t.base + sOnes, sZero - sOnes, 128),
-                         smem_desc(t.base + bofs, sZero - bofs, 128), idesc, 0);
+    uint32_t phase = 0;
+    auto load_row = [&](int tile, float *e) {
+        const int row = tile * kTileM + r;
 #pragma unroll
-                for (int kk = 0; kk < kH / 16; kk++)
-                    mma_bf16(t.tmem, smem_desc(act + kk * 256, 128, 1024), smem_desc(t.base + wofs + kk * 256, 128, 1024),
-                             idesc, 1);
-            }
-            mma_commit(t.bar);
-        }
-        if (!mbar_wait(t.bar, t.phase, polls)) {
-            done = false;
-            mbar_wait(t.bar, t.phase, LAMBDA_DEFAULT_MMA_POLLS);  // drain what was issued
-        }
-        t.phase ^= 1u;
-        fence_after();
-        if (layer < 3) {
-            if constexpr (kLowRegs) {
-                uint32_t a[32];
-                tmem_ld32(t.lane_base, a);
-                tmem_wait(a);
-                store_relu32(smem, t, a, 0);
-                tmem_ld32(t.lane_base + 32, a);
-                tmem_wait(a);
-                store_relu32(smem, t, a, 32);
-            } else {
-                uint32_t a[32], b[32];
-                tmem_ld32(t.lane_base, a);
-                tmem_ld32(t.lane_base + 32, b);
-                tmem_wait(a);
-                tmem_after_wait(b);
-                store_relu32(smem, t, a, 0);
-                store_relu32(smem, t, b, 32);
-            }
-        } else {
-            uint32_t o[4];
-            tmem_ld4(t.lane_base, o);
-            tmem_wait(o);
-            for (int i = 0; i < kOut; i++) y[i] = __uint_as_float(o[i]);
-        }
-    }
-    return wg_sync_and<G>(t.wg, done);
-}
-
-// Stores one encoded row (5 features, then the two constant-1 bias columns, zero
-// padded to K = 16) as this thread's row of its warpgroup's layer-1 operand.
-__device__ __forceinline__ void put_row(uint8_t *smem, const TileCtx &t, const float *e) {
-    float x[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) x[i] = i < kIn ? e[i] : (i < kIn + 2 ? 1.0f : 0.0f);
-    put8(smem, t.act, t.row, 0, kInPad, x);
-    put8(smem, t.act, t.row, 1, kInPad, x + 8);
-}
-
-// Inference over n_rows rows, or rows_per_count * *count rows when count is given
-// (a count the GPU produced, such as a bounce's thin-film hits): row i's input is
-// kRowStride floats already encoded (kQueries = false) or the i-th
-// lambda_film_query, encoded here (kQueries = true).
-// out: rows x (R_s, R_p, T_s, T_p). A CTA holds G warpgroups, each working through
-// its own 128-row tiles with its own accumulator, so G dependent layer chains
-// overlap per CTA while the weights are loaded once. Error bit 1 is set if an MMA
-// completion wait gave up after `polls` polls (LAMBDA_DEFAULT_MMA_POLLS normally).
-template <bool kQueries, int G>
-__global__ void __launch_bounds__(128 * G, G == 1 ? 1 : 8 / G) k_mlp_tc(const uint4 *__restrict__ packed,
-                                                                   const void *__restrict__ in, int n_rows, Range rg,
-                                                                   float4 *__restrict__ out, int *error,
-                                                                   uint32_t polls, const int *count = nullptr,
-                                                                   int rows_per_count = 0) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    const int rows = count ? rows_per_count * *count : n_rows;
-    const int tiles = (rows + kTileM - 1) / kTileM;
-    if (int(blockIdx.x) * G >= tiles) return;  // uniform per block, before any TMEM allocation
-    TileCtx t = tile_setup<G>(smem, packed);
-    bool ok = true;
-    const int wg = threadIdx.x >> 7;
-    for (int tile = blockIdx.x * G + wg; tile < tiles && ok; tile += gridDim.x * G) {
-        const int row = tile * kTileM + t.row;
-        float e[kIn] = {0, 0, 0, 0, 0};
-        if (row < rows) {
+        for (int i = 0; i < kIn; i++) e[i] = 0.0f;
+        if (tile < tiles && row < rows) {
             if constexpr (kQueries) {
                 const lambda_film_query q = static_cast<const lambda_film_query *>(in)[row];
                 const float v[kIn] = {q.lambda_nm, q.cos_theta, q.thickness_nm, q.n_film, q.n_sub};
@@ -458,13 +368,81 @@ __global__ void __launch_bounds__(128 * G, G == 1 ? 1 : 8 / G) k_mlp_tc(const ui
                 e[4] = x[4];
             }
         }
-        put_row(smem, t, e);
+    };
+    const int stride = int(gridDim.x) * kChains;
+    float e[kIn];
+    load_row(blockIdx.x * kChains + wg, e);
+    bool ok = true;
+    for (int tile = blockIdx.x * kChains + wg; tile < tiles && ok; tile += stride) {
+        const int row = tile * kTileM + r;
+        {
+            const uint32_t x[8] = {bf16x2(e[0], e[1]), bf16x2(e[2], e[3]), bf16x2(e[4], 1.0f), bf16x2(1.0f, 0.0f), 0, 0, 0, 0};
+            tmem_st8(opnd + lanes, x);
+            tmem_wait_st();
+        }
+        bool done = true;
         float y[kOut];
-        ok = mlp_tile<G, (G > 2)>(smem, t, y, polls);
+#pragma unroll 1
+        for (int layer = 0; layer < 4; layer++) {
+            // the operand rows are in tensor memory; one lane of warp 0 issues the MMAs
+            fence_before();
+            wg_sync(wg);
+            const int wofs = layer == 0 ? sW1 : (layer == 1 ? sW2 : (layer == 2 ? sW3 : sW4));
+            const int bofs = layer == 1 ? sB2 : (layer == 2 ? sB3 : sB4);
+            const uint64_t dw = smem_desc(base + wofs, 128, layer == 0 ? 256 : 1024);
+            const uint64_t db = smem_desc(base + bofs, sZero - bofs, 128);
+            if (wi == 0) {
+                if (elect_one()) {
+                    fence_after();
+                    if (layer == 0) {
+                        mma_bf16_ts(acc, opnd, dw, id64, 0);
+                    } else {
+                        const uint32_t idesc = layer == 3 ? id16 : id64;
+                        mma_bf16_ts(acc, ones, db, idesc, 0);
+#pragma unroll
+                        for (int kk = 0; kk < kH / 16; kk++)  // K step kk: operand columns 8kk.., weight bytes 256kk..
+                            mma_bf16_ts(acc, opnd + 8 * kk, dw + 16 * kk, idesc, 1);
+                    }
+                    mma_commit(bar);
+                }
+                __syncwarp();
+            }
+            if (layer == 3) load_row(tile + stride, e);  // under the output layer's MMAs
+            if (!mbar_wait(bar, phase, polls)) {
+                done = false;
+                mbar_wait(bar, phase, LAMBDA_DEFAULT_MMA_POLLS);  // drain what was issued
+            }
+            phase ^= 1u;
+            fence_after();
+            if (layer < 3) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    uint32_t a[32], x[16];
+                    tmem_ld32(acc + lanes + 32 * h, a);
+                    tmem_wait(a);
+#pragma unroll
+                    for (int i = 0; i < 16; i++) x[i] = relu_bf16x2(a[2 * i], a[2 * i + 1]);
+                    tmem_st16(opnd + lanes + 16 * h, x);
+                }
+                tmem_wait_st();
+            } else {
+                uint32_t o[4];
+                tmem_ld4(acc + lanes, o);
+                tmem_wait(o);
+#pragma unroll
+                for (int i = 0; i < kOut; i++) y[i] = __uint_as_float(o[i]);
+            }
+        }
+        ok = wg_sync_and(wg, done);
         if (ok && row < rows) out[row] = make_float4(y[0], y[1], y[2], y[3]);
     }
-    if (!ok && t.row == 0) atomicOr(error, 2);
-    tile_teardown<G>(t);
+    if (!ok && r == 0) atomicOr(error, 2);
+    // every TMEM access has completed (tcgen05 waits) before the columns are released
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (tid < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem0), "r"(kTmemAlloc) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -787,11 +765,15 @@ bool range_ok(const lambda_film_range &r) {
 // Dynamic shared memory of the MLP kernels (below the 48 KB default today; set so
 // that a larger layout needs no other change).
 cudaError_t configure_mlp_kernels() {
-    constexpr int G = kQueryWarpgroups;
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_tc<false, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOf<G>);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mlp_tc<true, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOf<G>);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmem);
     return e;
+}
+
+// Grid of the MLP kernel for `tiles` 128-row tiles: one CTA per SM (each allocates
+// all 512 TMEM columns), or fewer when there are fewer tiles than chains.
+int mlp_grid(int64_t tiles, int sm_count) {
+    return int(std::max<int64_t>(1, std::min<int64_t>((tiles + kChains - 1) / kChains, sm_count)));
 }
 
 }  // namespace mlp
@@ -828,16 +810,6 @@ lambda_status install(lambda_ctx *ctx, const float *params_host, const lambda_fi
     return LAMBDA_OK;
 }
 
-// Grid of the batched query kernel (kQueryWarpgroups warpgroups per CTA) for
-// `tiles` 128-row tiles: resident CTAs per SM, capped by TMEM, on every SM.
-template <bool kQueries>
-int query_grid(lambda_ctx *ctx, int tiles) {
-    constexpr int G = kQueryWarpgroups;
-    const int per_sm = std::min(resident_ctas((const void *)k_mlp_tc<kQueries, G>, ctx->device, 128 * G, kSmemOf<G>),
-                                512 / (G * kTmemCols));
-    return std::max(1, std::min((tiles + G - 1) / G, std::max(1, per_sm) * ctx->sm_count));
-}
-
 // Runs the MLP over n_rows encoded rows (kQueries = false) or film queries
 // (kQueries = true) on the context's stream and waits for it.
 template <bool kQueries>
@@ -848,8 +820,7 @@ lambda_status run_mlp(lambda_ctx *ctx, const void *in, int n_rows, float4 *out_d
     CK(cudaMemsetAsync(err, 0, 16, ctx->stream), "clear flags");
     const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
     const int tiles = (n_rows + kTileM - 1) / kTileM;
-    constexpr int G = kQueryWarpgroups;
-    k_mlp_tc<kQueries, G><<<query_grid<kQueries>(ctx, tiles), 128 * G, kSmemOf<G>, ctx->stream>>>(
+    k_mlp_tc<kQueries><<<mlp_grid(tiles, ctx->sm_count), kMlpThreads, kMlpSmem, ctx->stream>>>(
         reinterpret_cast<const uint4 *>(w), in, n_rows, to_range(ctx->surrogate_range), out_dev, err,
         ctx->limits.mma_polls);
     CK(cudaGetLastError(), "launch MLP kernel");
@@ -885,15 +856,13 @@ int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const
     auto grid = [&](int per_sm, int block) {
         return int(std::max<int64_t>(1, std::min<int64_t>((hits + block - 1) / block, int64_t(per_sm) * sm_count)));
     };
-    constexpr int G = kQueryWarpgroups;
     const int64_t tiles = (hits * kHero + kTileM - 1) / kTileM;
-    const int mlp_grid = int(std::max<int64_t>(1, std::min<int64_t>((tiles + G - 1) / G, int64_t(mlp_ctas_per_sm) * sm_count)));
     if (prof) prof->begin(9);
     k_film_encode<<<grid(film_encode_ctas, 256), 256, 0, s>>>(bounce, rp, sc, ps, fs, rows, in_domain);
     if (prof) prof->end();
     if (prof) prof->begin(10);
-    k_mlp_tc<false, G><<<mlp_grid, 128 * G, kSmemOf<G>, s>>>(w, rows, 0, Range{}, out, ps.error, limits.mma_polls,
-                                                             ps.counts + queue_slot(bounce, kQFilm), kHero);
+    k_mlp_tc<false><<<mlp_grid(tiles, sm_count), kMlpThreads, kMlpSmem, s>>>(
+        w, rows, 0, Range{}, out, ps.error, limits.mma_polls, ps.counts + queue_slot(bounce, kQFilm), kHero);
     if (prof) prof->end();
     if (prof) prof->begin(11);
     k_film_scatter<<<grid(film_scatter_ctas, 256), 256, 0, s>>>(bounce, rp, sc, ps, out, in_domain);
@@ -906,10 +875,8 @@ int lambda_ctx::launch_shade_surrogate(int bounce, const RenderParams &rp, const
 lambda_status lambda_ctx::ensure_surrogate_state(int pixels) {
     lambda_ctx *ctx = this;
     CK(configure_mlp_kernels(), "configure MLP kernels");
-    constexpr int G = kQueryWarpgroups;
     if (mlp_ctas_per_sm <= 0) {
-        const int per_sm = resident_ctas((const void *)k_mlp_tc<false, G>, device, 128 * G, kSmemOf<G>);
-        mlp_ctas_per_sm = std::max(1, std::min(per_sm, 512 / (G * kTmemCols)));
+        mlp_ctas_per_sm = 1;  // each CTA holds all 512 TMEM columns of its SM
         film_encode_ctas = resident_ctas((const void *)k_film_encode, device, 256, 0);
         film_scatter_ctas = resident_ctas((const void *)k_film_scatter, device, 256, 0);
     }
@@ -1259,10 +1226,9 @@ extern "C" lambda_status lambda_surrogate_eval_static(lambda_ctx *ctx, const lam
     k_encode_queries<<<(n + 255) / 256, 256, 0, ctx->stream>>>(queries, n, to_range(ctx->surrogate_range), sc.rows);
     const uint8_t *w = static_cast<const uint8_t *>(ctx->sbuf.weights_bf16.ptr);
     const int tiles = (n + kTileM - 1) / kTileM;
-    constexpr int G = kQueryWarpgroups;
-    k_mlp_tc<false, G><<<query_grid<false>(ctx, tiles), 128 * G, kSmemOf<G>, ctx->stream>>>(reinterpret_cast<const uint4 *>(w), sc.rows, n, Range{},
-                                                            reinterpret_cast<float4 *>(out), sc.error,
-                                                            ctx->limits.mma_polls);
+    k_mlp_tc<false><<<mlp_grid(tiles, ctx->sm_count), kMlpThreads, kMlpSmem, ctx->stream>>>(
+        reinterpret_cast<const uint4 *>(w), sc.rows, n, Range{}, reinterpret_cast<float4 *>(out), sc.error,
+        ctx->limits.mma_polls);
     CK(cudaGetLastError(), "launch MLP kernel");
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, sc.error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "read the static error word");
