@@ -60,6 +60,30 @@ def test_tensor_core_inference_matches_fp64_forward(ctx):
     assert (back == p).all()
 
 
+def test_tensor_core_inference_batch_sizes(ctx):
+    """Every batch size gives each query the same bits: a row's result depends only on
+    its own inputs, not on its tile, its chain (warpgroup), its CTA or the tile the
+    chain loads next. The sizes straddle one tile (128 rows), one CTA's five chains
+    (640 rows) and one tile per chain on every SM (148 x 640 rows), and the largest
+    batch is checked against the FP64 forward pass with BF16 rounding."""
+    p = _params(4, 0.2)
+    ctx.surrogate_set(p)
+    rng = np.random.default_rng(9)
+    n_max = 200_003
+    q = np.stack([rng.uniform(380, 780, n_max), rng.uniform(0, 1, n_max), rng.uniform(150, 850, n_max),
+                  rng.uniform(1.2, 1.8, n_max), rng.uniform(1.0, 2.0, n_max)], 1).astype(np.float32)
+    full = ctx.surrogate_eval(q)
+    for n in (1, 127, 128, 129, 639, 640, 641, 148 * 640, 148 * 640 + 1):
+        got = ctx.surrogate_eval(q[:n])
+        assert np.array_equal(got.view(np.uint32), full[:n].view(np.uint32)), f"n={n}"
+    x = surrogate.encode(q, lb.default_film_range())
+    want = port.mlp_forward(p.astype(np.float64), x, bf16=True)
+    err = np.abs(full - want)
+    scale = np.abs(want).max()
+    assert err.max() <= 1e-2 * scale
+    assert err.mean() <= 1e-3 * scale
+
+
 @pytest.fixture(scope="module")
 def trained(ctx):
     rep = ctx.surrogate_train(samples=1 << 21, epochs=4, batch=8192, lr=3e-3, seed=11)
