@@ -299,7 +299,7 @@ __device__ __forceinline__ bool wg_sync_and(int wg, bool v) {
 // (M = 128, N = 64 or 16, K = 16 each) take A from those columns and only the
 // weights from shared memory, so shared-memory bandwidth, which bounds the
 // operand-in-shared-memory form at N = 64, carries 24.5 KB per tile instead of about
-// 140 KB. Biases ride in the MMAs as before: layer 1 through its two constant-1
+// 140 KB. Biases ride in the MMAs: layer 1 through its two constant-1
 // columns; layers 2-4 through one extra K step, (1, 1, 0 ...) rows in tensor memory
 // against (b_hi, b_lo, 0 ...) rows whose second core matrix is the zero block.
 // One elected lane of the warpgroup's first warp issues a layer's MMAs and commits
